@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark: synaptic events/s of the grid-mode simulation step on B200.
+
+Workload (the scatter-bound roofline case): 1,000,000 LIF neurons (80 % E /
+20 % I), fixed out-degree 1,000 with targets uniform over all neurons
+(1e9 synapses: uint32 target + fp32 weight + uint8 delay, 9 GB), delays
+U{1..16} steps, dt = 0.1 ms, per-neuron 20 Hz Poisson drive (~10 Hz mean
+firing), no STDP, seeded synthetic network.  One bench step = 1,000 grid
+steps = 100 ms simulated; the default 10 timed steps simulate 1 s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one network per GPU, no collective on
+the data path: weak scaling), launched with torch.distributed.run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "synaptic events/s"
+UNIT = "events/s"
+BYTES_PER_EVENT = 9  # uint32 target + fp32 weight + uint8 delay
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--neurons", type=int, default=1_000_000)
+    ap.add_argument("--degree", type=int, default=1000)
+    ap.add_argument("--chunk", type=int, default=1000, help="grid steps per bench step")
+    ap.add_argument("--profile-steps", type=int, default=2000)
+    ap.add_argument("--cpu-steps", type=int, default=300, help="timed grid steps of the CPU sample")
+    ap.add_argument("--cpu-warmup", type=int, default=300)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args, seed=1):
+    from naer_b200 import spec as S
+    s = S.scatter_outdegree(n=args.neurons, k=args.degree, seed=seed)
+    # room for every spike of warm-up + timed + e2e + profile passes
+    s.raster_capacity = 1 << 26
+    return s
+
+
+def workload_config(args, synapses):
+    return {
+        "workload": f"scatter_outdegree: {args.neurons} LIF (80/20), fixed out-degree {args.degree}, "
+                    f"delays 1-16 steps, 20 Hz Poisson drive, no STDP",
+        "neurons": args.neurons,
+        "synapses": synapses,
+        "dt_ms": 0.1,
+        "step": f"{args.chunk} grid steps = {args.chunk * 0.1:.0f} ms simulated",
+        "aggregation": "atomic",
+        "l2": "inputs larger than L2 (9 B x synapses streamed; 126 MB L2)",
+        "parallelism": "replicas",
+    }
+
+
+class Clocks:
+    """nvidia-smi sampling in the background during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def reduce_max_sum(world, tmax, esum):
+    if world == 1:
+        return tmax, esum
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([tmax], dtype=torch.float64, device="cuda")
+    e = torch.tensor([esum], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(e.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_sample(args, spec, steps, warm):
+    """The oracle (multithreaded restatement of the reference's step) on the
+    host cores: `warm` untimed grid steps, then `steps` timed ones."""
+    from oracle import oracle as O
+    threads = O.max_threads()
+    o = O.OracleNet(spec, threads=threads, deterministic=False)
+    o.run(warm)
+    e0 = o.events
+    t0 = time.perf_counter()
+    o.run(steps)
+    dt = time.perf_counter() - t0
+    ev = o.events - e0
+    o.close()
+    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} grid steps ({steps * 0.1:.0f} ms simulated) of the same network after "
+                      f"{warm} warm-up steps; {ev} events in {dt:.2f} s"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    spec = workload(args)
+    from oracle import oracle as O
+    threads = O.max_threads()
+    o = O.OracleNet(spec, threads=threads, deterministic=False)
+    o.run(args.cpu_warmup)
+    per_step = max(10, args.cpu_steps // max(1, args.steps))
+    for _ in range(args.warmup):
+        o.run(max(1, per_step // 4))
+    e0 = o.events
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.run(per_step)
+    dt = time.perf_counter() - t0
+    ev = o.events - e0
+    value = ev / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(args, int(o.S)),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"each step {per_step} grid steps of the same network on the host cores "
+                                   f"(the reference's OpenCL kernels cannot run here: no OpenCL runtime)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    from naer_b200 import spec as S
+
+    spec = workload(args, seed=1 + rank)
+    net = S.build(spec, device=local)
+    stream = torch.cuda.ExternalStream(net.stream(), device=torch.device("cuda", local))
+    chunk = args.chunk
+
+    # warm-up
+    for _ in range(args.warmup):
+        net.run(chunk)
+    net.finish()
+
+    # timed region: device-resident inputs, CUDA events on the engine stream
+    clocks = Clocks(local) if rank == 0 else None
+    st0 = net.stats()
+    barrier(world)
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        net.run(chunk)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop() if clocks else None
+    ms = ev0.elapsed_time(ev1)
+    st1 = net.stats()
+    events = st1["events"] - st0["events"]
+    spikes = st1["spikes"] - st0["spikes"]
+    ms_max, events_all = reduce_max_sum(world, ms, float(events))
+    value = events_all / (ms_max / 1e3)
+
+    # roofline: per-kernel CUDA events around every launch on the engine stream
+    net.set_profiling(True)
+    p0 = net.stats()["events"]
+    net.run(args.profile_steps)
+    net.finish()
+    prof = net.profile()
+    net.set_profiling(False)
+    pev = net.stats()["events"] - p0
+    scatter_s = prof["scatter_ms"] / 1e3
+    lif_s = prof["lif_ms"] / 1e3
+    peak = None
+    peak_src = "fallback"
+    try:
+        peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]
+        peak_src = "measured"
+    except Exception:
+        peak = 6650.0
+    achieved = BYTES_PER_EVENT * pev / scatter_s / 1e9 if scatter_s > 0 else 0.0
+    traffic = None
+    tfile = ROOT / "profiles" / "scatter_traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get("bytes_per_event")
+            traffic = traffic * pev / max(1, prof["steps"]) if traffic else None
+        except Exception:
+            traffic = None
+
+    # end to end through the C ABI: step calls + raster readback into pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        cap = max(1, int(spikes / max(1, args.steps) * 4) + 100_000)
+        host = torch.empty((cap, 2), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        net.clear_spikes()
+        barrier(world)
+        e0 = net.stats()["events"]
+        t0 = time.perf_counter()
+        read = 0
+        d2h = 0
+        for _ in range(args.steps):
+            net.run(chunk)
+            n = net.read_raster(host, first=read)
+            read += n
+            d2h += n * 8
+        t1 = time.perf_counter()
+        e_ev = net.stats()["events"] - e0
+        e_s, e_all = reduce_max_sum(world, t1 - t0, float(e_ev))
+        e2e = {"value": e_all / e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
+               "d2h_bytes_per_step": int(d2h / args.steps),
+               "note": "naer_net_step + naer_net_read_raster per step; the network and its Poisson drive "
+                       "are device-resident, as in the reference, so no input crosses host->device"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        net.close()
+        cpu = cpu_sample(args, spec, args.cpu_steps, args.cpu_warmup)
+    else:
+        net.close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args, int(st1["synapses"])),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "kernel": "k_scatter_atomic",
+                         "peak_source": peak_src,
+                         "note": f"{BYTES_PER_EVENT} B x {pev} events over {prof['steps']} scatter launches, "
+                                 f"{prof['scatter_ms']:.2f} ms total (LIF {prof['lif_ms']:.2f} ms)"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 2 * chunk * args.steps,
+            "clocks": clk,
+            "spikes_per_s_sim": spikes / (args.steps * chunk * 1e-4) / args.neurons,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,226 @@
+/*
+ * naer_capi.h — C ABI of the B200 spiking-network step.
+ *
+ * This is the boundary the reference's C++ `Naer::Network`
+ * (include/naer/Network.h:15-142, src/Network.cpp) drives.  The reference
+ * holds OpenCL objects directly; here every device object lives behind an
+ * opaque handle and every entry point is a plain C function: no C++ or torch
+ * types cross the boundary, so ctypes, cgo, JNI or N-API can bind it.
+ *
+ * Conventions
+ *  - Every function returns an int status: NAER_OK (0) or a negative
+ *    NAER_E_* code.  naer_last_error() returns the message of the last
+ *    failure on the calling thread.  No exception crosses the ABI; the C++
+ *    wrapper in include/naer/Network.h turns a non-zero status into
+ *    std::runtime_error, as the reference does for every OpenCL failure
+ *    (e.g. src/Network.cpp:21-23, 146-149).
+ *  - Device memory is owned by the handle; host buffers are owned by the
+ *    caller.  A handle is used by one host thread at a time.
+ *  - Units: time in microseconds (reference: uint32 µs, Network.h:67) or in
+ *    grid steps; potentials and weights in the caller's unit (the reference
+ *    uses volts, lif.cl:3-6; the benchmark configurations use mV).
+ */
+#ifndef NAER_CAPI_H
+#define NAER_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define NAER_API __attribute__((visibility("default")))
+#else
+#define NAER_API
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define NAER_OK 0
+#define NAER_E_INVALID (-1)     /* bad argument or specification */
+#define NAER_E_OOM (-2)         /* device or host allocation failed */
+#define NAER_E_OVERFLOW (-3)    /* a fixed-capacity buffer would overflow */
+#define NAER_E_TIMEOUT (-4)     /* a bounded device wait gave up */
+#define NAER_E_CUDA (-5)        /* CUDA runtime error */
+#define NAER_E_STATE (-6)       /* call not valid in the handle's state */
+#define NAER_E_UNSUPPORTED (-7) /* feature not available in this build */
+
+/* ---- enumerations ---------------------------------------------------- */
+/* Neuron kinds of the reference (NeuronType enum use: Network.h:81-119,
+ * main.cpp:18-20): plastic LIF, static LIF, Poisson input. */
+#define NAER_NEURON_STDP 0u
+#define NAER_NEURON_NOP 1u
+#define NAER_NEURON_POISSON 2u
+
+/* Time discretisation.  GRID: fixed step dt_us with per-synapse delays and
+ * a delay ring buffer.  EVENT: the reference's window semantics
+ * (Network.cpp:122-256): exact per-event LIF decay in µs inside windows of
+ * dt_us and one axonal delay of dt_us. */
+#define NAER_MODE_GRID 0u
+#define NAER_MODE_EVENT 1u
+
+/* Spike aggregation into the ring buffer.  ATOMIC: float reductions, order
+ * not fixed.  DETERMINISTIC: per step, events sorted by ring cell and summed
+ * in ascending (source, synapse) order; bit-reproducible. */
+#define NAER_AGG_ATOMIC 0u
+#define NAER_AGG_DETERMINISTIC 1u
+
+/* Connection rules.  REF_BERNOULLI is the reference's pairwise Philox test
+ * (include/naer/kernels/network.cl:14-107); the fixed-degree rules draw
+ * targets (out-degree) or sources (in-degree) uniformly with Philox. */
+#define NAER_CONN_REF_BERNOULLI 0u
+#define NAER_CONN_FIXED_INDEGREE 1u
+#define NAER_CONN_FIXED_OUTDEGREE 2u
+
+/* ---- parameter blocks ------------------------------------------------- */
+typedef struct naer_net_params {
+    uint32_t mode;            /* NAER_MODE_* */
+    uint32_t aggregation;     /* NAER_AGG_* */
+    uint32_t dt_us;           /* grid step (default 100) / event window (1500) */
+    uint32_t record_spikes;   /* 1: append every spike to the device raster */
+    uint64_t raster_capacity; /* raster records kept on the device */
+    uint32_t poisson_seed;    /* Philox key word 1 of POISSON populations;
+                                 the reference passes 0x15ac7ebd every step
+                                 (Network.cpp:124) */
+    uint32_t stdp_enabled;    /* pair-based STDP on STDP->STDP synapses */
+    float tau_plus_ms;        /* pre trace time constant */
+    float tau_minus_ms;       /* post trace time constant */
+    float a_plus;             /* LTP amplitude, in units of w_max */
+    float a_minus;            /* LTD amplitude, in units of w_max */
+    float w_max;              /* weights clipped to [0, w_max] */
+    uint32_t stdp_history;    /* post spikes remembered per neuron for lazy LTP */
+} naer_net_params;
+
+typedef struct naer_pop_params {
+    float tau_m_ms;       /* membrane time constant (reference T_MEM, lif.cl:3) */
+    float v_th;           /* spike iff V > v_th (lif.cl:28) */
+    float v_reset;        /* V after a spike (lif.cl:32) */
+    float t_ref_ms;       /* refractory time (lif.cl:4,31) */
+    float v_init;         /* V at step 0 */
+    float rate_hz;        /* POISSON populations: rate (input_neuron_group.cl:4) */
+    float drive_rate_hz;  /* LIF populations: per-neuron Poisson drive, 0 = off */
+    float drive_weight;   /* LIF populations: weight of one drive event */
+    uint32_t drive_seed;  /* Philox key word 1 of the drive */
+    uint32_t pad_;
+} naer_pop_params;
+
+typedef struct naer_conn_spec {
+    uint32_t rule;        /* NAER_CONN_* */
+    uint32_t degree;      /* K of the fixed-degree rules */
+    double probability;   /* REF_BERNOULLI connection probability */
+    float weight;         /* weight; 0 => uniform in [wmin, wmax) (network.cl:97-100) */
+    float wmin;
+    float wmax;
+    uint32_t delay_min;   /* grid steps, >= 1 */
+    uint32_t delay_max;   /* grid steps, >= delay_min */
+    uint32_t pad_;
+    uint64_t seed;        /* REF_BERNOULLI uses the low 32 bits, as the
+                             reference does (Network.cpp:447,532) */
+} naer_conn_spec;
+
+typedef struct naer_stats {
+    uint64_t step;              /* grid steps (or event windows) simulated */
+    uint64_t events;            /* synaptic events delivered */
+    uint64_t spikes;            /* spikes recorded in the raster */
+    uint64_t raster_dropped;    /* spikes not recorded: raster full */
+    uint64_t stdp_hist_overflow;/* lazy-LTP lookups that hit the history limit */
+    uint64_t synapses;          /* synapses (unpadded) */
+    uint64_t device_bytes;      /* device memory held by the handle */
+    uint32_t neurons;
+    uint32_t ring_slots;
+} naer_stats;
+
+typedef struct naer_net naer_net;
+
+/* ---- library ---------------------------------------------------------- */
+NAER_API int naer_last_error(char* buf, size_t len);
+NAER_API int naer_device_count(int* count);
+NAER_API int naer_net_params_default(naer_net_params* p);
+NAER_API int naer_pop_params_default(uint32_t neuron_type, naer_pop_params* p);
+
+/* ---- one network: the plain form --------------------------------------- */
+
+/* Network::Network (Network.cpp:14-47): binds a device, creates the queue. */
+NAER_API int naer_net_create(int device, const naer_net_params* params, naer_net** out);
+
+/* Network::~Network (Network.cpp:49-75; the reference releases nothing). */
+NAER_API int naer_net_destroy(naer_net* net);
+
+/* Network::addPopulation (Network.cpp:77-83).  *type_address receives the
+ * address within the neuron type, as the reference's Population::baseAddress
+ * holds before compile(); naer_net_population_base gives the final address. */
+NAER_API int naer_net_add_population(naer_net* net, uint32_t neuron_type, uint32_t size,
+                                     const naer_pop_params* params, uint32_t* pop_id,
+                                     uint32_t* type_address);
+
+/* Network::addConnection (both overloads, Network.cpp:85-105). */
+NAER_API int naer_net_add_connection(naer_net* net, uint32_t src_pop, uint32_t dst_pop,
+                                     const naer_conn_spec* spec);
+
+/* Network::compile (Network.cpp:267-308): address layout, device buffers,
+ * connectivity generated on the device. */
+NAER_API int naer_net_compile(naer_net* net);
+
+/* Population::baseAddress after compile() (Network.cpp:283-285). */
+NAER_API int naer_net_population_base(naer_net* net, uint32_t pop_id, uint32_t* base_address);
+
+/* Network::step (Network.cpp:122-256), asynchronous: enqueues nsteps grid
+ * steps (GRID) or nsteps windows (EVENT) and returns. */
+NAER_API int naer_net_step(naer_net* net, uint64_t nsteps);
+
+/* Network::finish (Network.cpp:258-265): blocks until the queue drains and
+ * reports any device-side error. */
+NAER_API int naer_net_finish(naer_net* net);
+
+/* Network::getTime (Network.cpp:107-110), in µs, 64-bit. */
+NAER_API int naer_net_get_time_us(naer_net* net, uint64_t* time_us);
+/* Network::getSynapses / getNeurons (Network.cpp:112-120). */
+NAER_API int naer_net_get_synapses(naer_net* net, uint64_t* synapses);
+NAER_API int naer_net_get_neurons(naer_net* net, uint32_t* neurons);
+
+/* Counters; blocks like finish(). */
+NAER_API int naer_net_get_stats(naer_net* net, naer_stats* stats);
+
+/* Raster readback (the reference never reads spikes back).  Copies records
+ * [first, first + capacity) of the raster: steps[i] is the grid step (EVENT:
+ * the spike time in µs), ids[i] the reference address.  Records are grouped
+ * by step in increasing step order; within a step the order is arbitrary in
+ * ATOMIC mode and ascending address in DETERMINISTIC mode.  Blocks. */
+NAER_API int naer_net_read_spikes(naer_net* net, uint64_t first, uint64_t capacity,
+                                  uint32_t* steps, uint32_t* ids, uint64_t* count);
+NAER_API int naer_net_clear_spikes(naer_net* net);
+
+/* Raw raster records [first, first + capacity) copied straight into a
+ * caller buffer of 2 * capacity uint32 ({step, id} pairs, step order, no
+ * ordering within a step): the zero-copy-overhead readback for streaming.
+ * Blocks. */
+NAER_API int naer_net_read_raster(naer_net* net, uint64_t first, uint64_t capacity, uint32_t* records,
+                                  uint64_t* count);
+
+/* The CUDA stream (cudaStream_t) every launch of this handle is issued on,
+ * for callers that order their own work or record events against it. */
+NAER_API int naer_net_stream(naer_net* net, void** stream);
+
+/* Neuron state in address order (n = getNeurons()).  POISSON neurons report
+ * v = 0, refractory = 0. Blocks. */
+NAER_API int naer_net_read_state(naer_net* net, float* v, uint32_t* refractory);
+NAER_API int naer_net_write_state(naer_net* net, const float* v, const uint32_t* refractory);
+
+/* Connectivity in address order, unpadded: row_ptr[n+1], tgt/w/delay[S].
+ * Synapses of a row appear in the order the scatter visits them. Blocks. */
+NAER_API int naer_net_read_csr(naer_net* net, uint64_t* row_ptr, uint32_t* tgt, float* w,
+                               uint8_t* delay);
+
+/* Per-kernel device time accumulated while profiling is on (cudaEvent pairs
+ * around each launch; the reference's PROFILING counters, Network.h:11,50-55).
+ * names: "lif", "scatter". */
+NAER_API int naer_net_set_profiling(naer_net* net, int enable);
+NAER_API int naer_net_get_profile(naer_net* net, double* lif_ms, double* scatter_ms,
+                                  uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NAER_CAPI_H */

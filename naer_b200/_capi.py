@@ -1,0 +1,175 @@
+"""ctypes binding of include/naer/naer_capi.h (the library's C ABI).
+
+The library is the in-tree ``libnaer_b200.so`` built by ``naer_b200.build``.
+Loading fails loudly when it is missing: there is no fallback
+implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libnaer_b200.so"
+
+NAER_OK = 0
+NAER_E_INVALID = -1
+NAER_E_OOM = -2
+NAER_E_OVERFLOW = -3
+NAER_E_TIMEOUT = -4
+NAER_E_CUDA = -5
+NAER_E_STATE = -6
+NAER_E_UNSUPPORTED = -7
+
+STATUS_NAMES = {
+    NAER_E_INVALID: "NAER_E_INVALID",
+    NAER_E_OOM: "NAER_E_OOM",
+    NAER_E_OVERFLOW: "NAER_E_OVERFLOW",
+    NAER_E_TIMEOUT: "NAER_E_TIMEOUT",
+    NAER_E_CUDA: "NAER_E_CUDA",
+    NAER_E_STATE: "NAER_E_STATE",
+    NAER_E_UNSUPPORTED: "NAER_E_UNSUPPORTED",
+}
+
+NEURON_STDP, NEURON_NOP, NEURON_POISSON = 0, 1, 2
+MODE_GRID, MODE_EVENT = 0, 1
+AGG_ATOMIC, AGG_DETERMINISTIC = 0, 1
+CONN_REF_BERNOULLI, CONN_FIXED_INDEGREE, CONN_FIXED_OUTDEGREE = 0, 1, 2
+
+
+class NetParams(C.Structure):
+    _fields_ = [
+        ("mode", C.c_uint32),
+        ("aggregation", C.c_uint32),
+        ("dt_us", C.c_uint32),
+        ("record_spikes", C.c_uint32),
+        ("raster_capacity", C.c_uint64),
+        ("poisson_seed", C.c_uint32),
+        ("stdp_enabled", C.c_uint32),
+        ("tau_plus_ms", C.c_float),
+        ("tau_minus_ms", C.c_float),
+        ("a_plus", C.c_float),
+        ("a_minus", C.c_float),
+        ("w_max", C.c_float),
+        ("stdp_history", C.c_uint32),
+    ]
+
+
+class PopParams(C.Structure):
+    _fields_ = [
+        ("tau_m_ms", C.c_float),
+        ("v_th", C.c_float),
+        ("v_reset", C.c_float),
+        ("t_ref_ms", C.c_float),
+        ("v_init", C.c_float),
+        ("rate_hz", C.c_float),
+        ("drive_rate_hz", C.c_float),
+        ("drive_weight", C.c_float),
+        ("drive_seed", C.c_uint32),
+        ("pad_", C.c_uint32),
+    ]
+
+
+class ConnSpecC(C.Structure):
+    _fields_ = [
+        ("rule", C.c_uint32),
+        ("degree", C.c_uint32),
+        ("probability", C.c_double),
+        ("weight", C.c_float),
+        ("wmin", C.c_float),
+        ("wmax", C.c_float),
+        ("delay_min", C.c_uint32),
+        ("delay_max", C.c_uint32),
+        ("pad_", C.c_uint32),
+        ("seed", C.c_uint64),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("step", C.c_uint64),
+        ("events", C.c_uint64),
+        ("spikes", C.c_uint64),
+        ("raster_dropped", C.c_uint64),
+        ("stdp_hist_overflow", C.c_uint64),
+        ("synapses", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+        ("neurons", C.c_uint32),
+        ("ring_slots", C.c_uint32),
+    ]
+
+
+class NaerError(RuntimeError):
+    """A non-zero status from the C ABI (message from naer_last_error)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+_P = C.POINTER
+_vp = C.c_void_p
+
+# name -> argtypes (all return int status)
+PROTOTYPES = {
+    "naer_last_error": [C.c_char_p, C.c_size_t],
+    "naer_device_count": [_P(C.c_int)],
+    "naer_net_params_default": [_P(NetParams)],
+    "naer_pop_params_default": [C.c_uint32, _P(PopParams)],
+    "naer_net_create": [C.c_int, _P(NetParams), _P(_vp)],
+    "naer_net_destroy": [_vp],
+    "naer_net_add_population": [_vp, C.c_uint32, C.c_uint32, _P(PopParams), _P(C.c_uint32), _P(C.c_uint32)],
+    "naer_net_add_connection": [_vp, C.c_uint32, C.c_uint32, _P(ConnSpecC)],
+    "naer_net_compile": [_vp],
+    "naer_net_population_base": [_vp, C.c_uint32, _P(C.c_uint32)],
+    "naer_net_step": [_vp, C.c_uint64],
+    "naer_net_finish": [_vp],
+    "naer_net_get_time_us": [_vp, _P(C.c_uint64)],
+    "naer_net_get_synapses": [_vp, _P(C.c_uint64)],
+    "naer_net_get_neurons": [_vp, _P(C.c_uint32)],
+    "naer_net_get_stats": [_vp, _P(Stats)],
+    "naer_net_read_spikes": [_vp, C.c_uint64, C.c_uint64, _vp, _vp, _P(C.c_uint64)],
+    "naer_net_clear_spikes": [_vp],
+    "naer_net_read_raster": [_vp, C.c_uint64, C.c_uint64, _vp, _P(C.c_uint64)],
+    "naer_net_stream": [_vp, _P(_vp)],
+    "naer_net_read_state": [_vp, _vp, _vp],
+    "naer_net_write_state": [_vp, _vp, _vp],
+    "naer_net_read_csr": [_vp, _vp, _vp, _vp, _vp],
+    "naer_net_set_profiling": [_vp, C.c_int],
+    "naer_net_get_profile": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
+}
+
+_lib = None
+
+
+def load(path: os.PathLike | str | None = None) -> C.CDLL:
+    """Loads the CUDA library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"naer_b200 CUDA library not found at {p}; build it with `python -m naer_b200.build`")
+    lib = C.CDLL(str(p))
+    for name, args in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(4096)
+    load().naer_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != NAER_OK:
+        raise NaerError(status, last_error())
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args))

@@ -1,0 +1,198 @@
+// Device connectivity builders.  The reference builds its segmented CSR with
+// count_connections / integrate_connections / generate_connections
+// (include/naer/kernels/network.cl:14-107, driven by src/Network.cpp:421-569);
+// its scan runs on a single work-item and its fill order depends on local
+// atomics.  Here counts, a device scan (CUB, on the host side) and the fill
+// are all parallel and the row order is fixed.
+#include "build_kernels.cuh"
+
+namespace naer {
+
+__global__ void k_fill_u32(uint32_t* a, uint64_t n, uint32_t v) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+
+// REF_BERNOULLI: source s (local index) is connected to target d (local
+// index) iff uniform_rand(seed, d) < p, evaluated by the reference's
+// work-item s*32 + d%32 (count_connections, network.cl:25-41; the launch is
+// src_size*32 items in groups of 32, Network.cpp:462).
+__device__ __forceinline__ void bern_draw(const ConnBuild& cb, uint32_t s, uint32_t d, bool& conn,
+                                          double& x, uint32_t& word0) {
+    const u32x4 r = philox4x32_10(d, 0u, 0u, 0u, s * 32u + (d & 31u), cb.seed_lo);
+    x = (double)r.v[2] / 4294967295.0;
+    conn = x < cb.p;
+    word0 = r.v[0];
+}
+
+__global__ void k_bern_count(ConnBuild cb, uint32_t* cnt) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < cb.src_size; s += nw) {
+        uint32_t c = 0;
+        for (uint32_t d0 = 0; d0 < cb.dst_size; d0 += 32) {
+            const uint32_t d = d0 + lane;
+            bool conn = false;
+            double x;
+            uint32_t w0;
+            if (d < cb.dst_size) bern_draw(cb, s, d, conn, x, w0);
+            c += __popc(__ballot_sync(0xFFFFFFFFu, conn));
+        }
+        if (lane == 0) cnt[s] = c;
+    }
+}
+
+__global__ void k_bern_fill(ConnBuild cb, const uint64_t* cursor, uint32_t* tgt, float* w,
+                            uint8_t* dly) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < cb.src_size; s += nw) {
+        uint64_t pos = cursor[cb.src_storage + s];
+        for (uint32_t d0 = 0; d0 < cb.dst_size; d0 += 32) {
+            const uint32_t d = d0 + lane;
+            bool conn = false;
+            double x = 0.0;
+            uint32_t w0 = 0;
+            if (d < cb.dst_size) bern_draw(cb, s, d, conn, x, w0);
+            const uint32_t b = __ballot_sync(0xFFFFFFFFu, conn);
+            if (conn) {
+                const uint64_t o = pos + __popc(b & lt);
+                tgt[o] = cb.dst_storage + d;
+                w[o] = cb.weight == 0.0f ? conn_uniform_weight(cb.wmin, cb.wmax, __double2float_rn(x))
+                                         : cb.weight;
+                dly[o] = (uint8_t)conn_delay(cb.dmin, cb.dmax, w0);
+            }
+            pos += __popc(b);
+        }
+    }
+}
+
+// FIXED_OUTDEGREE: draw k of source s picks target umulhi(word, dst_size)
+// from Philox(ctr {s, k/4, 0, 0}, key {seed_lo, seed_hi}) word k%4; the
+// delay uses ctr word 2 = 1 and the random weight ctr word 2 = 2.
+__global__ void k_outdeg_fill(ConnBuild cb, const uint64_t* cursor, uint32_t* tgt, float* w,
+                              uint8_t* dly) {
+    const uint32_t blocks = (cb.K + 3u) >> 2;
+    const uint64_t total = (uint64_t)cb.src_size * blocks;
+    for (uint64_t it = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; it < total;
+         it += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = (uint32_t)(it / blocks);
+        const uint32_t b = (uint32_t)(it % blocks);
+        const u32x4 rt = philox4x32_10(s, b, 0u, 0u, cb.seed_lo, cb.seed_hi);
+        const u32x4 rd = philox4x32_10(s, b, 1u, 0u, cb.seed_lo, cb.seed_hi);
+        u32x4 rw;
+        if (cb.weight == 0.0f) rw = philox4x32_10(s, b, 2u, 0u, cb.seed_lo, cb.seed_hi);
+        const uint64_t base = cursor[cb.src_storage + s];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t k = b * 4u + j;
+            if (k >= cb.K) break;
+            const uint64_t o = base + k;
+            tgt[o] = cb.dst_storage + conn_pick(rt.v[j], cb.dst_size);
+            w[o] = cb.weight == 0.0f ? conn_uniform_weight(cb.wmin, cb.wmax, conn_unit_float(rw.v[j]))
+                                     : cb.weight;
+            dly[o] = (uint8_t)conn_delay(cb.dmin, cb.dmax, rd.v[j]);
+        }
+    }
+}
+
+// FIXED_INDEGREE: draw k of target i picks source umulhi(word, src_size)
+// from Philox(ctr {i, k/4, 0, 0}, key {seed_lo, seed_hi}) word k%4; delays
+// and random weights as for FIXED_OUTDEGREE, indexed by (i, k).
+__global__ void k_indeg_count(ConnBuild cb, uint32_t* cnt) {
+    const uint32_t blocks = (cb.K + 3u) >> 2;
+    const uint64_t total = (uint64_t)cb.dst_size * blocks;
+    for (uint64_t it = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; it < total;
+         it += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = (uint32_t)(it / blocks);
+        const uint32_t b = (uint32_t)(it % blocks);
+        const u32x4 r = philox4x32_10(i, b, 0u, 0u, cb.seed_lo, cb.seed_hi);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (b * 4u + j >= cb.K) break;
+            atomicAdd(cnt + conn_pick(r.v[j], cb.src_size), 1u);
+        }
+    }
+}
+
+__global__ void k_indeg_fill(ConnBuild cb, unsigned long long* cursor, unsigned long long* keys) {
+    const uint32_t blocks = (cb.K + 3u) >> 2;
+    const uint64_t total = (uint64_t)cb.dst_size * blocks;
+    for (uint64_t it = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; it < total;
+         it += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = (uint32_t)(it / blocks);
+        const uint32_t b = (uint32_t)(it % blocks);
+        const u32x4 r = philox4x32_10(i, b, 0u, 0u, cb.seed_lo, cb.seed_hi);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t k = b * 4u + j;
+            if (k >= cb.K) break;
+            const uint32_t s = conn_pick(r.v[j], cb.src_size);
+            const unsigned long long pos = atomicAdd(cursor + s, 1ull);
+            keys[pos] = (unsigned long long)i * cb.K + k;
+        }
+    }
+}
+
+// After the per-source segments of `keys` are sorted: write entry e of the
+// connection-local order into the source's row.
+__global__ void k_indeg_finalize(ConnBuild cb, const unsigned long long* keys, uint64_t total,
+                                 const uint64_t* conn_off, const uint64_t* cursor, uint32_t* tgt,
+                                 float* w, uint8_t* dly) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        // source: last s with conn_off[s] <= e
+        uint32_t lo = 0, hi = cb.src_size;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (conn_off[mid] <= e) lo = mid; else hi = mid;
+        }
+        const uint32_t s = lo;
+        const unsigned long long key = keys[e];
+        const uint32_t i = (uint32_t)(key / cb.K);
+        const uint32_t k = (uint32_t)(key % cb.K);
+        const uint32_t b = k >> 2, j = k & 3u;
+        const uint64_t o = cursor[cb.src_storage + s] + (e - conn_off[s]);
+        tgt[o] = cb.dst_storage + i;
+        const u32x4 rd = philox4x32_10(i, b, 1u, 0u, cb.seed_lo, cb.seed_hi);
+        dly[o] = (uint8_t)conn_delay(cb.dmin, cb.dmax, rd.v[j]);
+        if (cb.weight == 0.0f) {
+            const u32x4 rw = philox4x32_10(i, b, 2u, 0u, cb.seed_lo, cb.seed_hi);
+            w[o] = conn_uniform_weight(cb.wmin, cb.wmax, conn_unit_float(rw.v[j]));
+        } else {
+            w[o] = cb.weight;
+        }
+    }
+}
+
+__global__ void k_row_len_add(const uint32_t* cnt, uint32_t src_size, uint32_t src_storage,
+                              uint64_t* len) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < src_size; s += gridDim.x * blockDim.x)
+        len[src_storage + s] += cnt[s];
+}
+
+__global__ void k_row_pad(const uint64_t* len, uint32_t n, uint64_t* padded) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x)
+        padded[i] = i < n ? (len[i] + (kRowAlign - 1)) / kRowAlign * kRowAlign : 0ull;
+}
+
+__global__ void k_cursor_advance(const uint32_t* cnt, uint32_t src_size, uint32_t src_storage,
+                                 uint64_t* cursor) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < src_size; s += gridDim.x * blockDim.x)
+        cursor[src_storage + s] += cnt[s];
+}
+
+__global__ void k_pad_fill(const uint64_t* row_ptr, const uint64_t* len, uint32_t n, uint32_t* tgt,
+                           float* w, uint8_t* dly) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        for (uint64_t o = row_ptr[i] + len[i]; o < row_ptr[i + 1]; ++o) {
+            tgt[o] = kTgtSentinel;
+            w[o] = 0.0f;
+            dly[o] = 1;
+        }
+    }
+}
+
+}  // namespace naer

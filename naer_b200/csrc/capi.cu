@@ -1,0 +1,366 @@
+// extern "C" boundary: every entry point of include/naer/naer_capi.h.
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/naer/naer_capi.h"
+#include "engine.h"
+
+using naer::Error;
+
+struct naer_net {
+    std::unique_ptr<naer::Engine> eng;
+    naer::NetHost net;
+    uint32_t type_count[3] = {0, 0, 0};
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return NAER_OK;
+    } catch (const Error& e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(NAER_E_OOM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(NAER_E_INVALID, e.what());
+    }
+}
+
+void need(bool ok, int code, const char* msg) {
+    if (!ok) throw Error(code, msg);
+}
+
+void need_compiled(const naer_net* n) {
+    need(n != nullptr, NAER_E_INVALID, "null network handle");
+    need(n->net.compiled, NAER_E_STATE, "network is not compiled");
+}
+
+}  // namespace
+
+extern "C" {
+
+int naer_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return NAER_E_INVALID;
+    const size_t n = std::min(len - 1, g_last_error.size());
+    std::memcpy(buf, g_last_error.data(), n);
+    buf[n] = '\0';
+    return NAER_OK;
+}
+
+int naer_device_count(int* count) {
+    return guarded([&] {
+        need(count != nullptr, NAER_E_INVALID, "null pointer");
+        int n = 0;
+        const cudaError_t e = cudaGetDeviceCount(&n);
+        if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) {
+            (void)cudaGetLastError();
+            n = 0;
+        } else {
+            NAER_CK(e);
+        }
+        *count = n;
+    });
+}
+
+int naer_net_params_default(naer_net_params* p) {
+    if (!p) return fail(NAER_E_INVALID, "null pointer");
+    std::memset(p, 0, sizeof(*p));
+    p->mode = NAER_MODE_GRID;
+    p->aggregation = NAER_AGG_ATOMIC;
+    p->dt_us = 100;
+    p->record_spikes = 1;
+    p->raster_capacity = 1ull << 24;
+    p->poisson_seed = 0x15ac7ebdu;  // (uint32_t)0xbf785e3215ac7ebd, Network.cpp:124
+    p->stdp_enabled = 0;
+    p->tau_plus_ms = 20.0f;
+    p->tau_minus_ms = 20.0f;
+    p->a_plus = 0.01f;
+    p->a_minus = 0.0105f;
+    p->w_max = 0.5f;
+    p->stdp_history = 10;  // NAER_HIST_LENGTH, stdp_group.cl:4
+    return NAER_OK;
+}
+
+int naer_pop_params_default(uint32_t neuron_type, naer_pop_params* p) {
+    if (!p) return fail(NAER_E_INVALID, "null pointer");
+    if (neuron_type > NAER_NEURON_POISSON) return fail(NAER_E_INVALID, "unknown neuron type");
+    std::memset(p, 0, sizeof(*p));
+    // reference constants: lif.cl:3-6, input_neuron_group.cl:4
+    p->tau_m_ms = 20.0f;
+    p->v_th = 0.020f;
+    p->v_reset = 0.0f;
+    p->t_ref_ms = 2.0f;
+    p->v_init = 0.0f;
+    p->rate_hz = neuron_type == NAER_NEURON_POISSON ? 20.0f : 0.0f;
+    return NAER_OK;
+}
+
+int naer_net_create(int device, const naer_net_params* params, naer_net** out) {
+    return guarded([&] {
+        need(out != nullptr, NAER_E_INVALID, "null output pointer");
+        *out = nullptr;
+        naer_net_params p;
+        if (params) p = *params; else naer_net_params_default(&p);
+        need(p.mode == NAER_MODE_GRID || p.mode == NAER_MODE_EVENT, NAER_E_INVALID, "unknown mode");
+        need(p.aggregation <= NAER_AGG_DETERMINISTIC, NAER_E_INVALID, "unknown aggregation");
+        need(p.dt_us > 0, NAER_E_INVALID, "dt_us must be positive");
+        if (p.mode == NAER_MODE_EVENT)
+            throw Error(NAER_E_UNSUPPORTED, "event mode is not available in this build");
+        auto n = std::make_unique<naer_net>();
+        n->net.params = p;
+        n->eng = std::make_unique<naer::Engine>(device);
+        *out = n.release();
+    });
+}
+
+int naer_net_destroy(naer_net* net) {
+    if (!net) return NAER_OK;
+    return guarded([&] {
+        if (net->net.compiled) net->eng->free_net(net->net);
+        delete net;
+    });
+}
+
+int naer_net_add_population(naer_net* net, uint32_t neuron_type, uint32_t size,
+                            const naer_pop_params* params, uint32_t* pop_id, uint32_t* type_address) {
+    return guarded([&] {
+        need(net != nullptr, NAER_E_INVALID, "null network handle");
+        need(!net->net.compiled, NAER_E_STATE, "network already compiled");
+        need(neuron_type <= NAER_NEURON_POISSON, NAER_E_INVALID, "unknown neuron type");
+        uint64_t total = (uint64_t)net->type_count[0] + net->type_count[1] + net->type_count[2] + size;
+        need(total < 0x7FFFFFF0ull, NAER_E_INVALID, "too many neurons");
+        naer::PopSpec ps;
+        ps.type = neuron_type;
+        ps.size = size;
+        if (params) ps.prm = *params; else naer_pop_params_default(neuron_type, &ps.prm);
+        ps.type_address = net->type_count[neuron_type];
+        net->type_count[neuron_type] += size;
+        net->net.pops.push_back(ps);
+        if (pop_id) *pop_id = (uint32_t)net->net.pops.size() - 1;
+        if (type_address) *type_address = ps.type_address;
+    });
+}
+
+int naer_net_add_connection(naer_net* net, uint32_t src_pop, uint32_t dst_pop,
+                            const naer_conn_spec* spec) {
+    return guarded([&] {
+        need(net != nullptr && spec != nullptr, NAER_E_INVALID, "null argument");
+        need(!net->net.compiled, NAER_E_STATE, "network already compiled");
+        need(src_pop < net->net.pops.size() && dst_pop < net->net.pops.size(), NAER_E_INVALID,
+             "unknown population");
+        naer::ConnSpec c;
+        c.src = src_pop;
+        c.dst = dst_pop;
+        c.spec = *spec;
+        net->net.conns.push_back(c);
+    });
+}
+
+int naer_net_compile(naer_net* net) {
+    return guarded([&] {
+        need(net != nullptr, NAER_E_INVALID, "null network handle");
+        need(!net->net.compiled, NAER_E_STATE, "network already compiled");
+        net->eng->build(net->net);
+        const auto& P = net->net.params;
+        net->eng->install({&net->net}, P.raster_capacity, P.record_spikes != 0, P.aggregation);
+    });
+}
+
+int naer_net_population_base(naer_net* net, uint32_t pop_id, uint32_t* base_address) {
+    return guarded([&] {
+        need_compiled(net);
+        need(pop_id < net->net.pops.size() && base_address, NAER_E_INVALID, "bad argument");
+        *base_address = net->net.pops[pop_id].id_base;
+    });
+}
+
+int naer_net_step(naer_net* net, uint64_t nsteps) {
+    return guarded([&] {
+        need_compiled(net);
+        net->eng->run(nsteps);
+    });
+}
+
+int naer_net_finish(naer_net* net) {
+    return guarded([&] {
+        need_compiled(net);
+        net->eng->sync();
+        const naer::Ctl c = net->eng->read_ctl();
+        if (c.error) throw Error(NAER_E_CUDA, "device reported error flag " + std::to_string(c.error));
+    });
+}
+
+int naer_net_get_time_us(naer_net* net, uint64_t* time_us) {
+    return guarded([&] {
+        need(net && time_us, NAER_E_INVALID, "null argument");
+        *time_us = net->eng->host_step() * (uint64_t)net->net.params.dt_us;
+    });
+}
+
+int naer_net_get_synapses(naer_net* net, uint64_t* synapses) {
+    return guarded([&] {
+        need(net && synapses, NAER_E_INVALID, "null argument");
+        *synapses = net->net.synapses;
+    });
+}
+
+int naer_net_get_neurons(naer_net* net, uint32_t* neurons) {
+    return guarded([&] {
+        need(net && neurons, NAER_E_INVALID, "null argument");
+        *neurons = net->type_count[0] + net->type_count[1] + net->type_count[2];
+    });
+}
+
+int naer_net_get_stats(naer_net* net, naer_stats* st) {
+    return guarded([&] {
+        need_compiled(net);
+        need(st != nullptr, NAER_E_INVALID, "null argument");
+        const naer::Ctl c = net->eng->read_ctl();
+        std::memset(st, 0, sizeof(*st));
+        st->step = c.step;
+        st->events = c.events;
+        st->spikes = std::min<uint64_t>(c.raster_count, net->net.params.raster_capacity);
+        st->raster_dropped = c.raster_dropped;
+        st->stdp_hist_overflow = c.stdp_hist_overflow;
+        st->synapses = net->net.synapses;
+        st->device_bytes = net->eng->device_bytes();
+        st->neurons = net->net.n_ids;
+        st->ring_slots = net->net.ring_slots;
+    });
+}
+
+int naer_net_read_spikes(naer_net* net, uint64_t first, uint64_t capacity, uint32_t* steps,
+                         uint32_t* ids, uint64_t* count) {
+    return guarded([&] {
+        need_compiled(net);
+        need(count != nullptr && (capacity == 0 || (steps && ids)), NAER_E_INVALID, "null argument");
+        *count = net->eng->read_raster(first, capacity, steps, ids);
+    });
+}
+
+int naer_net_read_raster(naer_net* net, uint64_t first, uint64_t capacity, uint32_t* records,
+                         uint64_t* count) {
+    return guarded([&] {
+        need_compiled(net);
+        need(count != nullptr && (capacity == 0 || records), NAER_E_INVALID, "null argument");
+        *count = net->eng->read_raster_raw(first, capacity, records);
+    });
+}
+
+int naer_net_stream(naer_net* net, void** stream) {
+    return guarded([&] {
+        need(net != nullptr && stream != nullptr, NAER_E_INVALID, "null argument");
+        *stream = (void*)net->eng->stream();
+    });
+}
+
+int naer_net_clear_spikes(naer_net* net) {
+    return guarded([&] {
+        need_compiled(net);
+        net->eng->clear_raster();
+    });
+}
+
+int naer_net_read_state(naer_net* net, float* v, uint32_t* refractory) {
+    return guarded([&] {
+        need_compiled(net);
+        const auto& n = net->net;
+        std::vector<float> hv(n.n_storage);
+        std::vector<uint8_t> hr(n.n_storage);
+        net->eng->sync();
+        NAER_CK(cudaMemcpy(hv.data(), n.v, n.n_storage * 4ull, cudaMemcpyDeviceToHost));
+        NAER_CK(cudaMemcpy(hr.data(), n.refr, n.n_storage, cudaMemcpyDeviceToHost));
+        for (const auto& p : n.pops) {
+            const bool lif = p.type != naer::kPOISSON;
+            for (uint32_t k = 0; k < p.size; ++k) {
+                if (v) v[p.id_base + k] = lif ? hv[p.storage_base + k] : 0.0f;
+                if (refractory) refractory[p.id_base + k] = lif ? hr[p.storage_base + k] : 0u;
+            }
+        }
+    });
+}
+
+int naer_net_write_state(naer_net* net, const float* v, const uint32_t* refractory) {
+    return guarded([&] {
+        need_compiled(net);
+        const auto& n = net->net;
+        std::vector<float> hv(n.n_storage);
+        std::vector<uint8_t> hr(n.n_storage);
+        net->eng->sync();
+        NAER_CK(cudaMemcpy(hv.data(), n.v, n.n_storage * 4ull, cudaMemcpyDeviceToHost));
+        NAER_CK(cudaMemcpy(hr.data(), n.refr, n.n_storage, cudaMemcpyDeviceToHost));
+        for (const auto& p : n.pops) {
+            if (p.type == naer::kPOISSON) continue;
+            for (uint32_t k = 0; k < p.size; ++k) {
+                if (v) hv[p.storage_base + k] = v[p.id_base + k];
+                if (refractory) {
+                    need(refractory[p.id_base + k] <= 255, NAER_E_INVALID, "refractory count above 255");
+                    hr[p.storage_base + k] = (uint8_t)refractory[p.id_base + k];
+                }
+            }
+        }
+        NAER_CK(cudaMemcpy(n.v, hv.data(), n.n_storage * 4ull, cudaMemcpyHostToDevice));
+        NAER_CK(cudaMemcpy(n.refr, hr.data(), n.n_storage, cudaMemcpyHostToDevice));
+    });
+}
+
+int naer_net_read_csr(naer_net* net, uint64_t* row_ptr, uint32_t* tgt, float* w, uint8_t* delay) {
+    return guarded([&] {
+        need_compiled(net);
+        need(row_ptr != nullptr, NAER_E_INVALID, "null row_ptr");
+        const auto& n = net->net;
+        net->eng->sync();
+        std::vector<uint64_t> rp(n.n_storage + 1);
+        NAER_CK(cudaMemcpy(rp.data(), n.row_ptr, rp.size() * 8ull, cudaMemcpyDeviceToHost));
+        const uint64_t S = n.synapses_padded;
+        std::vector<uint32_t> ht(S);
+        std::vector<float> hw(S);
+        std::vector<uint8_t> hd(S);
+        if (S) {
+            NAER_CK(cudaMemcpy(ht.data(), n.tgt, S * 4ull, cudaMemcpyDeviceToHost));
+            NAER_CK(cudaMemcpy(hw.data(), n.w, S * 4ull, cudaMemcpyDeviceToHost));
+            NAER_CK(cudaMemcpy(hd.data(), n.dly, S, cudaMemcpyDeviceToHost));
+        }
+        uint64_t o = 0;
+        for (uint32_t id = 0; id < n.n_ids; ++id) {
+            row_ptr[id] = o;
+            const uint32_t s = n.storage_of_id[id];
+            for (uint64_t j = rp[s]; j < rp[s + 1]; ++j) {
+                if (ht[j] == naer::kTgtSentinel) continue;
+                if (tgt) tgt[o] = (uint32_t)n.id_of_storage[ht[j]];
+                if (w) w[o] = hw[j];
+                if (delay) delay[o] = hd[j];
+                ++o;
+            }
+        }
+        row_ptr[n.n_ids] = o;
+    });
+}
+
+int naer_net_set_profiling(naer_net* net, int enable) {
+    return guarded([&] {
+        need_compiled(net);
+        net->eng->set_profiling(enable != 0);
+    });
+}
+
+int naer_net_get_profile(naer_net* net, double* lif_ms, double* scatter_ms, uint64_t* launches) {
+    return guarded([&] {
+        need_compiled(net);
+        net->eng->get_profile(lif_ms, scatter_ms, launches);
+    });
+}
+
+}  // extern "C"

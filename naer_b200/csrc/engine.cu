@@ -1,0 +1,797 @@
+// Host engine implementation.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "build_kernels.cuh"
+#include "engine.h"
+#include "philox.cuh"
+#include "sim_kernels.cuh"
+
+namespace naer {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    (void)cudaGetLastError();
+    const int code = e == cudaErrorMemoryAllocation ? NAER_E_OOM : NAER_E_CUDA;
+    throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        NAER_CK(cudaGetDevice(&prev));
+        if (prev != dev) NAER_CK(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+__global__ void k_u32_to_u64(const uint32_t* in, uint32_t n, uint64_t* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x)
+        out[i] = i < n ? (uint64_t)in[i] : 0ull;
+}
+
+uint32_t round_up4(uint32_t x) { return (x + 3u) & ~3u; }
+
+uint32_t bit_width(uint64_t x) {
+    uint32_t b = 0;
+    while (x) {
+        ++b;
+        x >>= 1;
+    }
+    return b;
+}
+
+// Smallest z (plus a safety margin) whose first interval reaches past a
+// window of W µs; 0xFFFFFFFF disables the fast path.
+uint32_t poisson_z_hi(double rate, uint32_t W) {
+    if (!(rate > 0.0)) return 0xFFFFFFFFu;
+    if (ref_exp_interval_us(0xFFFFFFFEu, rate) < W) return 0xFFFFFFFFu;
+    uint64_t lo = 0, hi = 0xFFFFFFFEull;
+    while (hi - lo > 1) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (ref_exp_interval_us((uint32_t)mid, rate) >= W) hi = mid; else lo = mid;
+    }
+    return hi + 16 >= 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)(hi + 16);
+}
+
+uint32_t poisson_t0_limit(double rate) {
+    if (!(rate > 0.0)) return 0;
+    const uint64_t imax = ref_exp_interval_us(0xFFFFFFFEu, rate);
+    if (imax + 2 >= 0xFFFFFFFFull) return 0;
+    return (uint32_t)(0xFFFFFFFFull - (imax + 2));
+}
+
+template <typename F>
+void with_cub_tmp(Engine& eng, F&& f) {
+    size_t bytes = 0;
+    NAER_CK(f(nullptr, bytes));
+    void* tmp = eng.dalloc(bytes ? bytes : 16);
+    try {
+        NAER_CK(f(tmp, bytes));
+    } catch (...) {
+        eng.dfree(tmp, bytes ? bytes : 16);
+        throw;
+    }
+    NAER_CK(cudaStreamSynchronize(eng.stream()));
+    eng.dfree(tmp, bytes ? bytes : 16);
+}
+
+uint32_t grid_for(uint64_t items, uint32_t threads, uint32_t max_blocks) {
+    uint64_t b = (items + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > max_blocks) b = max_blocks;
+    return (uint32_t)b;
+}
+
+}  // namespace
+
+Engine::Engine(int device) : device_(device) {
+    int n = 0;
+    NAER_CK(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) throw Error(NAER_E_INVALID, "device index out of range");
+    NAER_CK(cudaSetDevice(device));
+    NAER_CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device));
+    NAER_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    d_ctl_ = static_cast<Ctl*>(dalloc(sizeof(Ctl)));
+    NAER_CK(cudaMemset(d_ctl_, 0, sizeof(Ctl)));
+    NAER_CK(cudaMallocHost(&h_pinned_, 256));
+}
+
+Engine::~Engine() {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device_);
+    cudaStreamSynchronize(stream_);
+    destroy_graph();
+    for (auto e : event_pool_) cudaEventDestroy(e);
+    for (auto e : prof_events_) cudaEventDestroy(e);
+    auto f = [](void* p) {
+        if (p) cudaFree(p);
+    };
+    f(d_ctl_);
+    f(d_nets_);
+    f(d_pops_);
+    f(d_chunks_);
+    f(d_queue_[0]);
+    f(d_queue_[1]);
+    f(d_raster_);
+    for (int i = 0; i < 2; ++i) {
+        f(q_keys_[i]);
+        f(q_vals_[i]);
+        f(e_keys_[i]);
+        f(e_vals_[i]);
+    }
+    f(q_sizes_);
+    f(q_offs_);
+    f(cub_tmp_);
+    if (h_pinned_) cudaFreeHost(h_pinned_);
+    cudaStreamDestroy(stream_);
+    if (prev >= 0) cudaSetDevice(prev);
+}
+
+void* Engine::dalloc(size_t bytes) {
+    void* p = nullptr;
+    NAER_CK(cudaMalloc(&p, bytes ? bytes : 16));
+    bytes_ += bytes;
+    return p;
+}
+
+void Engine::dfree(void* p, size_t bytes) {
+    if (!p) return;
+    NAER_CK(cudaFree(p));
+    bytes_ -= std::min<uint64_t>(bytes_, bytes);
+}
+
+// ---------------------------------------------------------------------------
+// network build
+
+static void layout(NetHost& n) {
+    const auto& P = n.params;
+    if (P.dt_us == 0) throw Error(NAER_E_INVALID, "dt_us must be positive");
+    uint32_t type_count[3] = {0, 0, 0};
+    for (const auto& p : n.pops) type_count[p.type] += p.size;
+    const uint32_t type_base[3] = {0, type_count[kSTDP], type_count[kSTDP] + type_count[kNOP]};
+    n.n_ids = type_count[0] + type_count[1] + type_count[2];
+    n.n_poisson = type_count[kPOISSON];
+    n.pop_order.clear();
+    for (uint32_t t = 0; t < 3; ++t)
+        for (uint32_t i = 0; i < n.pops.size(); ++i)
+            if (n.pops[i].type == t) n.pop_order.push_back(i);
+    uint32_t s = 0;
+    n.n_plastic = 0;
+    for (uint32_t i : n.pop_order) {
+        auto& p = n.pops[i];
+        p.id_base = type_base[p.type] + p.type_address;
+        p.storage_base = s;
+        s += round_up4(p.size);
+        if (p.type == kSTDP) n.n_plastic = s;
+    }
+    n.n_storage = std::max<uint32_t>(s, 4);
+    n.id_of_storage.assign(n.n_storage, -1);
+    n.storage_of_id.assign(n.n_ids, 0);
+    for (const auto& p : n.pops)
+        for (uint32_t k = 0; k < p.size; ++k) {
+            n.id_of_storage[p.storage_base + k] = (int32_t)(p.id_base + k);
+            n.storage_of_id[p.id_base + k] = p.storage_base + k;
+        }
+    uint32_t dmax = 1;
+    for (const auto& c : n.conns) {
+        const auto& sp = c.spec;
+        if (c.src >= n.pops.size() || c.dst >= n.pops.size())
+            throw Error(NAER_E_INVALID, "connection refers to an unknown population");
+        if (n.pops[c.dst].type == kPOISSON)
+            throw Error(NAER_E_INVALID, "POISSON populations cannot receive connections");
+        if (sp.rule > NAER_CONN_FIXED_OUTDEGREE) throw Error(NAER_E_INVALID, "unknown connection rule");
+        if (sp.delay_min < 1 || sp.delay_max < sp.delay_min || sp.delay_max > 254)
+            throw Error(NAER_E_INVALID, "delays must satisfy 1 <= delay_min <= delay_max <= 254");
+        if (sp.rule == NAER_CONN_REF_BERNOULLI && !(sp.probability >= 0.0 && sp.probability <= 1.0))
+            throw Error(NAER_E_INVALID, "probability must be in [0, 1]");
+        dmax = std::max(dmax, sp.delay_max);
+    }
+    n.ring_slots = dmax + 1;
+    for (const auto& p : n.pops) {
+        if (p.type == kPOISSON) continue;
+        const double tr = std::llround((double)p.prm.t_ref_ms * 1000.0 / P.dt_us);
+        if (tr < 0 || tr > 255) throw Error(NAER_E_INVALID, "refractory period must be 0..255 steps");
+        if (!(p.prm.tau_m_ms > 0.0f)) throw Error(NAER_E_INVALID, "tau_m_ms must be positive");
+    }
+    if (P.stdp_enabled && P.stdp_history == 0)
+        throw Error(NAER_E_INVALID, "stdp_history must be at least 1");
+}
+
+static ConnBuild make_cb(const NetHost& n, const ConnSpec& c) {
+    ConnBuild cb{};
+    const auto& s = c.spec;
+    cb.rule = s.rule;
+    cb.K = s.degree;
+    cb.p = s.probability;
+    cb.weight = s.weight;
+    cb.wmin = s.wmin;
+    cb.wmax = s.wmax;
+    cb.dmin = s.delay_min;
+    cb.dmax = s.delay_max;
+    cb.seed_lo = (uint32_t)s.seed;
+    cb.seed_hi = (uint32_t)(s.seed >> 32);
+    cb.src_size = n.pops[c.src].size;
+    cb.dst_size = n.pops[c.dst].size;
+    cb.src_storage = n.pops[c.src].storage_base;
+    cb.dst_storage = n.pops[c.dst].storage_base;
+    return cb;
+}
+
+void Engine::build(NetHost& n) {
+    DeviceGuard g(device_);
+    layout(n);
+    const uint32_t Ns = n.n_storage;
+    const uint32_t T = 256;
+    const uint32_t maxb = (uint32_t)sm_count_ * 16;
+    cudaStream_t st = stream_;
+    const uint64_t bytes0 = bytes_;
+
+    // --- connectivity: counts per (connection, source)
+    uint64_t* len = static_cast<uint64_t*>(dalloc(Ns * 8ull));
+    NAER_CK(cudaMemsetAsync(len, 0, Ns * 8ull, st));
+    std::vector<uint32_t*> cnt(n.conns.size(), nullptr);
+    for (size_t ci = 0; ci < n.conns.size(); ++ci) {
+        const ConnBuild cb = make_cb(n, n.conns[ci]);
+        cnt[ci] = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(cb.src_size, 1) * 4ull));
+        NAER_CK(cudaMemsetAsync(cnt[ci], 0, std::max<uint64_t>(cb.src_size, 1) * 4ull, st));
+        if (cb.src_size == 0 || cb.dst_size == 0) continue;
+        if (cb.rule == NAER_CONN_REF_BERNOULLI) {
+            k_bern_count<<<grid_for((uint64_t)cb.src_size * 32, T, maxb), T, 0, st>>>(cb, cnt[ci]);
+        } else if (cb.rule == NAER_CONN_FIXED_OUTDEGREE) {
+            k_fill_u32<<<grid_for(cb.src_size, T, maxb), T, 0, st>>>(cnt[ci], cb.src_size, cb.K);
+        } else {
+            const uint64_t items = (uint64_t)cb.dst_size * ((cb.K + 3) / 4);
+            if (items) k_indeg_count<<<grid_for(items, T, maxb), T, 0, st>>>(cb, cnt[ci]);
+        }
+        k_row_len_add<<<grid_for(cb.src_size, T, maxb), T, 0, st>>>(cnt[ci], cb.src_size,
+                                                                    cb.src_storage, len);
+        NAER_CK(cudaGetLastError());
+    }
+    uint64_t* padded = static_cast<uint64_t*>(dalloc((Ns + 1) * 8ull));
+    k_row_pad<<<grid_for(Ns + 1, T, maxb), T, 0, st>>>(len, Ns, padded);
+    n.row_ptr = static_cast<uint64_t*>(dalloc((Ns + 1) * 8ull));
+    with_cub_tmp(*this, [&](void* tmp, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(tmp, b, padded, n.row_ptr, (int)(Ns + 1), st);
+    });
+    NAER_CK(cudaMemcpyAsync(&n.synapses_padded, n.row_ptr + Ns, 8, cudaMemcpyDeviceToHost, st));
+    NAER_CK(cudaStreamSynchronize(st));
+    const uint64_t S = n.synapses_padded;
+    n.tgt = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(S, 4) * 4ull));
+    n.w = static_cast<float*>(dalloc(std::max<uint64_t>(S, 4) * 4ull));
+    n.dly = static_cast<uint8_t*>(dalloc(std::max<uint64_t>(S, 16)));
+    uint64_t* cursor = static_cast<uint64_t*>(dalloc(Ns * 8ull));
+    NAER_CK(cudaMemcpyAsync(cursor, n.row_ptr, Ns * 8ull, cudaMemcpyDeviceToDevice, st));
+
+    // --- fill rows, connection by connection
+    for (size_t ci = 0; ci < n.conns.size(); ++ci) {
+        const ConnBuild cb = make_cb(n, n.conns[ci]);
+        if (cb.src_size == 0 || cb.dst_size == 0) continue;
+        if (cb.rule == NAER_CONN_REF_BERNOULLI) {
+            k_bern_fill<<<grid_for((uint64_t)cb.src_size * 32, T, maxb), T, 0, st>>>(cb, cursor, n.tgt,
+                                                                                     n.w, n.dly);
+        } else if (cb.rule == NAER_CONN_FIXED_OUTDEGREE) {
+            const uint64_t items = (uint64_t)cb.src_size * ((cb.K + 3) / 4);
+            if (items)
+                k_outdeg_fill<<<grid_for(items, T, maxb), T, 0, st>>>(cb, cursor, n.tgt, n.w, n.dly);
+        } else if (cb.K > 0) {
+            uint64_t* off = static_cast<uint64_t*>(dalloc((cb.src_size + 1) * 8ull));
+            uint64_t* cnt64 = static_cast<uint64_t*>(dalloc((cb.src_size + 1) * 8ull));
+            k_u32_to_u64<<<grid_for(cb.src_size + 1, T, maxb), T, 0, st>>>(cnt[ci], cb.src_size, cnt64);
+            with_cub_tmp(*this, [&](void* tmp, size_t& b) {
+                return cub::DeviceScan::ExclusiveSum(tmp, b, cnt64, off, (int)(cb.src_size + 1), st);
+            });
+            uint64_t total = 0;
+            NAER_CK(cudaMemcpyAsync(&total, off + cb.src_size, 8, cudaMemcpyDeviceToHost, st));
+            NAER_CK(cudaStreamSynchronize(st));
+            if (total > 0x7FFFFFFFull)
+                throw Error(NAER_E_OVERFLOW, "a FIXED_INDEGREE connection exceeds 2^31 synapses");
+            unsigned long long* ccur = reinterpret_cast<unsigned long long*>(cnt64);
+            NAER_CK(cudaMemcpyAsync(ccur, off, cb.src_size * 8ull, cudaMemcpyDeviceToDevice, st));
+            auto* kin = static_cast<unsigned long long*>(dalloc(std::max<uint64_t>(total, 1) * 8ull));
+            auto* kout = static_cast<unsigned long long*>(dalloc(std::max<uint64_t>(total, 1) * 8ull));
+            const uint64_t items = (uint64_t)cb.dst_size * ((cb.K + 3) / 4);
+            k_indeg_fill<<<grid_for(items, T, maxb), T, 0, st>>>(cb, ccur, kin);
+            NAER_CK(cudaGetLastError());
+            with_cub_tmp(*this, [&](void* tmp, size_t& b) {
+                return cub::DeviceSegmentedSort::SortKeys(tmp, b, kin, kout, (int)total, (int)cb.src_size,
+                                                          off, off + 1, st);
+            });
+            k_indeg_finalize<<<grid_for(total, T, maxb), T, 0, st>>>(cb, kout, total, off, cursor, n.tgt,
+                                                                     n.w, n.dly);
+            NAER_CK(cudaGetLastError());
+            NAER_CK(cudaStreamSynchronize(st));
+            dfree(kin, std::max<uint64_t>(total, 1) * 8ull);
+            dfree(kout, std::max<uint64_t>(total, 1) * 8ull);
+            dfree(off, (cb.src_size + 1) * 8ull);
+            dfree(cnt64, (cb.src_size + 1) * 8ull);
+        }
+        k_cursor_advance<<<grid_for(cb.src_size, T, maxb), T, 0, st>>>(cnt[ci], cb.src_size,
+                                                                       cb.src_storage, cursor);
+        NAER_CK(cudaGetLastError());
+    }
+    k_pad_fill<<<grid_for(Ns, T, maxb), T, 0, st>>>(n.row_ptr, len, Ns, n.tgt, n.w, n.dly);
+    NAER_CK(cudaGetLastError());
+    std::vector<uint64_t> hlen(Ns);
+    NAER_CK(cudaMemcpyAsync(hlen.data(), len, Ns * 8ull, cudaMemcpyDeviceToHost, st));
+    NAER_CK(cudaStreamSynchronize(st));
+    n.synapses = 0;
+    for (uint64_t x : hlen) n.synapses += x;
+    for (size_t ci = 0; ci < cnt.size(); ++ci)
+        dfree(cnt[ci], std::max<uint64_t>(n.pops[n.conns[ci].src].size, 1) * 4ull);
+    dfree(len, Ns * 8ull);
+    dfree(padded, (Ns + 1) * 8ull);
+    dfree(cursor, Ns * 8ull);
+
+    // --- neuron state
+    n.v = static_cast<float*>(dalloc(Ns * 4ull));
+    n.refr = static_cast<uint8_t*>(dalloc(Ns));
+    n.ring = static_cast<float*>(dalloc((uint64_t)n.ring_slots * Ns * 4ull));
+    std::vector<float> v0(Ns, 0.0f);
+    for (const auto& p : n.pops)
+        if (p.type != kPOISSON)
+            for (uint32_t k = 0; k < p.size; ++k) v0[p.storage_base + k] = p.prm.v_init;
+    NAER_CK(cudaMemcpyAsync(n.v, v0.data(), Ns * 4ull, cudaMemcpyHostToDevice, st));
+    NAER_CK(cudaMemsetAsync(n.refr, 0, Ns, st));
+    NAER_CK(cudaMemsetAsync(n.ring, 0, (uint64_t)n.ring_slots * Ns * 4ull, st));
+
+    const auto& P = n.params;
+    const bool stdp = P.stdp_enabled && n.n_plastic > 0;
+    if (stdp) {
+        const uint32_t Np = n.n_plastic, K = P.stdp_history;
+        n.last_post = static_cast<int32_t*>(dalloc(Np * 4ull));
+        n.y_post = static_cast<float*>(dalloc(Np * 4ull));
+        n.hist = static_cast<int32_t*>(dalloc((uint64_t)Np * K * 4ull));
+        n.last_pre = static_cast<int32_t*>(dalloc(Np * 4ull));
+        n.x_pre = static_cast<float*>(dalloc(Np * 4ull));
+        NAER_CK(cudaMemsetAsync(n.last_post, 0xFF, Np * 4ull, st));
+        NAER_CK(cudaMemsetAsync(n.y_post, 0, Np * 4ull, st));
+        NAER_CK(cudaMemsetAsync(n.hist, 0xFF, (uint64_t)Np * K * 4ull, st));
+        NAER_CK(cudaMemsetAsync(n.last_pre, 0xFF, Np * 4ull, st));
+        NAER_CK(cudaMemsetAsync(n.x_pre, 0, Np * 4ull, st));
+        // exp(-k dt / tau) as float until it underflows (k dt / tau > 104)
+        const double tmax = std::max((double)P.tau_plus_ms, (double)P.tau_minus_ms) * 1000.0;
+        n.e_len = (uint32_t)std::min<double>(std::ceil(104.0 * tmax / P.dt_us) + 1.0, 1 << 24);
+        std::vector<float> ep(n.e_len), em(n.e_len);
+        for (uint32_t k = 0; k < n.e_len; ++k) {
+            ep[k] = (float)std::exp(-(double)k * P.dt_us / ((double)P.tau_plus_ms * 1000.0));
+            em[k] = (float)std::exp(-(double)k * P.dt_us / ((double)P.tau_minus_ms * 1000.0));
+        }
+        n.e_plus = static_cast<float*>(dalloc(n.e_len * 4ull));
+        n.e_minus = static_cast<float*>(dalloc(n.e_len * 4ull));
+        NAER_CK(cudaMemcpyAsync(n.e_plus, ep.data(), n.e_len * 4ull, cudaMemcpyHostToDevice, st));
+        NAER_CK(cudaMemcpyAsync(n.e_minus, em.data(), n.e_len * 4ull, cudaMemcpyHostToDevice, st));
+    }
+    NAER_CK(cudaStreamSynchronize(st));
+
+    NetDev& d = n.dev;
+    d = NetDev{};
+    d.v = n.v;
+    d.refr = n.refr;
+    d.ring = n.ring;
+    d.row_ptr = n.row_ptr;
+    d.tgt = n.tgt;
+    d.w = n.w;
+    d.dly = n.dly;
+    d.last_post = n.last_post;
+    d.y_post = n.y_post;
+    d.hist = n.hist;
+    d.last_pre = n.last_pre;
+    d.x_pre = n.x_pre;
+    d.e_plus = n.e_plus;
+    d.e_minus = n.e_minus;
+    d.start_step = 0;
+    d.n_storage = Ns;
+    d.ring_slots = n.ring_slots;
+    d.dt_us = P.dt_us;
+    d.n_plastic = stdp ? n.n_plastic : 0;
+    d.stdp_on = stdp ? 1u : 0u;
+    d.hist_len = P.stdp_history;
+    d.e_len = n.e_len;
+    d.a_plus = P.a_plus * P.w_max;
+    d.a_minus = P.a_minus * P.w_max;
+    d.w_max = P.w_max;
+    d.active = 1;
+    n.device_bytes = bytes_ - bytes0;
+    n.compiled = true;
+}
+
+void Engine::free_net(NetHost& n) {
+    DeviceGuard g(device_);
+    const uint32_t Ns = n.n_storage;
+    const uint64_t S = n.synapses_padded;
+    dfree(n.v, Ns * 4ull);
+    dfree(n.refr, Ns);
+    dfree(n.ring, (uint64_t)n.ring_slots * Ns * 4ull);
+    dfree(n.row_ptr, (Ns + 1) * 8ull);
+    dfree(n.tgt, std::max<uint64_t>(S, 4) * 4ull);
+    dfree(n.w, std::max<uint64_t>(S, 4) * 4ull);
+    dfree(n.dly, std::max<uint64_t>(S, 16));
+    const uint32_t Np = n.n_plastic, K = n.params.stdp_history;
+    dfree(n.last_post, Np * 4ull);
+    dfree(n.y_post, Np * 4ull);
+    dfree(n.hist, (uint64_t)Np * K * 4ull);
+    dfree(n.last_pre, Np * 4ull);
+    dfree(n.x_pre, Np * 4ull);
+    dfree(n.e_plus, n.e_len * 4ull);
+    dfree(n.e_minus, n.e_len * 4ull);
+    n.v = nullptr;
+    n.refr = nullptr;
+    n.ring = nullptr;
+    n.row_ptr = nullptr;
+    n.tgt = nullptr;
+    n.w = nullptr;
+    n.dly = nullptr;
+    n.last_post = n.last_pre = n.hist = nullptr;
+    n.y_post = n.x_pre = n.e_plus = n.e_minus = nullptr;
+    n.compiled = false;
+}
+
+// ---------------------------------------------------------------------------
+// descriptor tables
+
+void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity, bool record,
+                     uint32_t aggregation) {
+    DeviceGuard g(device_);
+    NAER_CK(cudaStreamSynchronize(stream_));
+    destroy_graph();
+    nets_ = nets;
+    aggregation_ = aggregation;
+    std::vector<PopDev> pops;
+    std::vector<ChunkDev> chunks;
+    h_nets_.clear();
+    uint64_t key_base = 0;
+    uint64_t qcap = 0;
+    for (uint32_t ni = 0; ni < nets.size(); ++ni) {
+        NetHost& n = *nets[ni];
+        NetDev d = n.dev;
+        d.ring_key_base = key_base;
+        key_base += (uint64_t)n.ring_slots * n.n_storage;
+        h_nets_.push_back(d);
+        qcap += n.n_storage;
+        const auto& P = n.params;
+        for (uint32_t pi : n.pop_order) {
+            const PopSpec& ps = n.pops[pi];
+            if (ps.size == 0) continue;
+            PopDev pd{};
+            pd.net = ni;
+            pd.type = ps.type;
+            pd.storage_base = ps.storage_base;
+            pd.size = ps.size;
+            pd.id_base = ps.id_base;
+            if (ps.type == kPOISSON) {
+                pd.rate_hz = (double)ps.prm.rate_hz;
+                pd.rng_seed = P.poisson_seed;
+                pd.rng_n = n.n_poisson;
+                pd.rng_idx_base = ps.type_address;
+            } else {
+                pd.t_ref_steps = (uint32_t)std::llround((double)ps.prm.t_ref_ms * 1000.0 / P.dt_us);
+                pd.v_th = ps.prm.v_th;
+                pd.v_reset = ps.prm.v_reset;
+                pd.prop = std::exp(-(double)P.dt_us / ((double)ps.prm.tau_m_ms * 1000.0));
+                pd.rate_hz = (double)ps.prm.drive_rate_hz;
+                pd.drive_w = ps.prm.drive_weight;
+                pd.rng_seed = ps.prm.drive_seed;
+                pd.rng_n = ps.size;
+                pd.rng_idx_base = 0;
+            }
+            pd.z_hi = poisson_z_hi(pd.rate_hz, P.dt_us);
+            pd.t0_limit = poisson_t0_limit(pd.rate_hz);
+            const uint32_t pidx = (uint32_t)pops.size();
+            pops.push_back(pd);
+            for (uint32_t f = ps.storage_base; f < ps.storage_base + ps.size; f += kLifChunk)
+                chunks.push_back(ChunkDev{pidx, f, ps.storage_base + ps.size, 0});
+        }
+    }
+    total_ring_cells_ = key_base;
+    if (qcap > 0xFFFFFFFFull) throw Error(NAER_E_OVERFLOW, "more than 2^32 neurons in one engine");
+
+    auto upload = [&](void*& dst, size_t& cap_bytes, const void* src, size_t bytes) {
+        if (bytes > cap_bytes) {
+            if (dst) dfree(dst, cap_bytes);
+            dst = dalloc(bytes);
+            cap_bytes = bytes;
+        }
+        if (bytes) NAER_CK(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    };
+    void* p = d_nets_;
+    upload(p, nets_bytes_, h_nets_.data(), h_nets_.size() * sizeof(NetDev));
+    d_nets_ = static_cast<NetDev*>(p);
+    p = d_pops_;
+    upload(p, pops_bytes_, pops.data(), pops.size() * sizeof(PopDev));
+    d_pops_ = static_cast<PopDev*>(p);
+    p = d_chunks_;
+    upload(p, chunks_bytes_, chunks.data(), chunks.size() * sizeof(ChunkDev));
+    d_chunks_ = static_cast<ChunkDev*>(p);
+
+    const size_t qbytes = std::max<uint64_t>(qcap, 1) * sizeof(SpikeRec);
+    if (qbytes > queue_bytes_) {
+        for (int i = 0; i < 2; ++i) {
+            if (d_queue_[i]) dfree(d_queue_[i], queue_bytes_);
+            d_queue_[i] = static_cast<SpikeRec*>(dalloc(qbytes));
+        }
+        queue_bytes_ = qbytes;
+    }
+    queue_cap_ = (uint32_t)qcap;
+    const size_t rbytes = std::max<uint64_t>(raster_capacity, 1) * sizeof(uint2);
+    if (rbytes != raster_bytes_) {
+        if (d_raster_) dfree(d_raster_, raster_bytes_);
+        d_raster_ = static_cast<uint2*>(dalloc(rbytes));
+        raster_bytes_ = rbytes;
+    }
+
+    eng_ = EngineDev{};
+    eng_.ctl = d_ctl_;
+    eng_.nets = d_nets_;
+    eng_.pops = d_pops_;
+    eng_.chunks = d_chunks_;
+    eng_.queue[0] = d_queue_[0];
+    eng_.queue[1] = d_queue_[1];
+    eng_.raster = d_raster_;
+    eng_.raster_cap = raster_capacity;
+    eng_.n_chunks = (uint32_t)chunks.size();
+    eng_.n_nets = (uint32_t)nets.size();
+    eng_.record = record ? 1u : 0u;
+    lif_grid_ = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 8));
+    scatter_grid_ = (uint32_t)sm_count_ * 4;
+}
+
+// ---------------------------------------------------------------------------
+// step loop
+
+void Engine::launch_step_atomic() {
+    k_lif<<<lif_grid_, kLifThreads, 0, stream_>>>(eng_);
+    k_scatter_atomic<<<scatter_grid_, kScatterThreads, 0, stream_>>>(eng_);
+}
+
+void Engine::destroy_graph() {
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+        graph_steps_ = 0;
+    }
+}
+
+void Engine::capture_graph(uint32_t steps) {
+    destroy_graph();
+    cudaGraph_t graph = nullptr;
+    NAER_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    for (uint32_t i = 0; i < steps; ++i) launch_step_atomic();
+    NAER_CK(cudaStreamEndCapture(stream_, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&graph_exec_, graph, 0);
+    cudaGraphDestroy(graph);
+    NAER_CK(e);
+    graph_steps_ = steps;
+}
+
+cudaEvent_t Engine::next_event() {
+    cudaEvent_t e;
+    if (!event_pool_.empty()) {
+        e = event_pool_.back();
+        event_pool_.pop_back();
+    } else {
+        NAER_CK(cudaEventCreate(&e));
+    }
+    prof_events_.push_back(e);
+    return e;
+}
+
+void Engine::resolve_profile() {
+    if (prof_events_.empty()) return;
+    NAER_CK(cudaStreamSynchronize(stream_));
+    // events come in groups of four: lif start/end, scatter start/end
+    for (size_t i = 0; i + 3 < prof_events_.size(); i += 4) {
+        float a = 0, b = 0;
+        NAER_CK(cudaEventElapsedTime(&a, prof_events_[i], prof_events_[i + 1]));
+        NAER_CK(cudaEventElapsedTime(&b, prof_events_[i + 2], prof_events_[i + 3]));
+        prof_lif_ms_ += a;
+        prof_scatter_ms_ += b;
+        ++prof_launches_;
+    }
+    for (auto e : prof_events_) event_pool_.push_back(e);
+    prof_events_.clear();
+}
+
+void Engine::run(uint64_t nsteps) {
+    DeviceGuard g(device_);
+    if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
+    if (aggregation_ == NAER_AGG_DETERMINISTIC) {
+        for (uint64_t i = 0; i < nsteps; ++i) run_deterministic_step();
+        return;
+    }
+    if (profiling_) {
+        for (uint64_t i = 0; i < nsteps; ++i) {
+            NAER_CK(cudaEventRecord(next_event(), stream_));
+            k_lif<<<lif_grid_, kLifThreads, 0, stream_>>>(eng_);
+            NAER_CK(cudaEventRecord(next_event(), stream_));
+            NAER_CK(cudaEventRecord(next_event(), stream_));
+            k_scatter_atomic<<<scatter_grid_, kScatterThreads, 0, stream_>>>(eng_);
+            NAER_CK(cudaEventRecord(next_event(), stream_));
+            ++host_step_;
+            if (prof_events_.size() >= 4096) resolve_profile();
+        }
+        NAER_CK(cudaGetLastError());
+        return;
+    }
+    const uint32_t G = 64;
+    uint64_t left = nsteps;
+    if (left >= G) {
+        if (graph_steps_ != G) capture_graph(G);
+        while (left >= G) {
+            NAER_CK(cudaGraphLaunch(graph_exec_, stream_));
+            left -= G;
+            host_step_ += G;
+        }
+    }
+    for (; left > 0; --left) {
+        launch_step_atomic();
+        ++host_step_;
+    }
+    NAER_CK(cudaGetLastError());
+}
+
+void Engine::ensure_det_capacity(uint64_t events) {
+    if (events <= e_cap_ && q_keys_[0]) return;
+    uint64_t cap = std::max<uint64_t>(events, 1 << 16);
+    if (cap < e_cap_ * 2 && e_cap_) cap = e_cap_ * 2;
+    for (int i = 0; i < 2; ++i) {
+        if (e_keys_[i]) dfree(e_keys_[i], e_cap_ * 8ull);
+        if (e_vals_[i]) dfree(e_vals_[i], e_cap_ * 4ull);
+        e_keys_[i] = static_cast<unsigned long long*>(dalloc(cap * 8ull));
+        e_vals_[i] = static_cast<float*>(dalloc(cap * 4ull));
+    }
+    e_cap_ = cap;
+    if (!q_keys_[0]) {
+        const uint64_t q = std::max<uint32_t>(queue_cap_, 1);
+        for (int i = 0; i < 2; ++i) {
+            q_keys_[i] = static_cast<unsigned long long*>(dalloc(q * 8ull));
+            q_vals_[i] = static_cast<uint32_t*>(dalloc(q * 4ull));
+        }
+        q_sizes_ = static_cast<uint32_t*>(dalloc(q * 4ull));
+        q_offs_ = static_cast<uint32_t*>(dalloc(q * 4ull));
+    }
+    // CUB scratch large enough for every sort/scan of this capacity
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    const int qn = (int)std::max<uint32_t>(queue_cap_, 1);
+    NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b1, q_keys_[0], q_keys_[1], q_vals_[0], q_vals_[1],
+                                            qn, 0, 64, stream_));
+    NAER_CK(cub::DeviceScan::ExclusiveSum(nullptr, b2, q_sizes_, q_offs_, qn, stream_));
+    NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b3, e_keys_[0], e_keys_[1], e_vals_[0], e_vals_[1],
+                                            (int)std::min<uint64_t>(cap, 0x7FFFFFFF), 0, 64, stream_));
+    const size_t need = std::max({b1, b2, b3});
+    if (need > cub_tmp_bytes_) {
+        if (cub_tmp_) dfree(cub_tmp_, cub_tmp_bytes_);
+        cub_tmp_ = dalloc(need);
+        cub_tmp_bytes_ = need;
+    }
+}
+
+void Engine::run_deterministic_step() {
+    cudaStream_t st = stream_;
+    if (!q_keys_[0]) ensure_det_capacity(1);
+    k_lif<<<lif_grid_, kLifThreads, 0, st>>>(eng_);
+    const uint32_t qb = (uint32_t)(host_step_ & 1ull);
+    NAER_CK(cudaMemcpyAsync(h_pinned_, &d_ctl_->q_count[qb], 4, cudaMemcpyDeviceToHost, st));
+    NAER_CK(cudaStreamSynchronize(st));
+    const uint32_t Q = h_pinned_[0];
+    if (Q > 0) {
+        const uint32_t T = 256;
+        k_det_queue_keys<<<(Q + T - 1) / T, T, 0, st>>>(eng_, qb, q_keys_[0], q_vals_[0], Q);
+        size_t b = cub_tmp_bytes_;
+        const int qbits = 32 + (int)bit_width(std::max<uint32_t>(eng_.n_nets, 1));
+        NAER_CK(cub::DeviceRadixSort::SortPairs(cub_tmp_, b, q_keys_[0], q_keys_[1], q_vals_[0], q_vals_[1],
+                                                (int)Q, 0, std::min(qbits, 64), st));
+        k_det_row_sizes<<<(Q + T - 1) / T, T, 0, st>>>(eng_, qb, q_vals_[1], Q, q_sizes_);
+        b = cub_tmp_bytes_;
+        NAER_CK(cub::DeviceScan::ExclusiveSum(cub_tmp_, b, q_sizes_, q_offs_, (int)Q, st));
+        NAER_CK(cudaMemcpyAsync(h_pinned_, q_offs_ + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
+        NAER_CK(cudaMemcpyAsync(h_pinned_ + 1, q_sizes_ + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
+        NAER_CK(cudaStreamSynchronize(st));
+        const uint64_t E = (uint64_t)h_pinned_[0] + h_pinned_[1];
+        if (E > 0x7FFFFFFFull) throw Error(NAER_E_OVERFLOW, "more than 2^31 events in one step");
+        if (E > 0) {
+            ensure_det_capacity(E);
+            k_det_emit<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + 7) / 8, (uint32_t)sm_count_ * 8)),
+                         kScatterThreads, 0, st>>>(eng_, qb, q_vals_[1], Q, q_offs_, e_keys_[0],
+                                                   e_vals_[0]);
+            b = cub_tmp_bytes_;
+            const int ebits = std::max<int>(1, (int)bit_width(total_ring_cells_));
+            NAER_CK(cub::DeviceRadixSort::SortPairs(cub_tmp_, b, e_keys_[0], e_keys_[1], e_vals_[0],
+                                                    e_vals_[1], (int)E, 0, ebits, st));
+            k_det_fold<<<(uint32_t)((E + T - 1) / T), T, 0, st>>>(d_nets_, eng_.n_nets, e_keys_[1],
+                                                                  e_vals_[1], (uint32_t)E);
+        }
+    }
+    k_advance<<<1, 32, 0, st>>>(eng_);
+    NAER_CK(cudaGetLastError());
+    ++host_step_;
+}
+
+void Engine::sync() {
+    DeviceGuard g(device_);
+    NAER_CK(cudaStreamSynchronize(stream_));
+    NAER_CK(cudaGetLastError());
+}
+
+Ctl Engine::read_ctl() {
+    DeviceGuard g(device_);
+    Ctl c;
+    NAER_CK(cudaMemcpyAsync(h_pinned_, d_ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, stream_));
+    NAER_CK(cudaStreamSynchronize(stream_));
+    std::memcpy(&c, h_pinned_, sizeof(Ctl));
+    return c;
+}
+
+uint64_t Engine::read_raster(uint64_t first, uint64_t cap, uint32_t* steps, uint32_t* ids) {
+    const Ctl c = read_ctl();
+    const uint64_t total = std::min<uint64_t>(c.raster_count, eng_.raster_cap);
+    if (first >= total || cap == 0) return 0;
+    const uint64_t n = std::min<uint64_t>(cap, total - first);
+    std::vector<uint2> rec(n);
+    DeviceGuard g(device_);
+    NAER_CK(cudaMemcpyAsync(rec.data(), d_raster_ + first, n * sizeof(uint2), cudaMemcpyDeviceToHost,
+                            stream_));
+    NAER_CK(cudaStreamSynchronize(stream_));
+    // records of one step are contiguous; order them by address
+    uint64_t a = 0;
+    while (a < n) {
+        uint64_t b = a + 1;
+        while (b < n && rec[b].x == rec[a].x) ++b;
+        std::sort(rec.begin() + a, rec.begin() + b,
+                  [](const uint2& l, const uint2& r) { return l.y < r.y; });
+        a = b;
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        steps[i] = rec[i].x;
+        ids[i] = rec[i].y;
+    }
+    return n;
+}
+
+uint64_t Engine::read_raster_raw(uint64_t first, uint64_t cap, uint32_t* records) {
+    const Ctl c = read_ctl();
+    const uint64_t total = std::min<uint64_t>(c.raster_count, eng_.raster_cap);
+    if (first >= total || cap == 0) return 0;
+    const uint64_t n = std::min<uint64_t>(cap, total - first);
+    DeviceGuard g(device_);
+    NAER_CK(cudaMemcpyAsync(records, d_raster_ + first, n * sizeof(uint2), cudaMemcpyDeviceToHost, stream_));
+    NAER_CK(cudaStreamSynchronize(stream_));
+    return n;
+}
+
+void Engine::clear_raster() {
+    DeviceGuard g(device_);
+    NAER_CK(cudaStreamSynchronize(stream_));
+    const unsigned long long z[2] = {0, 0};
+    NAER_CK(cudaMemcpy(&d_ctl_->raster_count, z, 8, cudaMemcpyHostToDevice));
+    NAER_CK(cudaMemcpy(&d_ctl_->raster_dropped, z, 8, cudaMemcpyHostToDevice));
+}
+
+void Engine::set_profiling(bool on) {
+    DeviceGuard g(device_);
+    if (!on) resolve_profile();
+    profiling_ = on;
+    if (on) {
+        prof_lif_ms_ = prof_scatter_ms_ = 0;
+        prof_launches_ = 0;
+    }
+}
+
+void Engine::get_profile(double* lif_ms, double* scatter_ms, uint64_t* launches) {
+    DeviceGuard g(device_);
+    resolve_profile();
+    if (lif_ms) *lif_ms = prof_lif_ms_;
+    if (scatter_ms) *scatter_ms = prof_scatter_ms_;
+    if (launches) *launches = prof_launches_;
+}
+
+}  // namespace naer

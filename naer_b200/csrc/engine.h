@@ -1,0 +1,163 @@
+// Host engine: owns device memory, builds networks, runs the step loop.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/naer/naer_capi.h"
+#include "engine_types.cuh"
+
+namespace naer {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+#define NAER_CK(x) ::naer::cuda_check((x), #x)
+
+struct PopSpec {
+    uint32_t type = kNOP;
+    uint32_t size = 0;
+    naer_pop_params prm{};
+    uint32_t type_address = 0;  // address within its neuron type (before compile)
+    // after layout
+    uint32_t id_base = 0;       // reference address (net-local)
+    uint32_t storage_base = 0;
+};
+
+struct ConnSpec {
+    uint32_t src = 0, dst = 0;
+    naer_conn_spec spec{};
+};
+
+// One network: description, layout and device arrays.
+struct NetHost {
+    naer_net_params params{};
+    std::vector<PopSpec> pops;
+    std::vector<ConnSpec> conns;
+    bool compiled = false;
+
+    // layout
+    std::vector<uint32_t> pop_order;   // pops in type order
+    uint32_t n_ids = 0, n_storage = 0, n_plastic = 0, ring_slots = 0;
+    uint32_t n_poisson = 0;
+    uint64_t synapses = 0, synapses_padded = 0;
+    std::vector<int32_t> id_of_storage;   // -1 for padding
+    std::vector<uint32_t> storage_of_id;
+
+    // device arrays (owned)
+    float* v = nullptr;
+    uint8_t* refr = nullptr;
+    float* ring = nullptr;
+    uint64_t* row_ptr = nullptr;
+    uint32_t* tgt = nullptr;
+    float* w = nullptr;
+    uint8_t* dly = nullptr;
+    int32_t* last_post = nullptr;
+    float* y_post = nullptr;
+    int32_t* hist = nullptr;
+    int32_t* last_pre = nullptr;
+    float* x_pre = nullptr;
+    float* e_plus = nullptr;
+    float* e_minus = nullptr;
+    uint32_t e_len = 0;
+    uint64_t device_bytes = 0;
+
+    NetDev dev{};
+};
+
+class Engine {
+public:
+    explicit Engine(int device);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+
+    // Lays out and builds a network on the device (connectivity included).
+    void build(NetHost& net);
+    void free_net(NetHost& net);
+    // Installs the nets' descriptor tables; nets must outlive the engine use.
+    void install(const std::vector<NetHost*>& nets, uint64_t raster_capacity, bool record,
+                 uint32_t aggregation);
+
+    void run(uint64_t nsteps);
+    void sync();
+    Ctl read_ctl();
+    uint64_t host_step() const { return host_step_; }
+
+    // raster records [first, first+cap) -> (step, id); returns count copied
+    uint64_t read_raster(uint64_t first, uint64_t cap, uint32_t* steps, uint32_t* ids);
+    uint64_t read_raster_raw(uint64_t first, uint64_t cap, uint32_t* records);
+    void clear_raster();
+
+    void set_profiling(bool on);
+    void get_profile(double* lif_ms, double* scatter_ms, uint64_t* launches);
+
+    uint64_t device_bytes() const { return bytes_; }
+
+    void* dalloc(size_t bytes);
+    void dfree(void* p, size_t bytes);
+
+private:
+    void launch_step_atomic();
+    void run_deterministic_step();
+    void capture_graph(uint32_t steps);
+    void destroy_graph();
+    void ensure_det_capacity(uint64_t events);
+
+    int device_ = 0;
+    int sm_count_ = 148;
+    cudaStream_t stream_ = nullptr;
+    uint64_t bytes_ = 0;
+
+    std::vector<NetHost*> nets_;
+    EngineDev eng_{};
+    NetDev* d_nets_ = nullptr;
+    PopDev* d_pops_ = nullptr;
+    ChunkDev* d_chunks_ = nullptr;
+    Ctl* d_ctl_ = nullptr;
+    SpikeRec* d_queue_[2] = {nullptr, nullptr};
+    uint2* d_raster_ = nullptr;
+    size_t nets_bytes_ = 0, pops_bytes_ = 0, chunks_bytes_ = 0, queue_bytes_ = 0, raster_bytes_ = 0;
+    std::vector<NetDev> h_nets_;
+    uint32_t queue_cap_ = 0;
+    uint32_t aggregation_ = NAER_AGG_ATOMIC;
+    uint32_t lif_grid_ = 0, scatter_grid_ = 0;
+    uint64_t host_step_ = 0;
+    uint64_t total_ring_cells_ = 0;
+
+    // CUDA graph of graph_steps_ atomic-mode steps
+    cudaGraphExec_t graph_exec_ = nullptr;
+    uint32_t graph_steps_ = 0;
+
+    // deterministic-mode scratch
+    unsigned long long* q_keys_[2] = {nullptr, nullptr};
+    uint32_t* q_vals_[2] = {nullptr, nullptr};
+    uint32_t* q_sizes_ = nullptr;
+    uint32_t* q_offs_ = nullptr;
+    unsigned long long* e_keys_[2] = {nullptr, nullptr};
+    float* e_vals_[2] = {nullptr, nullptr};
+    uint64_t e_cap_ = 0;
+    void* cub_tmp_ = nullptr;
+    size_t cub_tmp_bytes_ = 0;
+    uint32_t* h_pinned_ = nullptr;  // small pinned staging
+
+    // profiling
+    bool profiling_ = false;
+    std::vector<cudaEvent_t> prof_events_;
+    double prof_lif_ms_ = 0, prof_scatter_ms_ = 0;
+    uint64_t prof_launches_ = 0;
+    void resolve_profile();
+    cudaEvent_t next_event();
+    std::vector<cudaEvent_t> event_pool_;
+};
+
+}  // namespace naer

@@ -1,0 +1,124 @@
+// Device-visible descriptors shared by the kernels and the host engine.
+//
+// One engine holds any number of networks ("nets").  Every kernel reads its
+// work from these tables, so a plain run (one net), a packed batch and the
+// served slot table all go through the same kernels.
+//
+// Storage index space of a net: populations are laid out in the reference's
+// type order (STDP, then NOP, then POISSON; src/Network.cpp:267-285), each
+// population starting on a multiple of 4 so that four neurons share one
+// float4 of membrane potential.  The gaps are inert padding neurons (no
+// synapses in or out, never spike).  Reference addresses ("ids") are the
+// unpadded type-ordered addresses; each population records both bases.
+#pragma once
+#include <stdint.h>
+
+namespace naer {
+
+enum NeuronType : uint32_t { kSTDP = 0, kNOP = 1, kPOISSON = 2 };
+
+constexpr uint32_t kTgtSentinel = 0xFFFFFFFFu;  // padding entry in a CSR row
+constexpr uint32_t kRowAlign = 4;               // rows start on 16-byte boundaries
+constexpr uint32_t kLifThreads = 256;
+constexpr uint32_t kLifPerThread = 4;
+constexpr uint32_t kLifChunk = kLifThreads * kLifPerThread;  // neurons per LIF work item
+constexpr uint32_t kScatterThreads = 256;
+constexpr uint32_t kScatterUnroll = 8;  // 128-synapse slices in flight per warp
+
+struct PopDev {
+    uint32_t net;           // owning net slot
+    uint32_t type;          // NeuronType
+    uint32_t storage_base;  // first storage index (multiple of 4)
+    uint32_t size;          // neurons
+    uint32_t id_base;       // reference address of the first neuron (engine-global)
+    uint32_t t_ref_steps;   // refractory steps after a spike
+    float v_th;             // spike iff V > v_th (lif.cl:28)
+    float v_reset;
+    double prop;            // exp(-dt / tau_m), computed on the host
+    // Poisson generator (POISSON populations: their own spikes; LIF
+    // populations: per-neuron external drive).  rate_hz == 0 disables.
+    double rate_hz;
+    float drive_w;          // LIF drive weight per Poisson event
+    uint32_t rng_seed;      // Philox key word 1
+    uint32_t rng_n;         // N in the counter t0 * N + idx
+    uint32_t rng_idx_base;  // idx of the first neuron in the generator's index space
+    uint32_t z_hi;          // z in [z_hi, 0xFFFFFFFE] => first interval >= window
+    uint32_t t0_limit;      // fast path valid while t0 <= t0_limit (no u32 wrap)
+};
+
+struct NetDev {
+    float* v;               // [n_storage] membrane potential
+    uint8_t* refr;          // [n_storage] refractory countdown (steps)
+    float* ring;            // [ring_slots][n_storage] delayed input
+    const uint64_t* row_ptr;  // [n_storage + 1], row starts multiple of kRowAlign
+    const uint32_t* tgt;    // [S] target storage index or kTgtSentinel
+    float* w;               // [S] weight (written back by STDP)
+    const uint8_t* dly;     // [S] delay in steps, 1..ring_slots-1
+    // pair-based STDP state, one entry per plastic storage index
+    int32_t* last_post;     // step of the latest post spike, -1 = none
+    float* y_post;          // post trace right after last_post
+    int32_t* hist;          // [n_plastic][hist_len] post spike steps, newest first, -1 = none
+    int32_t* last_pre;      // step of the latest pre spike, -1 = none
+    float* x_pre;           // pre trace right after last_pre
+    const float* e_plus;    // [e_len] exp(-k dt / tau_plus) as float
+    const float* e_minus;   // [e_len] exp(-k dt / tau_minus) as float
+    uint64_t start_step;    // engine step at which this net's step 0 runs
+    uint64_t ring_key_base; // first ring cell of this net in the deterministic key space
+    uint32_t n_storage;     // multiple of 4
+    uint32_t ring_slots;    // D = max delay + 1
+    uint32_t dt_us;         // grid step in microseconds
+    uint32_t n_plastic;     // storage indices below this are STDP neurons
+    uint32_t stdp_on;       // plasticity enabled for this net
+    uint32_t hist_len;
+    uint32_t e_len;
+    float a_plus;           // A+ * w_max
+    float a_minus;          // A- * w_max
+    float w_max;
+    uint32_t active;        // 0 = slot idle (served form)
+    uint32_t pad_;
+};
+
+struct ChunkDev {
+    uint32_t pop;    // population index
+    uint32_t first;  // first storage index (multiple of 4)
+    uint32_t end;    // one past the last storage index of the population in this chunk
+    uint32_t pad_;
+};
+
+// One spike in the device queue.  aux0/aux1 carry the source's pre-synaptic
+// trace state before this spike (STDP sources), or the Poisson multiplicity
+// in aux0 (POISSON sources); the reference's spike record carries the same
+// pre information (previous_times, pre_traces: include/naer/naer_types.h:9-21).
+struct SpikeRec {
+    uint32_t net;
+    uint32_t src;    // storage index
+    int32_t aux0;    // old last_pre step | multiplicity
+    float aux1;      // old x_pre
+};
+
+struct Ctl {
+    unsigned long long step;        // engine step being simulated
+    unsigned long long raster_count;
+    unsigned long long events;      // synaptic events delivered
+    unsigned long long raster_dropped;
+    unsigned long long stdp_hist_overflow;
+    unsigned int q_count[2];
+    unsigned int scatter_done;
+    unsigned int error;
+};
+
+struct EngineDev {
+    Ctl* ctl;
+    const NetDev* nets;
+    const PopDev* pops;
+    const ChunkDev* chunks;
+    SpikeRec* queue[2];
+    uint2* raster;                  // {engine step, id}
+    unsigned long long raster_cap;
+    uint32_t n_chunks;
+    uint32_t n_nets;
+    uint32_t record;                // append spikes to the raster
+    uint32_t pad_;
+};
+
+}  // namespace naer

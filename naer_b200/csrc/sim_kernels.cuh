@@ -1,0 +1,95 @@
+// Simulation-step kernels (grid mode) and their device helpers.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "engine_types.cuh"
+#include "philox.cuh"
+
+namespace naer {
+
+// ---------------------------------------------------------------------------
+// Poisson window generator.  Restates simulate_poisson_neurons
+// (include/naer/kernels/input_neuron_group.cl:17-39) for one element:
+//   time = t0 + (uint)exprnd(rate, seed, t0 * N + idx)
+//   repeat 10 times: if time < t1 { emit; time += (uint)exprnd(rate, seed, time * N + idx) }
+// with key word 0 = the reference work-item id of idx (random.cl:8).
+// Returns the number of events in [t0, t1).
+static __device__ __noinline__ uint32_t poisson_exact(double rate, uint32_t seed, uint32_t n_gen,
+                                               uint32_t idx, uint32_t key0, uint32_t z0,
+                                               uint32_t t0, uint32_t t1) {
+    uint32_t time = t0 + ref_exp_interval_us(z0, rate);
+    uint32_t count = 0;
+    for (int m = 0; m < 10; ++m) {
+        if (!(time < t1)) break;
+        ++count;
+        const uint32_t z = philox_ref_z(time * n_gen + idx, key0, seed);
+        time += ref_exp_interval_us(z, rate);
+    }
+    return count;
+}
+
+__device__ __forceinline__ uint32_t poisson_count(const PopDev& p, uint32_t idx, uint32_t t0,
+                                                  uint32_t t1) {
+    const uint32_t key0 = ref_global_id(idx, kPoissonCapacity, kPoissonWorkgroup);
+    const uint32_t z0 = philox_ref_z(t0 * p.rng_n + idx, key0, p.rng_seed);
+    // Fast path: the first interval already reaches past the window.  z_hi is
+    // chosen on the host with a margin so that this agrees with the exact
+    // path for every z in [z_hi, 0xFFFFFFFE].
+    if (z0 >= p.z_hi && z0 != 0xFFFFFFFFu && t0 <= p.t0_limit) return 0;
+    return poisson_exact(p.rate_hz, p.rng_seed, p.rng_n, idx, key0, z0, t0, t1);
+}
+
+__device__ __forceinline__ float decay_lookup(const float* table, uint32_t len, int32_t k) {
+    return (k >= 0 && (uint32_t)k < len) ? __ldg(table + k) : 0.0f;
+}
+
+// Pair-based STDP for one plastic synapse at the pre spike of step t
+// (emission time).  Lazy LTP replays the post spikes of `tgt` in
+// (pre_last, t], oldest first, with the pre trace decayed from pre_last;
+// LTD uses the post trace at t.  Weights are clipped to [0, w_max] after
+// every update, so the sequence equals the online rule's.  Every operation
+// is an explicitly rounded fp32 op so the oracle can repeat it bit for bit.
+// Plays the role of update_synapse (include/naer/kernels/stdp.cl:8-30).
+__device__ __forceinline__ float stdp_update(const NetDev& n, float w, uint32_t tgt, int32_t t,
+                                             int32_t pre_last, float pre_x, uint32_t& overflow) {
+    if (pre_last >= 0) {
+        const int32_t* h = n.hist + (size_t)tgt * n.hist_len;
+        uint32_t c = 0;
+        while (c < n.hist_len && __ldcg(h + c) > pre_last) ++c;
+        if (c == n.hist_len) ++overflow;
+        for (int k = (int)c - 1; k >= 0; --k) {
+            const int32_t s = __ldcg(h + k);
+            const float x = __fmul_rn(pre_x, decay_lookup(n.e_plus, n.e_len, s - pre_last));
+            w = fminf(__fadd_rn(w, __fmul_rn(n.a_plus, x)), n.w_max);
+        }
+    }
+    const int32_t lp = __ldcg(n.last_post + tgt);
+    if (lp >= 0) {
+        const float y = __fmul_rn(__ldcg(n.y_post + tgt), decay_lookup(n.e_minus, n.e_len, t - lp));
+        w = fmaxf(__fsub_rn(w, __fmul_rn(n.a_minus, y)), 0.0f);
+    }
+    return w;
+}
+
+__device__ __forceinline__ uint32_t ring_slot(uint32_t t_mod, uint32_t d, uint32_t slots) {
+    uint32_t s = t_mod + d;
+    return s >= slots ? s - slots : s;
+}
+
+// Kernels ---------------------------------------------------------------------
+__global__ void k_lif(EngineDev eng);
+__global__ void k_scatter_atomic(EngineDev eng);
+__global__ void k_advance(EngineDev eng);
+// deterministic aggregation
+__global__ void k_det_queue_keys(EngineDev eng, uint32_t q, unsigned long long* keys,
+                                 uint32_t* vals, uint32_t count);
+__global__ void k_det_row_sizes(EngineDev eng, uint32_t q, const uint32_t* order, uint32_t count,
+                                uint32_t* sizes);
+__global__ void k_det_emit(EngineDev eng, uint32_t q, const uint32_t* order, uint32_t count,
+                           const uint32_t* offsets, unsigned long long* keys, float* vals);
+__global__ void k_det_fold(const NetDev* nets, uint32_t n_nets, const unsigned long long* keys,
+                           const float* vals, uint32_t count);
+
+}  // namespace naer

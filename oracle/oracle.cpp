@@ -1,0 +1,664 @@
+// ORACLE — test infrastructure only.  A CPU restatement of the reference's
+// simulation step (MatteoSchmider/Naer, OpenCL C kernels under
+// include/naer/kernels/ and host code src/Network.cpp), used by the tests,
+// the smoke check and the CPU baseline of the benchmark as the checker.  It
+// is never linked into, loaded by or called from the product library.
+//
+// Parity status: the reference cannot run in this environment (no OpenCL
+// runtime; several included .cl files and the Random123 submodule are not
+// in the reference tree), so this restatement is pinned only where a third
+// implementation exists: Philox4x32-10 is checked against cuRAND's
+// Philox4_32_10 (golden vectors under tests/golden).  The kernel semantics
+// below are otherwise restated from the reference source ("parity
+// unpinned" for those parts).
+//
+// Everything is written independently of the product sources: its own
+// Philox, its own layout (reference addresses, no padding), scalar loops.
+//
+// Build: oracle/Makefile -> oracle/liboracle.so (g++ -O2 -fopenmp
+// -ffp-contract=off; no fast-math, so fp32/fp64 operations round exactly as
+// written).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11): the generator behind Random123's
+// philox4x32 used at include/naer/kernels/random.cl:8-16.
+void oracle_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {
+    uint32_t c[4] = {ctr_in[0], ctr_in[1], ctr_in[2], ctr_in[3]};
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int round = 0; round < 10; ++round) {
+        if (round > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        const uint32_t n1 = (uint32_t)p1;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        const uint32_t n3 = (uint32_t)p0;
+        c[0] = n0;
+        c[1] = n1;
+        c[2] = n2;
+        c[3] = n3;
+    }
+    std::memcpy(out, c, sizeof(c));
+}
+
+}  // extern "C"
+
+namespace {
+
+inline void philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
+                   uint32_t out[4]) {
+    const uint32_t c[4] = {c0, c1, c2, c3};
+    const uint32_t k[2] = {k0, k1};
+    oracle_philox4x32_10(c, k, out);
+}
+
+// random.cl:6-24 — key {get_global_id(0), seed}, counter {iteration, 0, 0, 0},
+// the third output word over UINT_MAX, as double.
+inline double uniform_rand(uint32_t gid, uint32_t seed, uint32_t iteration, uint32_t* word0 = nullptr) {
+    uint32_t o[4];
+    philox(iteration, 0, 0, 0, gid, seed, o);
+    if (word0) *word0 = o[0];
+    return (double)o[2] / (double)4294967295u;
+}
+
+// random.cl:26-30 plus the (uint) cast of input_neuron_group.cl:29,37.
+// x == 1.0 gives +inf; the reference's cast is undefined there, the oracle
+// saturates to 0xFFFFFFFF.
+inline uint32_t exp_interval_us(uint32_t gid, uint32_t seed, uint32_t iteration, double rate) {
+    const double x = uniform_rand(gid, seed, iteration);
+    const double dt = std::log(1.0 - x) / (-(rate / 1000000.0));
+    if (!(dt < 4294967296.0)) return 0xFFFFFFFFu;
+    return (uint32_t)dt;
+}
+
+// Reference work-item id of element idx of a type with groups of
+// `capacity` processed by `wg` work-items (input_neuron_group.cl:17,26 with
+// Network.h:110-119: Poisson capacity 2048, workgroup 128).
+inline uint32_t poisson_gid(uint32_t idx) { return (idx / 2048u) * 128u + (idx % 2048u) % 128u; }
+
+// simulate_poisson_neurons (input_neuron_group.cl:17-39) for one element.
+uint32_t poisson_window(uint32_t idx, uint32_t n, uint32_t seed, double rate, uint32_t t0, uint32_t t1,
+                        uint32_t* times) {
+    const uint32_t gid = poisson_gid(idx);
+    uint32_t time = t0 + exp_interval_us(gid, seed, t0 * n + idx, rate);
+    uint32_t count = 0;
+    for (uint32_t multiple = 0; multiple < 10; ++multiple) {
+        if (time < t1) {
+            if (times) times[count] = time;
+            ++count;
+            time += exp_interval_us(gid, seed, time * n + idx, rate);
+        }
+    }
+    return count;
+}
+
+}  // namespace
+
+extern "C" {
+
+double oracle_uniform_rand(uint32_t gid, uint32_t seed, uint32_t iteration) {
+    return uniform_rand(gid, seed, iteration);
+}
+
+uint32_t oracle_exp_interval_us(uint32_t gid, uint32_t seed, uint32_t iteration, double rate) {
+    return exp_interval_us(gid, seed, iteration, rate);
+}
+
+uint32_t oracle_poisson_window(uint32_t idx, uint32_t n, uint32_t seed, double rate, uint32_t t0,
+                               uint32_t t1, uint32_t* times) {
+    return poisson_window(idx, n, seed, rate, t0, t1, times);
+}
+
+// ---------------------------------------------------------------------------
+// Network description (mirrors the product's C ABI parameter blocks).
+
+struct OrPop {
+    uint32_t type;  // 0 STDP, 1 NOP, 2 POISSON
+    uint32_t size;
+    float tau_m_ms, v_th, v_reset, t_ref_ms, v_init;
+    float rate_hz, drive_rate_hz, drive_weight;
+    uint32_t drive_seed, pad;
+};
+
+struct OrConn {
+    uint32_t src, dst, rule, degree;
+    double p;
+    float weight, wmin, wmax;
+    uint32_t dmin, dmax, pad;
+    uint64_t seed;
+};
+
+struct OrParams {
+    uint32_t dt_us;
+    uint32_t deterministic;  // 1: per-(step, cell) left fold; 0: parallel atomic adds
+    uint32_t poisson_seed;
+    uint32_t stdp_enabled;
+    float tau_plus_ms, tau_minus_ms, a_plus, a_minus, w_max;
+    uint32_t stdp_history;
+    int32_t threads;  // <= 0: all available
+};
+
+}  // extern "C"
+
+namespace {
+
+struct Net {
+    OrParams prm{};
+    std::vector<OrPop> pops;
+    std::vector<OrConn> conns;
+    // layout (reference addresses: Network.cpp:267-285)
+    std::vector<uint32_t> base;       // address of each population's first neuron
+    std::vector<uint32_t> type_addr;  // address within its type
+    uint32_t n = 0, n_poisson = 0, D = 2;
+    std::vector<uint8_t> kind;        // neuron type per address
+    std::vector<uint32_t> pop_of;     // population per address
+    // CSR in address order
+    std::vector<uint64_t> row_ptr;
+    std::vector<uint32_t> tgt;
+    std::vector<float> w;
+    std::vector<uint8_t> dly;
+    // state
+    std::vector<float> v;
+    std::vector<uint32_t> refr;
+    std::vector<float> ring;          // [D][n]
+    std::vector<int32_t> last_post, last_pre, hist;
+    std::vector<float> y_post, x_pre, e_plus, e_minus;
+    uint32_t e_len = 0;
+    bool plastic_on = false;
+    uint64_t step = 0;
+    uint64_t events = 0;
+    uint64_t hist_overflow = 0;
+    std::vector<uint32_t> sp_step, sp_id;
+    std::vector<float> partial;
+    std::vector<uint8_t> touched_flag;
+    std::vector<uint64_t> touched;
+};
+
+inline uint32_t pick(uint32_t word, uint32_t n) { return (uint32_t)(((uint64_t)word * n) >> 32); }
+
+inline uint32_t delay_of(const OrConn& c, uint32_t word) {
+    if (c.dmax <= c.dmin) return c.dmin;
+    return c.dmin + pick(word, c.dmax - c.dmin + 1);
+}
+
+inline float uniform_weight(float wmin, float wmax, float x) {
+    const float span = wmax - wmin;
+    const float prod = span * x;
+    return wmin + prod;
+}
+
+inline float unit_float(uint32_t word) { return (float)(word >> 8) * (1.0f / 16777216.0f); }
+
+void layout(Net& net) {
+    uint32_t count[3] = {0, 0, 0};
+    net.type_addr.resize(net.pops.size());
+    for (size_t i = 0; i < net.pops.size(); ++i) {
+        net.type_addr[i] = count[net.pops[i].type];
+        count[net.pops[i].type] += net.pops[i].size;
+    }
+    const uint32_t type_base[3] = {0, count[0], count[0] + count[1]};
+    net.n = count[0] + count[1] + count[2];
+    net.n_poisson = count[2];
+    net.base.resize(net.pops.size());
+    net.kind.assign(net.n, 0);
+    net.pop_of.assign(net.n, 0);
+    for (size_t i = 0; i < net.pops.size(); ++i) {
+        net.base[i] = type_base[net.pops[i].type] + net.type_addr[i];
+        for (uint32_t k = 0; k < net.pops[i].size; ++k) {
+            net.kind[net.base[i] + k] = (uint8_t)net.pops[i].type;
+            net.pop_of[net.base[i] + k] = (uint32_t)i;
+        }
+    }
+    uint32_t dmax = 1;
+    for (const auto& c : net.conns) dmax = std::max(dmax, c.dmax);
+    net.D = dmax + 1;
+}
+
+// Connectivity.  Rows: connections in declaration order; within a
+// connection REF_BERNOULLI by ascending target, FIXED_OUTDEGREE by draw k,
+// FIXED_INDEGREE by ascending (target, k).  Two passes: per-(connection,
+// source) counts, then the fill at prefix-sum offsets.
+void build_csr(Net& net) {
+    const size_t nc = net.conns.size();
+    std::vector<std::vector<uint32_t>> cnt(nc);
+    // pass 1: counts
+    for (size_t ci = 0; ci < nc; ++ci) {
+        const OrConn& c = net.conns[ci];
+        const OrPop& sp = net.pops[c.src];
+        const OrPop& dp = net.pops[c.dst];
+        const uint32_t seed_lo = (uint32_t)c.seed, seed_hi = (uint32_t)(c.seed >> 32);
+        cnt[ci].assign(sp.size, 0);
+        if (c.rule == 0) {
+            // count_connections (network.cl:14-49): the test for (s, d) runs on
+            // work-item s*32 + d%32 with counter d.
+#pragma omp parallel for schedule(dynamic, 16)
+            for (int64_t s = 0; s < (int64_t)sp.size; ++s) {
+                uint32_t k = 0;
+                for (uint32_t d = 0; d < dp.size; ++d)
+                    if (uniform_rand((uint32_t)s * 32u + d % 32u, seed_lo, d) < c.p) ++k;
+                cnt[ci][s] = k;
+            }
+        } else if (c.rule == 2) {
+            std::fill(cnt[ci].begin(), cnt[ci].end(), c.degree);
+        } else {
+            for (uint32_t i = 0; i < dp.size; ++i)
+                for (uint32_t b = 0; b < (c.degree + 3) / 4; ++b) {
+                    uint32_t os[4];
+                    philox(i, b, 0, 0, seed_lo, seed_hi, os);
+                    for (uint32_t j = 0; j < 4 && b * 4 + j < c.degree; ++j) ++cnt[ci][pick(os[j], sp.size)];
+                }
+        }
+    }
+    net.row_ptr.assign(net.n + 1, 0);
+    for (size_t ci = 0; ci < nc; ++ci) {
+        const uint32_t sb = net.base[net.conns[ci].src];
+        for (uint32_t s = 0; s < cnt[ci].size(); ++s) net.row_ptr[sb + s + 1] += cnt[ci][s];
+    }
+    for (uint32_t i = 0; i < net.n; ++i) net.row_ptr[i + 1] += net.row_ptr[i];
+    const uint64_t S = net.row_ptr[net.n];
+    net.tgt.resize(S);
+    net.w.resize(S);
+    net.dly.resize(S);
+    std::vector<uint64_t> cur(net.row_ptr.begin(), net.row_ptr.end() - 1);
+    // pass 2: fill
+    for (size_t ci = 0; ci < nc; ++ci) {
+        const OrConn& c = net.conns[ci];
+        const OrPop& sp = net.pops[c.src];
+        const OrPop& dp = net.pops[c.dst];
+        const uint32_t sb = net.base[c.src], db = net.base[c.dst];
+        const uint32_t seed_lo = (uint32_t)c.seed, seed_hi = (uint32_t)(c.seed >> 32);
+        if (c.rule == 0) {
+            // generate_connections (network.cl:63-107); weight 0 => random
+            // weight from the same draw (network.cl:97-100)
+#pragma omp parallel for schedule(dynamic, 16)
+            for (int64_t s = 0; s < (int64_t)sp.size; ++s) {
+                uint64_t o = cur[sb + s];
+                for (uint32_t d = 0; d < dp.size; ++d) {
+                    uint32_t word0 = 0;
+                    const double x = uniform_rand((uint32_t)s * 32u + d % 32u, seed_lo, d, &word0);
+                    if (!(x < c.p)) continue;
+                    net.tgt[o] = db + d;
+                    net.w[o] = c.weight == 0.0f ? uniform_weight(c.wmin, c.wmax, (float)x) : c.weight;
+                    net.dly[o] = (uint8_t)delay_of(c, word0);
+                    ++o;
+                }
+            }
+        } else if (c.rule == 2) {
+#pragma omp parallel for schedule(static)
+            for (int64_t s = 0; s < (int64_t)sp.size; ++s) {
+                const uint64_t o = cur[sb + s];
+                for (uint32_t b = 0; b < (c.degree + 3) / 4; ++b) {
+                    uint32_t ot[4], od[4], ow[4] = {0, 0, 0, 0};
+                    philox((uint32_t)s, b, 0, 0, seed_lo, seed_hi, ot);
+                    philox((uint32_t)s, b, 1, 0, seed_lo, seed_hi, od);
+                    if (c.weight == 0.0f) philox((uint32_t)s, b, 2, 0, seed_lo, seed_hi, ow);
+                    for (uint32_t j = 0; j < 4 && b * 4 + j < c.degree; ++j) {
+                        const uint64_t q = o + b * 4 + j;
+                        net.tgt[q] = db + pick(ot[j], dp.size);
+                        net.w[q] = c.weight == 0.0f ? uniform_weight(c.wmin, c.wmax, unit_float(ow[j])) : c.weight;
+                        net.dly[q] = (uint8_t)delay_of(c, od[j]);
+                    }
+                }
+            }
+        } else {
+            std::vector<uint64_t> pos(sp.size);
+            for (uint32_t s = 0; s < sp.size; ++s) pos[s] = cur[sb + s];
+            for (uint32_t i = 0; i < dp.size; ++i)
+                for (uint32_t b = 0; b < (c.degree + 3) / 4; ++b) {
+                    uint32_t os[4], od[4], ow[4] = {0, 0, 0, 0};
+                    philox(i, b, 0, 0, seed_lo, seed_hi, os);
+                    philox(i, b, 1, 0, seed_lo, seed_hi, od);
+                    if (c.weight == 0.0f) philox(i, b, 2, 0, seed_lo, seed_hi, ow);
+                    for (uint32_t j = 0; j < 4 && b * 4 + j < c.degree; ++j) {
+                        const uint64_t q = pos[pick(os[j], sp.size)]++;
+                        net.tgt[q] = db + i;
+                        net.w[q] = c.weight == 0.0f ? uniform_weight(c.wmin, c.wmax, unit_float(ow[j])) : c.weight;
+                        net.dly[q] = (uint8_t)delay_of(c, od[j]);
+                    }
+                }
+        }
+        for (uint32_t s = 0; s < sp.size; ++s) cur[sb + s] += cnt[ci][s];
+    }
+}
+
+void init_state(Net& net) {
+    net.v.assign(net.n, 0.0f);
+    net.refr.assign(net.n, 0);
+    for (size_t p = 0; p < net.pops.size(); ++p)
+        if (net.pops[p].type != 2)
+            for (uint32_t k = 0; k < net.pops[p].size; ++k) net.v[net.base[p] + k] = net.pops[p].v_init;
+    net.ring.assign((size_t)net.D * net.n, 0.0f);
+    const OrParams& P = net.prm;
+    uint32_t n_stdp = 0;
+    for (const auto& p : net.pops)
+        if (p.type == 0) n_stdp += p.size;
+    net.plastic_on = P.stdp_enabled && n_stdp > 0;
+    if (net.plastic_on) {
+        net.last_post.assign(net.n, -1);
+        net.last_pre.assign(net.n, -1);
+        net.y_post.assign(net.n, 0.0f);
+        net.x_pre.assign(net.n, 0.0f);
+        net.hist.assign((size_t)net.n * P.stdp_history, -1);
+        const double tmax = std::max((double)P.tau_plus_ms, (double)P.tau_minus_ms) * 1000.0;
+        net.e_len = (uint32_t)std::min<double>(std::ceil(104.0 * tmax / P.dt_us) + 1.0, 1 << 24);
+        net.e_plus.resize(net.e_len);
+        net.e_minus.resize(net.e_len);
+        for (uint32_t k = 0; k < net.e_len; ++k) {
+            net.e_plus[k] = (float)std::exp(-(double)k * P.dt_us / ((double)P.tau_plus_ms * 1000.0));
+            net.e_minus[k] = (float)std::exp(-(double)k * P.dt_us / ((double)P.tau_minus_ms * 1000.0));
+        }
+    }
+    net.partial.assign((size_t)net.D * net.n, 0.0f);
+    net.touched_flag.assign((size_t)net.D * net.n, 0);
+}
+
+inline float decay(const std::vector<float>& tab, int64_t k) {
+    return (k >= 0 && (uint64_t)k < tab.size()) ? tab[(size_t)k] : 0.0f;
+}
+
+struct Spike {
+    uint32_t src;
+    int32_t pre_last;  // STDP sources: previous pre spike step; POISSON: multiplicity
+    float pre_x;
+};
+
+// Pair-based STDP at the pre spike of step t: lazy LTP over the post spikes
+// of tgt in (pre_last, t], oldest first, then LTD with the post trace at t;
+// clip to [0, w_max] after every update.
+float stdp(Net& net, float wv, uint32_t tgt, int32_t t, int32_t pre_last, float pre_x, uint64_t& ovf) {
+    const OrParams& P = net.prm;
+    const float ap = P.a_plus * P.w_max;
+    const float am = P.a_minus * P.w_max;
+    if (pre_last >= 0) {
+        const int32_t* h = &net.hist[(size_t)tgt * P.stdp_history];
+        uint32_t c = 0;
+        while (c < P.stdp_history && h[c] > pre_last) ++c;
+        if (c == P.stdp_history) ++ovf;
+        for (int k = (int)c - 1; k >= 0; --k) {
+            const float x = pre_x * decay(net.e_plus, h[k] - pre_last);
+            const float inc = ap * x;
+            wv = std::min(wv + inc, P.w_max);
+        }
+    }
+    const int32_t lp = net.last_post[tgt];
+    if (lp >= 0) {
+        const float y = net.y_post[tgt] * decay(net.e_minus, t - lp);
+        const float dec = am * y;
+        wv = std::max(wv - dec, 0.0f);
+    }
+    return wv;
+}
+
+// One grid step (dt = prm.dt_us): neuron update for every address, then the
+// scatter of this step's spikes into the ring.  Returns nothing; spikes are
+// appended to sp_step/sp_id.
+void grid_step(Net& net) {
+    const OrParams& P = net.prm;
+    const uint32_t t = (uint32_t)net.step;
+    const uint32_t slot = t % net.D;
+    const uint32_t t0 = t * P.dt_us, t1 = t0 + P.dt_us;
+    const int nthreads =
+#ifdef _OPENMP
+        P.threads > 0 ? P.threads : omp_get_max_threads();
+#else
+        1;
+#endif
+    std::vector<std::vector<Spike>> per_thread(nthreads);
+    std::vector<double> prop(net.pops.size());
+    std::vector<uint32_t> tref(net.pops.size());
+    for (size_t p = 0; p < net.pops.size(); ++p) {
+        prop[p] = std::exp(-(double)P.dt_us / ((double)net.pops[p].tau_m_ms * 1000.0));
+        tref[p] = (uint32_t)std::llround((double)net.pops[p].t_ref_ms * 1000.0 / P.dt_us);
+    }
+    float* ring_slot = &net.ring[(size_t)slot * net.n];
+
+#pragma omp parallel num_threads(nthreads)
+    {
+#ifdef _OPENMP
+        const int tid = omp_get_thread_num();
+#else
+        const int tid = 0;
+#endif
+        std::vector<Spike>& out = per_thread[tid];
+#pragma omp for schedule(static)
+        for (int64_t ii = 0; ii < (int64_t)net.n; ++ii) {
+            const uint32_t i = (uint32_t)ii;
+            const uint32_t pi = net.pop_of[i];
+            const OrPop& pop = net.pops[pi];
+            if (pop.type == 2) {
+                if (!(pop.rate_hz > 0.0f)) continue;
+                const uint32_t idx = net.type_addr[pi] + (i - net.base[pi]);
+                const uint32_t m = poisson_window(idx, net.n_poisson, P.poisson_seed, (double)pop.rate_hz, t0, t1,
+                                                  nullptr);
+                if (m) out.push_back(Spike{i, (int32_t)m, 0.0f});
+                continue;
+            }
+            const float I = ring_slot[i];
+            ring_slot[i] = 0.0f;
+            if (net.refr[i] > 0) {
+                net.refr[i] -= 1;
+                continue;
+            }
+            float v = (float)((double)net.v[i] * prop[pi]);
+            v = v + I;
+            if (pop.drive_rate_hz > 0.0f) {
+                const uint32_t m = poisson_window(i - net.base[pi], pop.size, pop.drive_seed,
+                                                  (double)pop.drive_rate_hz, t0, t1, nullptr);
+                for (uint32_t k = 0; k < m; ++k) v = v + pop.drive_weight;
+            }
+            if (v > pop.v_th) {
+                v = pop.v_reset;
+                net.refr[i] = tref[pi];
+                Spike sp{i, 0, 0.0f};
+                if (net.plastic_on && pop.type == 0) {
+                    const int32_t ts = (int32_t)t;
+                    const int32_t lp = net.last_post[i];
+                    const float y = lp >= 0 ? net.y_post[i] * decay(net.e_minus, ts - lp) : 0.0f;
+                    net.y_post[i] = y + 1.0f;
+                    net.last_post[i] = ts;
+                    int32_t* h = &net.hist[(size_t)i * P.stdp_history];
+                    for (int k = (int)P.stdp_history - 1; k > 0; --k) h[k] = h[k - 1];
+                    h[0] = ts;
+                    sp.pre_last = net.last_pre[i];
+                    sp.pre_x = net.x_pre[i];
+                    const float x = sp.pre_last >= 0 ? net.x_pre[i] * decay(net.e_plus, ts - sp.pre_last) : 0.0f;
+                    net.x_pre[i] = x + 1.0f;
+                    net.last_pre[i] = ts;
+                }
+                out.push_back(sp);
+            }
+            net.v[i] = v;
+        }
+    }
+    // spikes in ascending address order (static schedule keeps chunks ordered)
+    std::vector<Spike> spikes;
+    for (auto& pt : per_thread) spikes.insert(spikes.end(), pt.begin(), pt.end());
+    for (const auto& sp : spikes) {
+        net.sp_step.push_back(t);
+        net.sp_id.push_back(sp.src);
+    }
+
+    const uint32_t tmod = t % net.D;
+    uint64_t ev = 0, ovf = 0;
+    auto deliver_weight = [&](const Spike& sp, uint64_t j) -> float {
+        float wv = net.w[j];
+        const uint32_t tg = net.tgt[j];
+        const bool src_plastic = net.plastic_on && net.kind[sp.src] == 0;
+        if (src_plastic && net.kind[tg] == 0) {
+            wv = stdp(net, wv, tg, (int32_t)t, sp.pre_last, sp.pre_x, ovf);
+            net.w[j] = wv;
+        }
+        if (!src_plastic && sp.pre_last > 1) wv = wv * (float)sp.pre_last;
+        return wv;
+    };
+    auto cell_of = [&](uint64_t j) -> uint64_t {
+        uint32_t sl = tmod + net.dly[j];
+        if (sl >= net.D) sl -= net.D;
+        return (uint64_t)sl * net.n + net.tgt[j];
+    };
+
+    if (P.deterministic) {
+        // per (step, cell): left fold in (source, synapse) order, then add
+        for (const auto& sp : spikes) {
+            for (uint64_t j = net.row_ptr[sp.src]; j < net.row_ptr[sp.src + 1]; ++j) {
+                const float wv = deliver_weight(sp, j);
+                const uint64_t cell = cell_of(j);
+                if (!net.touched_flag[cell]) {
+                    net.touched_flag[cell] = 1;
+                    net.touched.push_back(cell);
+                    net.partial[cell] = wv;
+                } else {
+                    net.partial[cell] = net.partial[cell] + wv;
+                }
+                ++ev;
+            }
+        }
+        for (uint64_t cell : net.touched) {
+            net.ring[cell] = net.ring[cell] + net.partial[cell];
+            net.touched_flag[cell] = 0;
+        }
+        net.touched.clear();
+    } else {
+        // the multithreaded baseline: spikes in parallel, atomic float adds
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : ev, ovf) num_threads(nthreads)
+        for (int64_t si = 0; si < (int64_t)spikes.size(); ++si) {
+            const Spike& sp = spikes[(size_t)si];
+            uint64_t local_ovf = 0;
+            for (uint64_t j = net.row_ptr[sp.src]; j < net.row_ptr[sp.src + 1]; ++j) {
+                float wv = net.w[j];
+                const uint32_t tg = net.tgt[j];
+                const bool src_plastic = net.plastic_on && net.kind[sp.src] == 0;
+                if (src_plastic && net.kind[tg] == 0) {
+                    wv = stdp(net, wv, tg, (int32_t)t, sp.pre_last, sp.pre_x, local_ovf);
+                    net.w[j] = wv;
+                }
+                if (!src_plastic && sp.pre_last > 1) wv = wv * (float)sp.pre_last;
+                std::atomic_ref<float>(net.ring[cell_of(j)]).fetch_add(wv, std::memory_order_relaxed);
+                ++ev;
+            }
+            ovf += local_ovf;
+        }
+    }
+    net.events += ev;
+    net.hist_overflow += ovf;
+    ++net.step;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* oracle_net_create(const OrParams* prm, const OrPop* pops, uint32_t npops, const OrConn* conns,
+                        uint32_t nconns) {
+    Net* net = new Net();
+    net->prm = *prm;
+    net->pops.assign(pops, pops + npops);
+    net->conns.assign(conns, conns + nconns);
+    layout(*net);
+    return net;
+}
+
+void oracle_net_destroy(void* h) { delete static_cast<Net*>(h); }
+
+int oracle_net_build(void* h) {
+    Net& net = *static_cast<Net*>(h);
+    build_csr(net);
+    init_state(net);
+    return 0;
+}
+
+uint32_t oracle_net_neurons(void* h) { return static_cast<Net*>(h)->n; }
+uint64_t oracle_net_synapses(void* h) { return static_cast<Net*>(h)->tgt.size(); }
+uint32_t oracle_net_ring_slots(void* h) { return static_cast<Net*>(h)->D; }
+uint32_t oracle_net_population_base(void* h, uint32_t pop) { return static_cast<Net*>(h)->base[pop]; }
+
+void oracle_net_copy_csr(void* h, uint64_t* row_ptr, uint32_t* tgt, float* w, uint8_t* d) {
+    const Net& net = *static_cast<Net*>(h);
+    std::copy(net.row_ptr.begin(), net.row_ptr.end(), row_ptr);
+    if (tgt) std::copy(net.tgt.begin(), net.tgt.end(), tgt);
+    if (w) std::copy(net.w.begin(), net.w.end(), w);
+    if (d) std::copy(net.dly.begin(), net.dly.end(), d);
+}
+
+// Replace weights (address-order CSR) before running, e.g. with the
+// product's own arrays.
+void oracle_net_set_weights(void* h, const float* w) {
+    Net& net = *static_cast<Net*>(h);
+    std::copy(w, w + net.w.size(), net.w.begin());
+}
+
+int oracle_net_run(void* h, uint64_t nsteps) {
+    Net& net = *static_cast<Net*>(h);
+    for (uint64_t k = 0; k < nsteps; ++k) grid_step(net);
+    return 0;
+}
+
+uint64_t oracle_net_step(void* h) { return static_cast<Net*>(h)->step; }
+uint64_t oracle_net_events(void* h) { return static_cast<Net*>(h)->events; }
+uint64_t oracle_net_hist_overflow(void* h) { return static_cast<Net*>(h)->hist_overflow; }
+uint64_t oracle_net_spike_count(void* h) { return static_cast<Net*>(h)->sp_id.size(); }
+
+void oracle_net_copy_spikes(void* h, uint32_t* steps, uint32_t* ids) {
+    const Net& net = *static_cast<Net*>(h);
+    std::copy(net.sp_step.begin(), net.sp_step.end(), steps);
+    std::copy(net.sp_id.begin(), net.sp_id.end(), ids);
+}
+
+void oracle_net_clear_spikes(void* h) {
+    Net& net = *static_cast<Net*>(h);
+    net.sp_step.clear();
+    net.sp_id.clear();
+}
+
+void oracle_net_copy_state(void* h, float* v, uint32_t* refr) {
+    const Net& net = *static_cast<Net*>(h);
+    for (uint32_t i = 0; i < net.n; ++i) {
+        const bool lif = net.kind[i] != 2;
+        if (v) v[i] = lif ? net.v[i] : 0.0f;
+        if (refr) refr[i] = lif ? net.refr[i] : 0u;
+    }
+}
+
+void oracle_net_set_state(void* h, const float* v, const uint32_t* refr) {
+    Net& net = *static_cast<Net*>(h);
+    for (uint32_t i = 0; i < net.n; ++i) {
+        if (net.kind[i] == 2) continue;
+        if (v) net.v[i] = v[i];
+        if (refr) net.refr[i] = refr[i];
+    }
+}
+
+void oracle_net_copy_ring(void* h, float* ring) {
+    const Net& net = *static_cast<Net*>(h);
+    std::copy(net.ring.begin(), net.ring.end(), ring);
+}
+
+void oracle_net_copy_weights(void* h, float* w) {
+    const Net& net = *static_cast<Net*>(h);
+    std::copy(net.w.begin(), net.w.end(), w);
+}
+
+int oracle_max_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,220 @@
+"""The oracle against independent restatements, golden vectors and the
+properties of the reference's algorithm (CPU only)."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from naer_b200 import _capi as capi
+from naer_b200 import spec as S
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+M = 0xFFFFFFFF
+
+
+def py_philox(ctr, key):
+    """Philox4x32-10 in plain Python (Salmon et al., SC'11), a third restatement."""
+    c = [int(x) & M for x in ctr]
+    k0, k1 = int(key[0]) & M, int(key[1]) & M
+    for r in range(10):
+        if r:
+            k0 = (k0 + 0x9E3779B9) & M
+            k1 = (k1 + 0xBB67AE85) & M
+        p0 = 0xD2511F53 * c[0]
+        p1 = 0xCD9E8D57 * c[2]
+        c = [((p1 >> 32) ^ c[1] ^ k0) & M, p1 & M, ((p0 >> 32) ^ c[3] ^ k1) & M, p0 & M]
+    return c
+
+
+def test_philox_matches_python_restatement(oracle_mod):
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        ctr = rng.integers(0, 2**32, 4, dtype=np.uint64)
+        key = rng.integers(0, 2**32, 2, dtype=np.uint64)
+        assert list(oracle_mod.philox4x32_10(ctr, key)) == py_philox(ctr, key)
+    for ctr, key in [([0, 0, 0, 0], [0, 0]), ([M] * 4, [M, M])]:
+        assert list(oracle_mod.philox4x32_10(ctr, key)) == py_philox(ctr, key)
+
+
+def test_philox_matches_curand_golden(oracle_mod):
+    """cuRAND's Philox4_32_10 outputs (generated on a B200 by
+    tests/golden/gen_philox_curand.py) pin the oracle's Philox."""
+    f = GOLDEN / "philox_curand.json"
+    if not f.exists():
+        pytest.skip("golden vectors not generated yet")
+    data = json.loads(f.read_text())
+    assert len(data["cases"]) >= 64
+    for case in data["cases"]:
+        seed, subseq, offset = case["seed"], case["subsequence"], case["offset"]
+        blk = offset // 4
+        ctr = [blk & M, blk >> 32, subseq & M, subseq >> 32]
+        key = [seed & M, seed >> 32]
+        assert list(oracle_mod.philox4x32_10(ctr, key)) == case["out"], case
+
+
+def test_uniform_rand_is_reference_formula(oracle_mod):
+    # random.cl:6-24: key {gid, seed}, counter {iter,0,0,0}, word z / UINT_MAX
+    for gid, seed, it in [(0, 0, 0), (5, 0x15AC7EBD, 123456), (2**31, 7, 2**32 - 1)]:
+        z = py_philox([it, 0, 0, 0], [gid, seed])[2]
+        assert oracle_mod.uniform_rand(gid, seed, it) == z / 4294967295.0
+
+
+def test_poisson_window_semantics(oracle_mod):
+    # input_neuron_group.cl:29-38: first draw from t0, at most 10 spikes,
+    # each time + (uint)exprnd(...) with counter time * N + idx
+    import math
+    n, seed, rate = 4096, 0x15AC7EBD, 20.0
+    for idx in [0, 1, 127, 128, 2047, 2048, 4095]:
+        for t0 in [0, 1500, 3000, 1_000_000]:
+            times = oracle_mod.poisson_window(idx, n, seed, rate, t0, t0 + 1500)
+            gid = (idx // 2048) * 128 + (idx % 2048) % 128
+            z = py_philox([(t0 * n + idx) & M, 0, 0, 0], [gid, seed])[2]
+            first = t0 + int(math.log(1.0 - z / 4294967295.0) / (-(rate / 1e6)))
+            if first < t0 + 1500:
+                assert len(times) >= 1 and times[0] == first
+            else:
+                assert len(times) == 0
+            assert np.all(np.diff(times.astype(np.int64)) >= 0) and len(times) <= 10
+
+
+def test_poisson_rate(oracle_mod):
+    # 2000 generators x 200 windows of 1.5 ms at 20 Hz: mean count 0.03
+    counts = [len(oracle_mod.poisson_window(i, 2000, 99, 20.0, t0, t0 + 1500))
+              for i in range(0, 2000, 7) for t0 in range(0, 300_000, 1500)]
+    assert np.mean(counts) == pytest.approx(0.03, rel=0.1)
+
+
+def small_spec(rule, **kw):
+    s = S.NetSpec()
+    P = s.add_pop(S.POISSON, 50, rate_hz=50.0)
+    E = s.add_pop(S.NOP, 120)
+    I = s.add_pop(S.STDP, 37)
+    s.connect(P, E, rule, 0.5, probability=0.2, degree=7, dmin=1, dmax=5, seed=11, **kw)
+    s.connect(E, I, rule, 0.0, probability=0.3, degree=5, wmin=0.1, wmax=0.4, dmin=2, dmax=2, seed=12)
+    s.connect(E, E, rule, -0.2, probability=0.1, degree=3, dmin=1, dmax=9, seed=13)
+    return s
+
+
+@pytest.mark.parametrize("rule", [capi.CONN_REF_BERNOULLI, capi.CONN_FIXED_INDEGREE, capi.CONN_FIXED_OUTDEGREE])
+def test_csr_rules(oracle_mod, rule):
+    s = small_spec(rule)
+    o = oracle_mod.OracleNet(s)
+    rp, tg, w, d = o.csr()
+    assert rp[0] == 0 and rp[-1] == len(tg) == o.S
+    base = {i: o.population_base(i) for i in range(3)}
+    # address layout: STDP first, then NOP, then POISSON (Network.cpp:271-272)
+    assert base[2] == 0 and base[1] == 37 and base[0] == 37 + 120
+    assert d.min() >= 1 and d.max() <= 9
+    E0, E1 = base[1], base[1] + 120
+    if rule == capi.CONN_FIXED_OUTDEGREE:
+        for a in range(base[0], base[0] + 50):
+            assert rp[a + 1] - rp[a] == 7
+        for a in range(E0, E1):
+            assert rp[a + 1] - rp[a] == 5 + 3
+    if rule == capi.CONN_FIXED_INDEGREE:
+        # each E target appears 7 times among the Poisson rows
+        rows = tg[rp[base[0]]:rp[base[0] + 50]]
+        assert np.all(np.bincount(rows - E0, minlength=120) == 7)
+    if rule == capi.CONN_REF_BERNOULLI:
+        # within one connection, targets ascend (network.cl:88-105 in order)
+        for a in range(base[0], base[0] + 50):
+            assert np.all(np.diff(tg[rp[a]:rp[a + 1]].astype(np.int64)) > 0)
+        frac = (rp[base[0] + 50] - rp[base[0]]) / (50 * 120)
+        assert frac == pytest.approx(0.2, abs=0.03)
+    # random weights (weight 0) lie in [wmin, wmax)
+    ei = np.concatenate([np.arange(int(rp[a]), int(rp[a + 1])) for a in range(E0, E1)]).astype(np.int64)
+    ws = w[ei]
+    rnd = ws[(ws >= 0.1 - 1e-7) & (ws <= 0.4)]
+    assert rnd.size > 0
+
+
+def test_bernoulli_is_reference_draw(oracle_mod):
+    """network.cl:34-41: (s, d) connected iff uniform_rand(seed32, d) on
+    work-item s*32 + d%32 is below p; weight from the same draw when 0."""
+    s = S.NetSpec()
+    A = s.add_pop(S.NOP, 9)
+    B = s.add_pop(S.NOP, 70)
+    seed = 0xBF785E3215AC7EBD
+    s.connect(A, B, capi.CONN_REF_BERNOULLI, 0.0, probability=0.35, wmin=-1.0, wmax=2.0, seed=seed)
+    o = oracle_mod.OracleNet(s)
+    rp, tg, w, d = o.csr()
+    bB = o.population_base(1)
+    for a in range(9):
+        exp_t, exp_w = [], []
+        for dd in range(70):
+            z = py_philox([dd, 0, 0, 0], [a * 32 + dd % 32, seed & M])[2]
+            x = z / 4294967295.0
+            if x < 0.35:
+                exp_t.append(bB + dd)
+                exp_w.append(np.float32(-1.0) + np.float32(3.0) * np.float32(x))
+        got = slice(rp[a], rp[a + 1])
+        assert list(tg[got]) == exp_t
+        assert np.array_equal(w[got], np.array(exp_w, dtype=np.float32))
+
+
+def test_lif_free_decay_matches_closed_form(oracle_mod):
+    """No input: V_t = fp32(fp64(V_{t-1}) * exp(-dt/tau)) each step."""
+    s = S.NetSpec()
+    s.add_pop(S.NOP, 4, v_init=19.0, tau_m_ms=10.0)
+    o = oracle_mod.OracleNet(s, deterministic=True)
+    o.run(37)
+    v, r = o.state()
+    P = np.exp(-100.0 / 10000.0)
+    x = np.float32(19.0)
+    for _ in range(37):
+        x = np.float32(np.float64(x) * P)
+    assert np.all(v == x) and np.all(r == 0)
+
+
+def test_lif_threshold_reset_refractory(oracle_mod):
+    """A neuron above threshold spikes once, resets to V_reset and ignores
+    input for t_ref steps (lif.cl:21-33 on the grid)."""
+    s = S.NetSpec()
+    s.add_pop(S.NOP, 1, v_init=25.0, v_th=20.0, v_reset=10.0, t_ref_ms=0.5, drive_rate_hz=5e4,
+              drive_weight=3.0, drive_seed=5)
+    o = oracle_mod.OracleNet(s, deterministic=True)
+    o.run(40)
+    st, ids = o.spikes()
+    assert st[0] == 0
+    assert np.all(np.diff(st.astype(np.int64)) >= 6)  # 5 refractory steps between spikes
+
+
+def test_deterministic_rerun_is_identical(oracle_mod):
+    s = S.brunel_small(poisson_weight=1.0)
+    a = oracle_mod.OracleNet(s, deterministic=True, threads=3)
+    b = oracle_mod.OracleNet(s, deterministic=True, threads=1)
+    a.run(300)
+    b.run(300)
+    sa, ia = a.spikes()
+    sb, ib = b.spikes()
+    assert np.array_equal(sa, sb) and np.array_equal(ia, ib) and len(ia) > 100
+    assert np.array_equal(a.state()[0], b.state()[0])
+
+
+def test_stdp_weights_stay_clipped(oracle_mod):
+    s = S.plastic_indegree(n=500, k=50, drive_weight=21.0)
+    o = oracle_mod.OracleNet(s, deterministic=True)
+    w0 = o.weights()
+    o.run(500)
+    w1 = o.weights()
+    rp, tg, _, _ = o.csr()
+    assert not np.array_equal(w0, w1)
+    nE = 400
+    src = np.repeat(np.arange(o.n), np.diff(rp).astype(np.int64))
+    ee = (src < nE) & (tg < nE)
+    assert np.all((w1[ee] >= 0.0) & (w1[ee] <= 0.5))
+    assert np.array_equal(w0[~ee], w1[~ee])
+
+
+def test_golden_oracle_fixture(oracle_mod):
+    """Regression fixture of the oracle itself (tests/golden/gen_oracle_fixtures.py)."""
+    f = GOLDEN / "oracle_brunel_small.npz"
+    if not f.exists():
+        pytest.skip("fixture not generated")
+    g = np.load(f)
+    o = oracle_mod.OracleNet(S.brunel_small(poisson_weight=1.0), deterministic=True)
+    o.run(int(g["steps"]))
+    st, ids = o.spikes()
+    assert np.array_equal(st, g["spike_steps"]) and np.array_equal(ids, g["spike_ids"])
+    assert np.array_equal(o.state()[0], g["v"])
