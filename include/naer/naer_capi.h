@@ -218,6 +218,10 @@ NAER_API int naer_net_read_csr(naer_net* net, uint64_t* row_ptr, uint32_t* tgt, 
 NAER_API int naer_net_set_profiling(naer_net* net, int enable);
 NAER_API int naer_net_get_profile(naer_net* net, double* lif_ms, double* scatter_ms,
                                   uint64_t* launches);
+/* Finer split of the same device time (ms): [0] LIF, [1] wait for all LIF
+ * blocks, [2] scatter, [3] Poisson draws of the next step, [4] wait for all
+ * scatter blocks.  Measured by the first block of the step kernel. */
+NAER_API int naer_net_get_phases(naer_net* net, double* phase_ms5);
 
 #ifdef __cplusplus
 }

@@ -137,6 +137,7 @@ PROTOTYPES = {
     "naer_net_read_csr": [_vp, _vp, _vp, _vp, _vp],
     "naer_net_set_profiling": [_vp, C.c_int],
     "naer_net_get_profile": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
+    "naer_net_get_phases": [_vp, _vp],
 }
 
 _lib = None

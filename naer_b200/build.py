@@ -43,7 +43,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not _stale():
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", str(tmp), *[str(CSRC / s) for s in SOURCES]]
+    extra = os.environ.get("NAER_NVCC_FLAGS", "").split()  # tuning sweeps, e.g. -DNAER_RUN_MIN_BLOCKS=3
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", str(tmp), *[str(CSRC / s) for s in SOURCES]]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True, cwd=str(PKG))

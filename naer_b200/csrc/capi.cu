@@ -230,10 +230,10 @@ int naer_net_get_stats(naer_net* net, naer_stats* st) {
         const naer::Ctl c = net->eng->read_ctl();
         std::memset(st, 0, sizeof(*st));
         st->step = c.step;
-        st->events = c.events;
-        st->spikes = std::min<uint64_t>(c.raster_count, net->net.params.raster_capacity);
+        st->events = net->eng->events_total();
+        st->spikes = std::min<uint64_t>(c.raster_next, net->net.params.raster_capacity);
         st->raster_dropped = c.raster_dropped;
-        st->stdp_hist_overflow = c.stdp_hist_overflow;
+        st->stdp_hist_overflow = net->eng->overflow_total();
         st->synapses = net->net.synapses;
         st->device_bytes = net->eng->device_bytes();
         st->neurons = net->net.n_ids;
@@ -360,6 +360,14 @@ int naer_net_get_profile(naer_net* net, double* lif_ms, double* scatter_ms, uint
     return guarded([&] {
         need_compiled(net);
         net->eng->get_profile(lif_ms, scatter_ms, launches);
+    });
+}
+
+int naer_net_get_phases(naer_net* net, double* phase_ms5) {
+    return guarded([&] {
+        need_compiled(net);
+        need(phase_ms5 != nullptr, NAER_E_INVALID, "null argument");
+        net->eng->get_phases(phase_ms5);
     });
 }
 

@@ -110,9 +110,6 @@ Engine::~Engine() {
     cudaGetDevice(&prev);
     cudaSetDevice(device_);
     cudaStreamSynchronize(stream_);
-    destroy_graph();
-    for (auto e : event_pool_) cudaEventDestroy(e);
-    for (auto e : prof_events_) cudaEventDestroy(e);
     auto f = [](void* p) {
         if (p) cudaFree(p);
     };
@@ -120,8 +117,14 @@ Engine::~Engine() {
     f(d_nets_);
     f(d_pops_);
     f(d_chunks_);
-    f(d_queue_[0]);
-    f(d_queue_[1]);
+    for (int i = 0; i < 2; ++i) {
+        f(d_queue_[i]);
+        f(d_qid_[i]);
+        f(d_counts_[i]);
+    }
+    f(d_ev_part_);
+    f(d_ovf_part_);
+    f(det_prefix_);
     f(d_raster_);
     for (int i = 0; i < 2; ++i) {
         f(q_keys_[i]);
@@ -325,7 +328,11 @@ void Engine::build(NetHost& n) {
     NAER_CK(cudaMemcpyAsync(hlen.data(), len, Ns * 8ull, cudaMemcpyDeviceToHost, st));
     NAER_CK(cudaStreamSynchronize(st));
     n.synapses = 0;
-    for (uint64_t x : hlen) n.synapses += x;
+    n.max_row_padded = 0;
+    for (uint64_t x : hlen) {
+        n.synapses += x;
+        n.max_row_padded = std::max<uint64_t>(n.max_row_padded, (x + kRowAlign - 1) / kRowAlign * kRowAlign);
+    }
     for (size_t ci = 0; ci < cnt.size(); ++ci)
         dfree(cnt[ci], std::max<uint64_t>(n.pops[n.conns[ci].src].size, 1) * 4ull);
     dfree(len, Ns * 8ull);
@@ -336,6 +343,8 @@ void Engine::build(NetHost& n) {
     n.v = static_cast<float*>(dalloc(Ns * 4ull));
     n.refr = static_cast<uint8_t*>(dalloc(Ns));
     n.ring = static_cast<float*>(dalloc((uint64_t)n.ring_slots * Ns * 4ull));
+    n.drive = static_cast<uint8_t*>(dalloc((uint64_t)kDriveSlots * Ns));
+    NAER_CK(cudaMemsetAsync(n.drive, 0, (uint64_t)kDriveSlots * Ns, st));
     std::vector<float> v0(Ns, 0.0f);
     for (const auto& p : n.pops)
         if (p.type != kPOISSON)
@@ -378,6 +387,7 @@ void Engine::build(NetHost& n) {
     d.v = n.v;
     d.refr = n.refr;
     d.ring = n.ring;
+    d.drive = n.drive;
     d.row_ptr = n.row_ptr;
     d.tgt = n.tgt;
     d.w = n.w;
@@ -412,6 +422,8 @@ void Engine::free_net(NetHost& n) {
     dfree(n.v, Ns * 4ull);
     dfree(n.refr, Ns);
     dfree(n.ring, (uint64_t)n.ring_slots * Ns * 4ull);
+    dfree(n.drive, (uint64_t)kDriveSlots * Ns);
+    n.drive = nullptr;
     dfree(n.row_ptr, (Ns + 1) * 8ull);
     dfree(n.tgt, std::max<uint64_t>(S, 4) * 4ull);
     dfree(n.w, std::max<uint64_t>(S, 4) * 4ull);
@@ -443,7 +455,6 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
                      uint32_t aggregation) {
     DeviceGuard g(device_);
     NAER_CK(cudaStreamSynchronize(stream_));
-    destroy_graph();
     nets_ = nets;
     aggregation_ = aggregation;
     std::vector<PopDev> pops;
@@ -489,7 +500,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
             const uint32_t pidx = (uint32_t)pops.size();
             pops.push_back(pd);
             for (uint32_t f = ps.storage_base; f < ps.storage_base + ps.size; f += kLifChunk)
-                chunks.push_back(ChunkDev{pidx, f, ps.storage_base + ps.size, 0});
+                chunks.push_back(ChunkDev{pidx, f, ps.storage_base + ps.size, ni});
         }
     }
     total_ring_cells_ = key_base;
@@ -513,15 +524,66 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     upload(p, chunks_bytes_, chunks.data(), chunks.size() * sizeof(ChunkDev));
     d_chunks_ = static_cast<ChunkDev*>(p);
 
-    const size_t qbytes = std::max<uint64_t>(qcap, 1) * sizeof(SpikeRec);
-    if (qbytes > queue_bytes_) {
-        for (int i = 0; i < 2; ++i) {
-            if (d_queue_[i]) dfree(d_queue_[i], queue_bytes_);
-            d_queue_[i] = static_cast<SpikeRec*>(dalloc(qbytes));
+    eng_ = EngineDev{};
+    eng_.n_chunks = (uint32_t)chunks.size();
+    eng_.n_nets = (uint32_t)nets.size();
+
+    // launch geometry: the persistent kernel's cooperative grid (all blocks
+    // resident).  Prefer the variant that keeps neuron state in shared
+    // memory, with as many blocks per SM as its footprint allows; the
+    // deterministic path's LIF uses the same queue regions.
+    int dev_smem_optin = 0;
+    NAER_CK(cudaDeviceGetAttribute(&dev_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+    cudaFuncAttributes fa{};
+    NAER_CK(cudaFuncGetAttributes(&fa, k_run<true>));
+    dev_smem_optin -= (int)fa.sharedSizeBytes;
+    NAER_CK(cudaFuncSetAttribute(k_run<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_smem_optin));
+    use_smem_state_ = false;
+    lif_grid_ = 0;
+    for (int bps = 4; bps >= 1 && !use_smem_state_; --bps) {
+        const uint32_t grid = (uint32_t)bps * sm_count_;
+        const uint32_t own = std::max<uint32_t>(1, (eng_.n_chunks + grid - 1) / grid);
+        const size_t smem = run_smem_bytes(grid, own, true);
+        if (smem > (size_t)dev_smem_optin) continue;
+        int occ = 0;
+        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_run<true>, kLifThreads, smem));
+        if (occ >= bps) {
+            use_smem_state_ = true;
+            lif_grid_ = grid;
+            scatter_smem_ = smem;
         }
-        queue_bytes_ = qbytes;
     }
-    queue_cap_ = (uint32_t)qcap;
+    if (!use_smem_state_) {
+        int occ = 0;
+        const size_t smem_bound = run_smem_bytes((uint32_t)sm_count_ * 4, 1, false);
+        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_run<false>, kLifThreads, smem_bound));
+        if (occ < 1) throw Error(NAER_E_CUDA, "the step kernel cannot be resident on this device");
+        lif_grid_ = (uint32_t)std::min(occ, 4) * sm_count_;
+        scatter_smem_ = run_smem_bytes(lif_grid_, 1, false);
+    }
+    scatter_grid_ = lif_grid_;
+    const uint32_t chunks_per_block = (eng_.n_chunks + lif_grid_ - 1) / lif_grid_;
+    const uint32_t region_cap = std::max<uint32_t>(1, chunks_per_block) * kLifChunk;
+
+    // fold per-block event counters of a previous installation into the base
+    if (d_ev_part_) {
+        events_base_ += sum_parts(d_ev_part_, ev_part_n_);
+        overflow_base_ += sum_parts(d_ovf_part_, ev_part_n_);
+    }
+    const uint64_t qentries = (uint64_t)lif_grid_ * region_cap;
+    if (qentries > 0xFFFFFFFFull) throw Error(NAER_E_OVERFLOW, "spike queue larger than 2^32 entries");
+    for (int i = 0; i < 2; ++i) {
+        regrow(reinterpret_cast<void*&>(d_queue_[i]), queue_bytes_[i], qentries * sizeof(SpikeRec));
+        regrow(reinterpret_cast<void*&>(d_qid_[i]), qid_bytes_[i], qentries * sizeof(uint32_t));
+        regrow(reinterpret_cast<void*&>(d_counts_[i]), counts_bytes_[i], (lif_grid_ + 1) * sizeof(uint32_t));
+        NAER_CK(cudaMemset(d_counts_[i], 0, (lif_grid_ + 1) * sizeof(uint32_t)));
+    }
+    regrow(reinterpret_cast<void*&>(d_ev_part_), ev_part_bytes_, scatter_grid_ * sizeof(unsigned long long));
+    regrow(reinterpret_cast<void*&>(d_ovf_part_), ovf_part_bytes_, scatter_grid_ * sizeof(unsigned long long));
+    NAER_CK(cudaMemset(d_ev_part_, 0, scatter_grid_ * sizeof(unsigned long long)));
+    NAER_CK(cudaMemset(d_ovf_part_, 0, scatter_grid_ * sizeof(unsigned long long)));
+    ev_part_n_ = scatter_grid_;
+    queue_cap_ = (uint32_t)qentries;
     const size_t rbytes = std::max<uint64_t>(raster_capacity, 1) * sizeof(uint2);
     if (rbytes != raster_bytes_) {
         if (d_raster_) dfree(d_raster_, raster_bytes_);
@@ -529,76 +591,75 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
         raster_bytes_ = rbytes;
     }
 
-    eng_ = EngineDev{};
     eng_.ctl = d_ctl_;
     eng_.nets = d_nets_;
     eng_.pops = d_pops_;
     eng_.chunks = d_chunks_;
-    eng_.queue[0] = d_queue_[0];
-    eng_.queue[1] = d_queue_[1];
+    for (int i = 0; i < 2; ++i) {
+        eng_.queue[i] = d_queue_[i];
+        eng_.qid[i] = d_qid_[i];
+        eng_.counts[i] = d_counts_[i];
+    }
+    eng_.ev_part = d_ev_part_;
+    eng_.ovf_part = d_ovf_part_;
     eng_.raster = d_raster_;
     eng_.raster_cap = raster_capacity;
-    eng_.n_chunks = (uint32_t)chunks.size();
-    eng_.n_nets = (uint32_t)nets.size();
+    eng_.lif_grid = lif_grid_;
+    eng_.region_cap = region_cap;
     eng_.record = record ? 1u : 0u;
-    lif_grid_ = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 8));
-    scatter_grid_ = (uint32_t)sm_count_ * 4;
+    // warps per spike: enough pieces to cover the longest row once
+    uint64_t max_row = 0;
+    for (NetHost* n : nets) max_row = std::max<uint64_t>(max_row, n->max_row_padded);
+    eng_.scatter_split =
+        (uint32_t)std::min<uint64_t>(16, std::max<uint64_t>(1, (max_row + kScatterPiece - 1) / kScatterPiece));
+}
+
+void Engine::regrow(void*& p, size_t& have, size_t need) {
+    need = std::max<size_t>(need, 16);
+    if (need <= have && p) return;
+    if (p) dfree(p, have);
+    p = dalloc(need);
+    have = need;
+}
+
+uint64_t Engine::sum_parts(const unsigned long long* d, uint32_t n) {
+    if (!d || n == 0) return 0;
+    std::vector<unsigned long long> h(n);
+    NAER_CK(cudaMemcpyAsync(h.data(), d, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
+    NAER_CK(cudaStreamSynchronize(stream_));
+    uint64_t t = 0;
+    for (auto x : h) t += x;
+    return t;
+}
+
+uint64_t Engine::events_total() {
+    DeviceGuard g(device_);
+    const Ctl c = read_ctl();
+    return events_base_ + c.events + sum_parts(d_ev_part_, ev_part_n_);
+}
+
+uint64_t Engine::overflow_total() {
+    DeviceGuard g(device_);
+    const Ctl c = read_ctl();
+    return overflow_base_ + c.stdp_hist_overflow + sum_parts(d_ovf_part_, ev_part_n_);
 }
 
 // ---------------------------------------------------------------------------
 // step loop
 
-void Engine::launch_step_atomic() {
-    k_lif<<<lif_grid_, kLifThreads, 0, stream_>>>(eng_);
-    k_scatter_atomic<<<scatter_grid_, kScatterThreads, 0, stream_>>>(eng_);
+void Engine::launch_run(uint32_t steps) {
+    unsigned long long s0 = host_step_;
+    NAER_CK(cudaMemsetAsync(&d_ctl_->bar_arrive, 0, sizeof(unsigned long long), stream_));
+    void* args[] = {&eng_, &s0, &steps};
+    const void* fn = use_smem_state_ ? (const void*)k_run<true> : (const void*)k_run<false>;
+    NAER_CK(cudaLaunchCooperativeKernel(fn, dim3(lif_grid_), dim3(kLifThreads), args, scatter_smem_, stream_));
+    host_step_ += steps;
 }
 
-void Engine::destroy_graph() {
-    if (graph_exec_) {
-        cudaGraphExecDestroy(graph_exec_);
-        graph_exec_ = nullptr;
-        graph_steps_ = 0;
-    }
-}
-
-void Engine::capture_graph(uint32_t steps) {
-    destroy_graph();
-    cudaGraph_t graph = nullptr;
-    NAER_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    for (uint32_t i = 0; i < steps; ++i) launch_step_atomic();
-    NAER_CK(cudaStreamEndCapture(stream_, &graph));
-    const cudaError_t e = cudaGraphInstantiate(&graph_exec_, graph, 0);
-    cudaGraphDestroy(graph);
-    NAER_CK(e);
-    graph_steps_ = steps;
-}
-
-cudaEvent_t Engine::next_event() {
-    cudaEvent_t e;
-    if (!event_pool_.empty()) {
-        e = event_pool_.back();
-        event_pool_.pop_back();
-    } else {
-        NAER_CK(cudaEventCreate(&e));
-    }
-    prof_events_.push_back(e);
-    return e;
-}
-
-void Engine::resolve_profile() {
-    if (prof_events_.empty()) return;
-    NAER_CK(cudaStreamSynchronize(stream_));
-    // events come in groups of four: lif start/end, scatter start/end
-    for (size_t i = 0; i + 3 < prof_events_.size(); i += 4) {
-        float a = 0, b = 0;
-        NAER_CK(cudaEventElapsedTime(&a, prof_events_[i], prof_events_[i + 1]));
-        NAER_CK(cudaEventElapsedTime(&b, prof_events_[i + 2], prof_events_[i + 3]));
-        prof_lif_ms_ += a;
-        prof_scatter_ms_ += b;
-        ++prof_launches_;
-    }
-    for (auto e : prof_events_) event_pool_.push_back(e);
-    prof_events_.clear();
+void Engine::launch_drive(uint64_t s_first, uint32_t nsteps) {
+    const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 16));
+    k_drive<<<grid, kLifThreads, 0, stream_>>>(eng_, (unsigned long long)s_first, nsteps);
+    NAER_CK(cudaGetLastError());
 }
 
 void Engine::run(uint64_t nsteps) {
@@ -608,33 +669,13 @@ void Engine::run(uint64_t nsteps) {
         for (uint64_t i = 0; i < nsteps; ++i) run_deterministic_step();
         return;
     }
-    if (profiling_) {
-        for (uint64_t i = 0; i < nsteps; ++i) {
-            NAER_CK(cudaEventRecord(next_event(), stream_));
-            k_lif<<<lif_grid_, kLifThreads, 0, stream_>>>(eng_);
-            NAER_CK(cudaEventRecord(next_event(), stream_));
-            NAER_CK(cudaEventRecord(next_event(), stream_));
-            k_scatter_atomic<<<scatter_grid_, kScatterThreads, 0, stream_>>>(eng_);
-            NAER_CK(cudaEventRecord(next_event(), stream_));
-            ++host_step_;
-            if (prof_events_.size() >= 4096) resolve_profile();
-        }
-        NAER_CK(cudaGetLastError());
-        return;
-    }
-    const uint32_t G = 64;
-    uint64_t left = nsteps;
-    if (left >= G) {
-        if (graph_steps_ != G) capture_graph(G);
-        while (left >= G) {
-            NAER_CK(cudaGraphLaunch(graph_exec_, stream_));
-            left -= G;
-            host_step_ += G;
-        }
-    }
-    for (; left > 0; --left) {
-        launch_step_atomic();
-        ++host_step_;
+    // Poisson counts of a chunk of steps are drawn first (full occupancy),
+    // then the persistent kernel simulates the chunk
+    while (nsteps > 0) {
+        const uint32_t n = (uint32_t)std::min<uint64_t>(nsteps, kDriveSlots);
+        launch_drive(host_step_, n);
+        launch_run(n);
+        nsteps -= n;
     }
     NAER_CK(cudaGetLastError());
 }
@@ -659,15 +700,17 @@ void Engine::ensure_det_capacity(uint64_t events) {
         q_sizes_ = static_cast<uint32_t*>(dalloc(q * 4ull));
         q_offs_ = static_cast<uint32_t*>(dalloc(q * 4ull));
     }
+    if (!det_prefix_) det_prefix_ = static_cast<uint32_t*>(dalloc((lif_grid_ + 1) * sizeof(uint32_t)));
     // CUB scratch large enough for every sort/scan of this capacity
-    size_t b1 = 0, b2 = 0, b3 = 0;
+    size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
     const int qn = (int)std::max<uint32_t>(queue_cap_, 1);
     NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b1, q_keys_[0], q_keys_[1], q_vals_[0], q_vals_[1],
                                             qn, 0, 64, stream_));
     NAER_CK(cub::DeviceScan::ExclusiveSum(nullptr, b2, q_sizes_, q_offs_, qn, stream_));
     NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b3, e_keys_[0], e_keys_[1], e_vals_[0], e_vals_[1],
                                             (int)std::min<uint64_t>(cap, 0x7FFFFFFF), 0, 64, stream_));
-    const size_t need = std::max({b1, b2, b3});
+    NAER_CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_counts_[0], det_prefix_, (int)(lif_grid_ + 1), stream_));
+    const size_t need = std::max({b1, b2, b3, b4});
     if (need > cub_tmp_bytes_) {
         if (cub_tmp_) dfree(cub_tmp_, cub_tmp_bytes_);
         cub_tmp_ = dalloc(need);
@@ -678,19 +721,22 @@ void Engine::ensure_det_capacity(uint64_t events) {
 void Engine::run_deterministic_step() {
     cudaStream_t st = stream_;
     if (!q_keys_[0]) ensure_det_capacity(1);
+    const uint32_t T = 256;
+    launch_drive(host_step_, 1);
     k_lif<<<lif_grid_, kLifThreads, 0, st>>>(eng_);
     const uint32_t qb = (uint32_t)(host_step_ & 1ull);
-    NAER_CK(cudaMemcpyAsync(h_pinned_, &d_ctl_->q_count[qb], 4, cudaMemcpyDeviceToHost, st));
+    size_t b = cub_tmp_bytes_;
+    NAER_CK(cub::DeviceScan::ExclusiveSum(cub_tmp_, b, d_counts_[qb], det_prefix_, (int)(lif_grid_ + 1), st));
+    NAER_CK(cudaMemcpyAsync(h_pinned_, det_prefix_ + lif_grid_, 4, cudaMemcpyDeviceToHost, st));
     NAER_CK(cudaStreamSynchronize(st));
     const uint32_t Q = h_pinned_[0];
     if (Q > 0) {
-        const uint32_t T = 256;
-        k_det_queue_keys<<<(Q + T - 1) / T, T, 0, st>>>(eng_, qb, q_keys_[0], q_vals_[0], Q);
-        size_t b = cub_tmp_bytes_;
+        k_det_queue_keys<<<(Q + T - 1) / T, T, 0, st>>>(eng_, det_prefix_, q_keys_[0], q_vals_[0], Q);
+        b = cub_tmp_bytes_;
         const int qbits = 32 + (int)bit_width(std::max<uint32_t>(eng_.n_nets, 1));
         NAER_CK(cub::DeviceRadixSort::SortPairs(cub_tmp_, b, q_keys_[0], q_keys_[1], q_vals_[0], q_vals_[1],
                                                 (int)Q, 0, std::min(qbits, 64), st));
-        k_det_row_sizes<<<(Q + T - 1) / T, T, 0, st>>>(eng_, qb, q_vals_[1], Q, q_sizes_);
+        k_det_row_sizes<<<(Q + T - 1) / T, T, 0, st>>>(eng_, q_vals_[1], Q, q_sizes_);
         b = cub_tmp_bytes_;
         NAER_CK(cub::DeviceScan::ExclusiveSum(cub_tmp_, b, q_sizes_, q_offs_, (int)Q, st));
         NAER_CK(cudaMemcpyAsync(h_pinned_, q_offs_ + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
@@ -698,11 +744,11 @@ void Engine::run_deterministic_step() {
         NAER_CK(cudaStreamSynchronize(st));
         const uint64_t E = (uint64_t)h_pinned_[0] + h_pinned_[1];
         if (E > 0x7FFFFFFFull) throw Error(NAER_E_OVERFLOW, "more than 2^31 events in one step");
+        k_det_raster<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + T - 1) / T, 1024)), T, 0, st>>>(eng_, q_vals_[1], Q);
         if (E > 0) {
             ensure_det_capacity(E);
             k_det_emit<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + 7) / 8, (uint32_t)sm_count_ * 8)),
-                         kScatterThreads, 0, st>>>(eng_, qb, q_vals_[1], Q, q_offs_, e_keys_[0],
-                                                   e_vals_[0]);
+                         kScatterThreads, 0, st>>>(eng_, q_vals_[1], Q, q_offs_, e_keys_[0], e_vals_[0]);
             b = cub_tmp_bytes_;
             const int ebits = std::max<int>(1, (int)bit_width(total_ring_cells_));
             NAER_CK(cub::DeviceRadixSort::SortPairs(cub_tmp_, b, e_keys_[0], e_keys_[1], e_vals_[0],
@@ -710,6 +756,8 @@ void Engine::run_deterministic_step() {
             k_det_fold<<<(uint32_t)((E + T - 1) / T), T, 0, st>>>(d_nets_, eng_.n_nets, e_keys_[1],
                                                                   e_vals_[1], (uint32_t)E);
         }
+    } else {
+        k_det_raster<<<1, 32, 0, st>>>(eng_, nullptr, 0);
     }
     k_advance<<<1, 32, 0, st>>>(eng_);
     NAER_CK(cudaGetLastError());
@@ -733,7 +781,7 @@ Ctl Engine::read_ctl() {
 
 uint64_t Engine::read_raster(uint64_t first, uint64_t cap, uint32_t* steps, uint32_t* ids) {
     const Ctl c = read_ctl();
-    const uint64_t total = std::min<uint64_t>(c.raster_count, eng_.raster_cap);
+    const uint64_t total = std::min<uint64_t>(c.raster_next, eng_.raster_cap);
     if (first >= total || cap == 0) return 0;
     const uint64_t n = std::min<uint64_t>(cap, total - first);
     std::vector<uint2> rec(n);
@@ -759,7 +807,7 @@ uint64_t Engine::read_raster(uint64_t first, uint64_t cap, uint32_t* steps, uint
 
 uint64_t Engine::read_raster_raw(uint64_t first, uint64_t cap, uint32_t* records) {
     const Ctl c = read_ctl();
-    const uint64_t total = std::min<uint64_t>(c.raster_count, eng_.raster_cap);
+    const uint64_t total = std::min<uint64_t>(c.raster_next, eng_.raster_cap);
     if (first >= total || cap == 0) return 0;
     const uint64_t n = std::min<uint64_t>(cap, total - first);
     DeviceGuard g(device_);
@@ -771,27 +819,33 @@ uint64_t Engine::read_raster_raw(uint64_t first, uint64_t cap, uint32_t* records
 void Engine::clear_raster() {
     DeviceGuard g(device_);
     NAER_CK(cudaStreamSynchronize(stream_));
-    const unsigned long long z[2] = {0, 0};
-    NAER_CK(cudaMemcpy(&d_ctl_->raster_count, z, 8, cudaMemcpyHostToDevice));
-    NAER_CK(cudaMemcpy(&d_ctl_->raster_dropped, z, 8, cudaMemcpyHostToDevice));
+    const unsigned long long z = 0;
+    NAER_CK(cudaMemcpy(&d_ctl_->raster_base, &z, 8, cudaMemcpyHostToDevice));
+    NAER_CK(cudaMemcpy(&d_ctl_->raster_next, &z, 8, cudaMemcpyHostToDevice));
+    NAER_CK(cudaMemcpy(&d_ctl_->raster_dropped, &z, 8, cudaMemcpyHostToDevice));
 }
 
 void Engine::set_profiling(bool on) {
     DeviceGuard g(device_);
-    if (!on) resolve_profile();
-    profiling_ = on;
+    // the persistent kernel always times its phases; enabling resets the totals
     if (on) {
-        prof_lif_ms_ = prof_scatter_ms_ = 0;
-        prof_launches_ = 0;
+        sync();
+        const unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        NAER_CK(cudaMemcpy(&d_ctl_->prof_lif_ns, z, sizeof(z), cudaMemcpyHostToDevice));
     }
+    profiling_ = on;
+}
+
+void Engine::get_phases(double* ms5) {
+    const Ctl c = read_ctl();
+    for (int q = 0; q < 5; ++q) ms5[q] = c.prof_phase_ns[q] * 1e-6;
 }
 
 void Engine::get_profile(double* lif_ms, double* scatter_ms, uint64_t* launches) {
-    DeviceGuard g(device_);
-    resolve_profile();
-    if (lif_ms) *lif_ms = prof_lif_ms_;
-    if (scatter_ms) *scatter_ms = prof_scatter_ms_;
-    if (launches) *launches = prof_launches_;
+    const Ctl c = read_ctl();
+    if (lif_ms) *lif_ms = c.prof_lif_ns * 1e-6;
+    if (scatter_ms) *scatter_ms = c.prof_scatter_ns * 1e-6;
+    if (launches) *launches = c.prof_steps;
 }
 
 }  // namespace naer

@@ -46,7 +46,7 @@ struct NetHost {
     std::vector<uint32_t> pop_order;   // pops in type order
     uint32_t n_ids = 0, n_storage = 0, n_plastic = 0, ring_slots = 0;
     uint32_t n_poisson = 0;
-    uint64_t synapses = 0, synapses_padded = 0;
+    uint64_t synapses = 0, synapses_padded = 0, max_row_padded = 0;
     std::vector<int32_t> id_of_storage;   // -1 for padding
     std::vector<uint32_t> storage_of_id;
 
@@ -54,6 +54,7 @@ struct NetHost {
     float* v = nullptr;
     uint8_t* refr = nullptr;
     float* ring = nullptr;
+    uint8_t* drive = nullptr;
     uint64_t* row_ptr = nullptr;
     uint32_t* tgt = nullptr;
     float* w = nullptr;
@@ -100,18 +101,22 @@ public:
 
     void set_profiling(bool on);
     void get_profile(double* lif_ms, double* scatter_ms, uint64_t* launches);
+    void get_phases(double* ms5);
 
     uint64_t device_bytes() const { return bytes_; }
+    uint64_t events_total();
+    uint64_t overflow_total();
 
     void* dalloc(size_t bytes);
     void dfree(void* p, size_t bytes);
 
 private:
-    void launch_step_atomic();
+    void launch_run(uint32_t steps);
+    void launch_drive(uint64_t s_first, uint32_t nsteps);
     void run_deterministic_step();
-    void capture_graph(uint32_t steps);
-    void destroy_graph();
     void ensure_det_capacity(uint64_t events);
+    void regrow(void*& p, size_t& have, size_t need);
+    uint64_t sum_parts(const unsigned long long* d, uint32_t n);
 
     int device_ = 0;
     int sm_count_ = 148;
@@ -125,8 +130,18 @@ private:
     ChunkDev* d_chunks_ = nullptr;
     Ctl* d_ctl_ = nullptr;
     SpikeRec* d_queue_[2] = {nullptr, nullptr};
+    uint32_t* d_qid_[2] = {nullptr, nullptr};
+    uint32_t* d_counts_[2] = {nullptr, nullptr};
+    unsigned long long* d_ev_part_ = nullptr;
+    unsigned long long* d_ovf_part_ = nullptr;
+    uint32_t ev_part_n_ = 0;
+    uint64_t events_base_ = 0, overflow_base_ = 0;
     uint2* d_raster_ = nullptr;
-    size_t nets_bytes_ = 0, pops_bytes_ = 0, chunks_bytes_ = 0, queue_bytes_ = 0, raster_bytes_ = 0;
+    size_t nets_bytes_ = 0, pops_bytes_ = 0, chunks_bytes_ = 0, raster_bytes_ = 0;
+    size_t queue_bytes_[2] = {0, 0}, qid_bytes_[2] = {0, 0}, counts_bytes_[2] = {0, 0};
+    size_t ev_part_bytes_ = 0, ovf_part_bytes_ = 0;
+    size_t scatter_smem_ = 0;
+    uint32_t* det_prefix_ = nullptr;
     std::vector<NetDev> h_nets_;
     uint32_t queue_cap_ = 0;
     uint32_t aggregation_ = NAER_AGG_ATOMIC;
@@ -134,9 +149,6 @@ private:
     uint64_t host_step_ = 0;
     uint64_t total_ring_cells_ = 0;
 
-    // CUDA graph of graph_steps_ atomic-mode steps
-    cudaGraphExec_t graph_exec_ = nullptr;
-    uint32_t graph_steps_ = 0;
 
     // deterministic-mode scratch
     unsigned long long* q_keys_[2] = {nullptr, nullptr};
@@ -150,14 +162,8 @@ private:
     size_t cub_tmp_bytes_ = 0;
     uint32_t* h_pinned_ = nullptr;  // small pinned staging
 
-    // profiling
     bool profiling_ = false;
-    std::vector<cudaEvent_t> prof_events_;
-    double prof_lif_ms_ = 0, prof_scatter_ms_ = 0;
-    uint64_t prof_launches_ = 0;
-    void resolve_profile();
-    cudaEvent_t next_event();
-    std::vector<cudaEvent_t> event_pool_;
+    bool use_smem_state_ = false;
 };
 
 }  // namespace naer

@@ -23,7 +23,12 @@ constexpr uint32_t kLifThreads = 256;
 constexpr uint32_t kLifPerThread = 4;
 constexpr uint32_t kLifChunk = kLifThreads * kLifPerThread;  // neurons per LIF work item
 constexpr uint32_t kScatterThreads = 256;
-constexpr uint32_t kScatterUnroll = 8;  // 128-synapse slices in flight per warp
+constexpr uint32_t kScatterUnroll = 2;  // 128-synapse slices in flight per warp
+constexpr uint32_t kScatterPiece = 128 * kScatterUnroll;  // synapses per warp iteration
+// Steps of Poisson counts drawn ahead (ring of slots); small enough that the
+// counts and the delay ring stay resident in L2 together.
+constexpr uint32_t kDriveSlots = 16;
+constexpr uint32_t kLifBatch = 4;     // owned chunks whose loads are issued together
 
 struct PopDev {
     uint32_t net;           // owning net slot
@@ -50,6 +55,7 @@ struct NetDev {
     float* v;               // [n_storage] membrane potential
     uint8_t* refr;          // [n_storage] refractory countdown (steps)
     float* ring;            // [ring_slots][n_storage] delayed input
+    uint8_t* drive;         // [kDriveSlots][n_storage] Poisson events per step (drive or own spikes)
     const uint64_t* row_ptr;  // [n_storage + 1], row starts multiple of kRowAlign
     const uint32_t* tgt;    // [S] target storage index or kTgtSentinel
     float* w;               // [S] weight (written back by STDP)
@@ -82,7 +88,7 @@ struct ChunkDev {
     uint32_t pop;    // population index
     uint32_t first;  // first storage index (multiple of 4)
     uint32_t end;    // one past the last storage index of the population in this chunk
-    uint32_t pad_;
+    uint32_t net;    // net slot of the population
 };
 
 // One spike in the device queue.  aux0/aux1 carry the source's pre-synaptic
@@ -96,29 +102,54 @@ struct SpikeRec {
     float aux1;      // old x_pre
 };
 
+// Device control block.
+//   step        engine step being simulated (read by the kernels of the
+//               deterministic path; the persistent kernel takes it as an
+//               argument and stores the end step)
+//   raster_base raster records before the current step (deterministic path)
+//   raster_next raster records kept so far
+//   bar_arrive  grid barrier arrivals of the persistent kernel (zeroed per launch)
+//   error       first device-side error (negated NAER status), 0 = none
+//   prof_*      phase times of the persistent kernel (block 0, %globaltimer)
 struct Ctl {
-    unsigned long long step;        // engine step being simulated
-    unsigned long long raster_count;
-    unsigned long long events;      // synaptic events delivered
+    unsigned long long step;
+    unsigned long long raster_base;
+    unsigned long long raster_next;
     unsigned long long raster_dropped;
+    unsigned long long events;      // deterministic-mode events (atomic mode: per-block counters)
     unsigned long long stdp_hist_overflow;
-    unsigned int q_count[2];
-    unsigned int scatter_done;
+    unsigned long long prof_lif_ns;
+    unsigned long long prof_scatter_ns;
+    unsigned long long prof_steps;
+    unsigned long long prof_phase_ns[5];  // LIF, barrier 1, scatter items, Poisson draws, barrier 2
+    unsigned long long bar_arrive;  // grid barrier arrivals of the running launch
     unsigned int error;
+    unsigned int pad_;
 };
 
+constexpr int NAER_STATUS_TIMEOUT = -4;  // NAER_E_TIMEOUT of the C ABI
+
+// Spike queue: LIF block b compacts its spikes into region
+// [b * region_cap, (b + 1) * region_cap) of the step's buffer and writes
+// their number to counts[b]; the scatter prefix-sums the counts.
 struct EngineDev {
     Ctl* ctl;
     const NetDev* nets;
     const PopDev* pops;
     const ChunkDev* chunks;
     SpikeRec* queue[2];
+    uint32_t* qid[2];               // reference address of each queued spike
+    uint32_t* counts[2];            // [lif_grid] spikes per LIF block region
+    unsigned long long* ev_part;    // [scatter_grid] events delivered, per scatter block
+    unsigned long long* ovf_part;   // [scatter_grid] lazy-LTP history overflows, per block
     uint2* raster;                  // {engine step, id}
     unsigned long long raster_cap;
     uint32_t n_chunks;
     uint32_t n_nets;
+    uint32_t lif_grid;
+    uint32_t region_cap;
     uint32_t record;                // append spikes to the raster
-    uint32_t pad_;
+    uint32_t scatter_split;         // warps per spike (row pieces of kScatterPiece)
 };
 
 }  // namespace naer

@@ -16,7 +16,7 @@ namespace naer {
 //   repeat 10 times: if time < t1 { emit; time += (uint)exprnd(rate, seed, time * N + idx) }
 // with key word 0 = the reference work-item id of idx (random.cl:8).
 // Returns the number of events in [t0, t1).
-static __device__ __noinline__ uint32_t poisson_exact(double rate, uint32_t seed, uint32_t n_gen,
+static __device__ __forceinline__ uint32_t poisson_exact(double rate, uint32_t seed, uint32_t n_gen,
                                                uint32_t idx, uint32_t key0, uint32_t z0,
                                                uint32_t t0, uint32_t t1) {
     uint32_t time = t0 + ref_exp_interval_us(z0, rate);
@@ -28,6 +28,16 @@ static __device__ __noinline__ uint32_t poisson_exact(double rate, uint32_t seed
         time += ref_exp_interval_us(z, rate);
     }
     return count;
+}
+
+// First draw of the window (word z of Philox at counter t0 * N + idx).
+__device__ __forceinline__ uint32_t poisson_z0(const PopDev& p, uint32_t idx, uint32_t t0) {
+    return philox_ref_z(t0 * p.rng_n + idx, ref_global_id(idx, kPoissonCapacity, kPoissonWorkgroup), p.rng_seed);
+}
+
+// True when the first draw alone proves the window empty.
+__device__ __forceinline__ bool poisson_quiet(const PopDev& p, uint32_t z0, uint32_t t0) {
+    return z0 >= p.z_hi && z0 != 0xFFFFFFFFu && t0 <= p.t0_limit;
 }
 
 __device__ __forceinline__ uint32_t poisson_count(const PopDev& p, uint32_t idx, uint32_t t0,
@@ -45,6 +55,33 @@ __device__ __forceinline__ float decay_lookup(const float* table, uint32_t len, 
     return (k >= 0 && (uint32_t)k < len) ? __ldg(table + k) : 0.0f;
 }
 
+// Register copy of a net's plasticity fields (the kernels copy descriptor
+// fields once per work item so that stores and atomics cannot force reloads).
+struct StdpView {
+    const int32_t* __restrict__ hist;
+    const int32_t* __restrict__ last_post;
+    const float* __restrict__ y_post;
+    const float* __restrict__ e_plus;
+    const float* __restrict__ e_minus;
+    uint32_t hist_len, e_len;
+    float a_plus, a_minus, w_max;
+};
+
+__device__ __forceinline__ StdpView stdp_view(const NetDev& n) {
+    StdpView v;
+    v.hist = n.hist;
+    v.last_post = n.last_post;
+    v.y_post = n.y_post;
+    v.e_plus = n.e_plus;
+    v.e_minus = n.e_minus;
+    v.hist_len = n.hist_len;
+    v.e_len = n.e_len;
+    v.a_plus = n.a_plus;
+    v.a_minus = n.a_minus;
+    v.w_max = n.w_max;
+    return v;
+}
+
 // Pair-based STDP for one plastic synapse at the pre spike of step t
 // (emission time).  Lazy LTP replays the post spikes of `tgt` in
 // (pre_last, t], oldest first, with the pre trace decayed from pre_last;
@@ -52,7 +89,7 @@ __device__ __forceinline__ float decay_lookup(const float* table, uint32_t len, 
 // every update, so the sequence equals the online rule's.  Every operation
 // is an explicitly rounded fp32 op so the oracle can repeat it bit for bit.
 // Plays the role of update_synapse (include/naer/kernels/stdp.cl:8-30).
-__device__ __forceinline__ float stdp_update(const NetDev& n, float w, uint32_t tgt, int32_t t,
+__device__ __forceinline__ float stdp_update(const StdpView& n, float w, uint32_t tgt, int32_t t,
                                              int32_t pre_last, float pre_x, uint32_t& overflow) {
     if (pre_last >= 0) {
         const int32_t* h = n.hist + (size_t)tgt * n.hist_len;
@@ -80,15 +117,19 @@ __device__ __forceinline__ uint32_t ring_slot(uint32_t t_mod, uint32_t d, uint32
 
 // Kernels ---------------------------------------------------------------------
 __global__ void k_lif(EngineDev eng);
-__global__ void k_scatter_atomic(EngineDev eng);
+template <bool kSmem>
+__global__ void k_run(EngineDev eng, unsigned long long s0, uint32_t nsteps);
+// dynamic shared memory of k_run for a grid and a number of owned chunks per block
+size_t run_smem_bytes(uint32_t grid, uint32_t own_max, bool smem_state);
 __global__ void k_advance(EngineDev eng);
+__global__ void k_drive(EngineDev eng, unsigned long long s_first, uint32_t nsteps);
 // deterministic aggregation
-__global__ void k_det_queue_keys(EngineDev eng, uint32_t q, unsigned long long* keys,
+__global__ void k_det_queue_keys(EngineDev eng, const uint32_t* prefix, unsigned long long* keys,
                                  uint32_t* vals, uint32_t count);
-__global__ void k_det_row_sizes(EngineDev eng, uint32_t q, const uint32_t* order, uint32_t count,
-                                uint32_t* sizes);
-__global__ void k_det_emit(EngineDev eng, uint32_t q, const uint32_t* order, uint32_t count,
-                           const uint32_t* offsets, unsigned long long* keys, float* vals);
+__global__ void k_det_row_sizes(EngineDev eng, const uint32_t* order, uint32_t count, uint32_t* sizes);
+__global__ void k_det_raster(EngineDev eng, const uint32_t* order, uint32_t count);
+__global__ void k_det_emit(EngineDev eng, const uint32_t* order, uint32_t count, const uint32_t* offsets,
+                           unsigned long long* keys, float* vals);
 __global__ void k_det_fold(const NetDev* nets, uint32_t n_nets, const unsigned long long* keys,
                            const float* vals, uint32_t count);
 

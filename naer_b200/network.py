@@ -274,4 +274,8 @@ class Network:
         capi.call("naer_net_get_profile", self._h, C.byref(lif), C.byref(sc), C.byref(n))
         self.nop_time = lif.value / 1e3
         self.scatter_time = sc.value / 1e3
-        return {"lif_ms": lif.value, "scatter_ms": sc.value, "steps": n.value}
+        ph = (C.c_double * 5)()
+        capi.call("naer_net_get_phases", self._h, C.cast(ph, C.c_void_p))
+        names = ["lif", "lif_wait", "scatter", "poisson", "scatter_wait"]
+        return {"lif_ms": lif.value, "scatter_ms": sc.value, "steps": n.value,
+                "phases_ms": {k: ph[i] for i, k in enumerate(names)}}
