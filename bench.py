@@ -253,7 +253,9 @@ def run_ours(args):
     ms_max, events_all = reduce_max_sum(world, ms, float(events))
     value = events_all / (ms_max / 1e3)
 
-    # roofline: per-kernel CUDA events around every launch on the engine stream
+    # roofline: CUDA events around every launch on the engine stream; the
+    # dominant kernel is the persistent step kernel k_run (LIF + scatter of
+    # 16 grid steps per launch), timed against 9 B per delivered event
     net.set_profiling(True)
     p0 = net.stats()["events"]
     net.run(args.profile_steps)
@@ -261,8 +263,8 @@ def run_ours(args):
     prof = net.profile()
     net.set_profiling(False)
     pev = net.stats()["events"] - p0
-    scatter_s = prof["scatter_ms"] / 1e3
-    lif_s = prof["lif_ms"] / 1e3
+    kern_s = prof["step_kernel_ms"] / 1e3
+    launches = max(1, prof["step_kernel_launches"])
     peak = None
     peak_src = "fallback"
     try:
@@ -270,13 +272,15 @@ def run_ours(args):
         peak_src = "measured"
     except Exception:
         peak = 6650.0
-    achieved = BYTES_PER_EVENT * pev / scatter_s / 1e9 if scatter_s > 0 else 0.0
+    achieved = BYTES_PER_EVENT * pev / kern_s / 1e9 if kern_s > 0 else 0.0
+    ph = prof["phases_ms"]
+    ph_tot = sum(ph.values()) or 1.0
     traffic = None
-    tfile = ROOT / "profiles" / "scatter_traffic.json"
+    tfile = ROOT / "profiles" / "k_run_traffic.json"
     if tfile.exists():
         try:
-            traffic = json.loads(tfile.read_text()).get("bytes_per_event")
-            traffic = traffic * pev / max(1, prof["steps"]) if traffic else None
+            t = json.loads(tfile.read_text())
+            traffic = t["bytes_per_event"] * pev / launches
         except Exception:
             traffic = None
 
@@ -319,13 +323,16 @@ def run_ours(args):
             "config": workload_config(args, int(st1["synapses"])),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
-                         "kernel": "k_scatter_atomic",
+                         "kernel": "k_run (persistent step kernel: LIF + scatter)",
                          "peak_source": peak_src,
-                         "note": f"{BYTES_PER_EVENT} B x {pev} events over {prof['steps']} scatter launches, "
-                                 f"{prof['scatter_ms']:.2f} ms total (LIF {prof['lif_ms']:.2f} ms)"},
+                         "note": f"{BYTES_PER_EVENT} B x {pev} events over {launches} k_run launches "
+                                 f"({args.profile_steps} grid steps), {prof['step_kernel_ms']:.2f} ms of k_run "
+                                 f"(CUDA events); Poisson-draw kernel {prof['drive_kernel_ms']:.2f} ms; "
+                                 f"phase split of k_run (block 0): "
+                                 + ", ".join(f"{k} {v / ph_tot:.0%}" for k, v in ph.items())},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": 2 * chunk * args.steps,
+            "gpu_launches": 2 * ((chunk + 15) // 16) * args.steps,
             "clocks": clk,
             "spikes_per_s_sim": spikes / (args.steps * chunk * 1e-4) / args.neurons,
         }

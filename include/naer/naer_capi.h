@@ -219,9 +219,15 @@ NAER_API int naer_net_set_profiling(naer_net* net, int enable);
 NAER_API int naer_net_get_profile(naer_net* net, double* lif_ms, double* scatter_ms,
                                   uint64_t* launches);
 /* Finer split of the same device time (ms): [0] LIF, [1] wait for all LIF
- * blocks, [2] scatter, [3] Poisson draws of the next step, [4] wait for all
- * scatter blocks.  Measured by the first block of the step kernel. */
+ * blocks, [2] scatter of the delay-1 synapses (whole rows of STDP sources),
+ * [3] scatter of the remaining synapses of the previous step, overlapping
+ * the next LIF, [4] wait for all scatter blocks.  Measured by the first
+ * block of the step kernel. */
 NAER_API int naer_net_get_phases(naer_net* net, double* phase_ms5);
+/* CUDA-event durations (ms) of the launches issued while profiling: the
+ * Poisson-draw kernels and the persistent step kernels (and their count). */
+NAER_API int naer_net_get_launch_times(naer_net* net, double* drive_ms, double* step_kernel_ms,
+                                       uint64_t* step_kernel_launches);
 
 #ifdef __cplusplus
 }

@@ -138,6 +138,7 @@ PROTOTYPES = {
     "naer_net_set_profiling": [_vp, C.c_int],
     "naer_net_get_profile": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
     "naer_net_get_phases": [_vp, _vp],
+    "naer_net_get_launch_times": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
 }
 
 _lib = None

@@ -195,4 +195,73 @@ __global__ void k_pad_fill(const uint64_t* row_ptr, const uint64_t* len, uint32_
     }
 }
 
+// Delay-1 synapses of each row (valid entries only).
+__global__ void k_count_d1(const uint64_t* row_ptr, const uint64_t* len, uint32_t n, const uint8_t* dly,
+                           uint32_t* n1) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const uint64_t b = row_ptr[i], e = b + len[i];
+        uint32_t c = 0;
+        for (uint64_t j = b + lane; j < e; j += 32) c += dly[j] == 1 ? 1u : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+        if (lane == 0) n1[i] = c;
+    }
+}
+
+__global__ void k_row_pad_split(const uint64_t* len, const uint32_t* n1, uint32_t n, uint64_t* padded) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
+        if (i == n) {
+            padded[i] = 0;
+            continue;
+        }
+        const uint64_t a = n1[i], b = len[i] - n1[i];
+        padded[i] = (a + kRowAlign - 1) / kRowAlign * kRowAlign + (b + kRowAlign - 1) / kRowAlign * kRowAlign;
+    }
+}
+
+// Stable partition of row i into [delay-1 part | pad | other part | pad]:
+// one warp per row, ballots give every entry its place in its part.
+__global__ void k_partition_d1(const uint64_t* row_ptr, const uint64_t* len, const uint32_t* n1, uint32_t n,
+                               const uint64_t* row_ptr2, const uint32_t* tgt, const float* w, const uint8_t* dly,
+                               uint32_t* tgt2, float* w2, uint8_t* dly2, uint32_t* row_mid) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const uint64_t b = row_ptr[i], L = len[i];
+        const uint64_t o = row_ptr2[i], o_end = row_ptr2[i + 1];
+        const uint32_t a = n1[i];
+        const uint64_t mid = (a + kRowAlign - 1) / kRowAlign * kRowAlign;
+        uint64_t r1 = 0, r2 = 0;
+        for (uint64_t j0 = 0; j0 < L; j0 += 32) {
+            const uint64_t j = j0 + lane;
+            const bool valid = j < L;
+            const bool one = valid && dly[b + j] == 1;
+            const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, one);
+            const uint32_t m2 = __ballot_sync(0xFFFFFFFFu, valid && !one);
+            if (valid) {
+                const uint64_t q = one ? o + r1 + __popc(m1 & lt) : o + mid + r2 + __popc(m2 & lt);
+                tgt2[q] = tgt[b + j];
+                w2[q] = w[b + j];
+                dly2[q] = dly[b + j];
+            }
+            r1 += __popc(m1);
+            r2 += __popc(m2);
+        }
+        for (uint64_t q = o + a + lane; q < o + mid; q += 32) {
+            tgt2[q] = kTgtSentinel;
+            w2[q] = 0.0f;
+            dly2[q] = 1;
+        }
+        for (uint64_t q = o + mid + (L - a) + lane; q < o_end; q += 32) {
+            tgt2[q] = kTgtSentinel;
+            w2[q] = 0.0f;
+            dly2[q] = 1;
+        }
+        if (lane == 0) row_mid[i] = (uint32_t)mid;
+    }
+}
+
 }  // namespace naer

@@ -3,7 +3,10 @@
 // Row order of a source (the order the scatter visits synapses, which fixes
 // the deterministic aggregation order): connections in declaration order;
 // inside one connection, REF_BERNOULLI by ascending target, FIXED_OUTDEGREE
-// by draw index k, FIXED_INDEGREE by ascending (target, k).
+// by draw index k, FIXED_INDEGREE by ascending (target, k); finally a stable
+// partition puts the delay-1 synapses first.  In device memory the two parts
+// of a row each start on a 16-byte boundary (sentinel padding between and
+// after them); row_mid holds the offset of the second part.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -76,5 +79,11 @@ __global__ void k_cursor_advance(const uint32_t* cnt, uint32_t src_size, uint32_
                                  uint64_t* cursor);
 __global__ void k_pad_fill(const uint64_t* row_ptr, const uint64_t* len, uint32_t n, uint32_t* tgt,
                            float* w, uint8_t* dly);
+__global__ void k_count_d1(const uint64_t* row_ptr, const uint64_t* len, uint32_t n, const uint8_t* dly,
+                           uint32_t* n1);
+__global__ void k_row_pad_split(const uint64_t* len, const uint32_t* n1, uint32_t n, uint64_t* padded);
+__global__ void k_partition_d1(const uint64_t* row_ptr, const uint64_t* len, const uint32_t* n1, uint32_t n,
+                               const uint64_t* row_ptr2, const uint32_t* tgt, const float* w, const uint8_t* dly,
+                               uint32_t* tgt2, float* w2, uint8_t* dly2, uint32_t* row_mid);
 
 }  // namespace naer

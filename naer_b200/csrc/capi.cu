@@ -363,6 +363,14 @@ int naer_net_get_profile(naer_net* net, double* lif_ms, double* scatter_ms, uint
     });
 }
 
+int naer_net_get_launch_times(naer_net* net, double* drive_ms, double* step_kernel_ms,
+                              uint64_t* step_kernel_launches) {
+    return guarded([&] {
+        need_compiled(net);
+        net->eng->get_launch_times(drive_ms, step_kernel_ms, step_kernel_launches);
+    });
+}
+
 int naer_net_get_phases(naer_net* net, double* phase_ms5) {
     return guarded([&] {
         need_compiled(net);

@@ -126,6 +126,7 @@ Engine::~Engine() {
     f(d_ovf_part_);
     f(det_prefix_);
     f(d_raster_);
+    for (auto ev : timer_events_) cudaEventDestroy(ev);
     for (int i = 0; i < 2; ++i) {
         f(q_keys_[i]);
         f(q_vals_[i]);
@@ -324,15 +325,49 @@ void Engine::build(NetHost& n) {
     }
     k_pad_fill<<<grid_for(Ns, T, maxb), T, 0, st>>>(n.row_ptr, len, Ns, n.tgt, n.w, n.dly);
     NAER_CK(cudaGetLastError());
+    // canonical order: stable partition of every row, delay-1 synapses first,
+    // each part starting on a 16-byte boundary
+    {
+        uint32_t* n1 = static_cast<uint32_t*>(dalloc(Ns * 4ull));
+        k_count_d1<<<grid_for((uint64_t)Ns * 32, T, maxb), T, 0, st>>>(n.row_ptr, len, Ns, n.dly, n1);
+        uint64_t* padded2 = static_cast<uint64_t*>(dalloc((Ns + 1) * 8ull));
+        k_row_pad_split<<<grid_for(Ns + 1, T, maxb), T, 0, st>>>(len, n1, Ns, padded2);
+        uint64_t* row_ptr2 = static_cast<uint64_t*>(dalloc((Ns + 1) * 8ull));
+        with_cub_tmp(*this, [&](void* tmp, size_t& b) {
+            return cub::DeviceScan::ExclusiveSum(tmp, b, padded2, row_ptr2, (int)(Ns + 1), st);
+        });
+        uint64_t S2 = 0;
+        NAER_CK(cudaMemcpyAsync(&S2, row_ptr2 + Ns, 8, cudaMemcpyDeviceToHost, st));
+        NAER_CK(cudaStreamSynchronize(st));
+        uint32_t* tgt2 = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(S2, 4) * 4ull));
+        float* w2 = static_cast<float*>(dalloc(std::max<uint64_t>(S2, 4) * 4ull));
+        uint8_t* dly2 = static_cast<uint8_t*>(dalloc(std::max<uint64_t>(S2, 16)));
+        n.row_mid = static_cast<uint32_t*>(dalloc(Ns * 4ull));
+        k_partition_d1<<<grid_for((uint64_t)Ns * 32, T, maxb), T, 0, st>>>(
+            n.row_ptr, len, n1, Ns, row_ptr2, n.tgt, n.w, n.dly, tgt2, w2, dly2, n.row_mid);
+        NAER_CK(cudaGetLastError());
+        std::vector<uint64_t> hpad(Ns);
+        NAER_CK(cudaMemcpyAsync(hpad.data(), padded2, Ns * 8ull, cudaMemcpyDeviceToHost, st));
+        NAER_CK(cudaStreamSynchronize(st));
+        dfree(n.tgt, std::max<uint64_t>(S, 4) * 4ull);
+        dfree(n.w, std::max<uint64_t>(S, 4) * 4ull);
+        dfree(n.dly, std::max<uint64_t>(S, 16));
+        dfree(n.row_ptr, (Ns + 1) * 8ull);
+        dfree(padded2, (Ns + 1) * 8ull);
+        dfree(n1, Ns * 4ull);
+        n.tgt = tgt2;
+        n.w = w2;
+        n.dly = dly2;
+        n.row_ptr = row_ptr2;
+        n.synapses_padded = S2;
+        n.max_row_padded = 0;
+        for (uint64_t x : hpad) n.max_row_padded = std::max<uint64_t>(n.max_row_padded, x);
+    }
     std::vector<uint64_t> hlen(Ns);
     NAER_CK(cudaMemcpyAsync(hlen.data(), len, Ns * 8ull, cudaMemcpyDeviceToHost, st));
     NAER_CK(cudaStreamSynchronize(st));
     n.synapses = 0;
-    n.max_row_padded = 0;
-    for (uint64_t x : hlen) {
-        n.synapses += x;
-        n.max_row_padded = std::max<uint64_t>(n.max_row_padded, (x + kRowAlign - 1) / kRowAlign * kRowAlign);
-    }
+    for (uint64_t x : hlen) n.synapses += x;
     for (size_t ci = 0; ci < cnt.size(); ++ci)
         dfree(cnt[ci], std::max<uint64_t>(n.pops[n.conns[ci].src].size, 1) * 4ull);
     dfree(len, Ns * 8ull);
@@ -389,6 +424,7 @@ void Engine::build(NetHost& n) {
     d.ring = n.ring;
     d.drive = n.drive;
     d.row_ptr = n.row_ptr;
+    d.row_mid = n.row_mid;
     d.tgt = n.tgt;
     d.w = n.w;
     d.dly = n.dly;
@@ -425,6 +461,8 @@ void Engine::free_net(NetHost& n) {
     dfree(n.drive, (uint64_t)kDriveSlots * Ns);
     n.drive = nullptr;
     dfree(n.row_ptr, (Ns + 1) * 8ull);
+    dfree(n.row_mid, Ns * 4ull);
+    n.row_mid = nullptr;
     dfree(n.tgt, std::max<uint64_t>(S, 4) * 4ull);
     dfree(n.w, std::max<uint64_t>(S, 4) * 4ull);
     dfree(n.dly, std::max<uint64_t>(S, 16));
@@ -652,13 +690,53 @@ void Engine::launch_run(uint32_t steps) {
     NAER_CK(cudaMemsetAsync(&d_ctl_->bar_arrive, 0, sizeof(unsigned long long), stream_));
     void* args[] = {&eng_, &s0, &steps};
     const void* fn = use_smem_state_ ? (const void*)k_run<true> : (const void*)k_run<false>;
+    if (profiling_) NAER_CK(cudaEventRecord(timer_event(), stream_));
     NAER_CK(cudaLaunchCooperativeKernel(fn, dim3(lif_grid_), dim3(kLifThreads), args, scatter_smem_, stream_));
+    if (profiling_) {
+        NAER_CK(cudaEventRecord(timer_event(), stream_));
+        timer_kinds_.push_back(1);
+    }
     host_step_ += steps;
+}
+
+cudaEvent_t Engine::timer_event() {
+    cudaEvent_t e;
+    NAER_CK(cudaEventCreate(&e));
+    timer_events_.push_back(e);
+    return e;
+}
+
+// Sums the CUDA-event durations of the timed launches (pairs of events in
+// launch order: drive kernels and persistent step kernels).
+void Engine::resolve_timers() {
+    if (timer_events_.empty()) return;
+    NAER_CK(cudaStreamSynchronize(stream_));
+    size_t e = 0;
+    for (size_t i = 0; i < timer_kinds_.size(); ++i) {
+        float ms = 0;
+        NAER_CK(cudaEventElapsedTime(&ms, timer_events_[e], timer_events_[e + 1]));
+        e += 2;
+        if (timer_kinds_[i] == 0) {
+            drive_ms_ += ms;
+        } else {
+            run_ms_ += ms;
+            ++run_launches_;
+        }
+    }
+    for (auto ev : timer_events_) cudaEventDestroy(ev);
+    timer_events_.clear();
+    timer_kinds_.clear();
+    run_pairs_.clear();
 }
 
 void Engine::launch_drive(uint64_t s_first, uint32_t nsteps) {
     const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 16));
+    if (profiling_) NAER_CK(cudaEventRecord(timer_event(), stream_));
     k_drive<<<grid, kLifThreads, 0, stream_>>>(eng_, (unsigned long long)s_first, nsteps);
+    if (profiling_) {
+        NAER_CK(cudaEventRecord(timer_event(), stream_));
+        timer_kinds_.push_back(0);
+    }
     NAER_CK(cudaGetLastError());
 }
 
@@ -828,12 +906,23 @@ void Engine::clear_raster() {
 void Engine::set_profiling(bool on) {
     DeviceGuard g(device_);
     // the persistent kernel always times its phases; enabling resets the totals
+    resolve_timers();
     if (on) {
+        drive_ms_ = run_ms_ = 0;
+        run_launches_ = 0;
         sync();
         const unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         NAER_CK(cudaMemcpy(&d_ctl_->prof_lif_ns, z, sizeof(z), cudaMemcpyHostToDevice));
     }
     profiling_ = on;
+}
+
+void Engine::get_launch_times(double* drive_ms, double* run_ms, uint64_t* run_launches) {
+    DeviceGuard g(device_);
+    resolve_timers();
+    if (drive_ms) *drive_ms = drive_ms_;
+    if (run_ms) *run_ms = run_ms_;
+    if (run_launches) *run_launches = run_launches_;
 }
 
 void Engine::get_phases(double* ms5) {

@@ -56,6 +56,7 @@ struct NetHost {
     float* ring = nullptr;
     uint8_t* drive = nullptr;
     uint64_t* row_ptr = nullptr;
+    uint32_t* row_mid = nullptr;
     uint32_t* tgt = nullptr;
     float* w = nullptr;
     uint8_t* dly = nullptr;
@@ -102,6 +103,7 @@ public:
     void set_profiling(bool on);
     void get_profile(double* lif_ms, double* scatter_ms, uint64_t* launches);
     void get_phases(double* ms5);
+    void get_launch_times(double* drive_ms, double* run_ms, uint64_t* run_launches);
 
     uint64_t device_bytes() const { return bytes_; }
     uint64_t events_total();
@@ -164,6 +166,14 @@ private:
 
     bool profiling_ = false;
     bool use_smem_state_ = false;
+    // CUDA-event timing of launches while profiling (pairs in launch order)
+    std::vector<cudaEvent_t> timer_events_;
+    std::vector<int> timer_kinds_;  // 0 drive, 1 step kernel
+    std::vector<uint32_t> run_pairs_;
+    double drive_ms_ = 0, run_ms_ = 0;
+    uint64_t run_launches_ = 0;
+    cudaEvent_t timer_event();
+    void resolve_timers();
 };
 
 }  // namespace naer

@@ -57,6 +57,7 @@ struct NetDev {
     float* ring;            // [ring_slots][n_storage] delayed input
     uint8_t* drive;         // [kDriveSlots][n_storage] Poisson events per step (drive or own spikes)
     const uint64_t* row_ptr;  // [n_storage + 1], row starts multiple of kRowAlign
+    const uint32_t* row_mid;  // [n_storage] offset of the row's part of delay > 1 (multiple of kRowAlign)
     const uint32_t* tgt;    // [S] target storage index or kTgtSentinel
     float* w;               // [S] weight (written back by STDP)
     const uint8_t* dly;     // [S] delay in steps, 1..ring_slots-1
@@ -121,7 +122,7 @@ struct Ctl {
     unsigned long long prof_lif_ns;
     unsigned long long prof_scatter_ns;
     unsigned long long prof_steps;
-    unsigned long long prof_phase_ns[5];  // LIF, barrier 1, scatter items, Poisson draws, barrier 2
+    unsigned long long prof_phase_ns[5];  // LIF, barrier 1, early scatter, late scatter, barrier 2
     unsigned long long bar_arrive;  // grid barrier arrivals of the running launch
     unsigned int error;
     unsigned int pad_;

@@ -276,6 +276,10 @@ class Network:
         self.scatter_time = sc.value / 1e3
         ph = (C.c_double * 5)()
         capi.call("naer_net_get_phases", self._h, C.cast(ph, C.c_void_p))
-        names = ["lif", "lif_wait", "scatter", "poisson", "scatter_wait"]
+        names = ["lif", "lif_wait", "scatter_early", "scatter_late", "scatter_wait"]
+        dr, rk = C.c_double(), C.c_double()
+        nl = C.c_uint64()
+        capi.call("naer_net_get_launch_times", self._h, C.byref(dr), C.byref(rk), C.byref(nl))
         return {"lif_ms": lif.value, "scatter_ms": sc.value, "steps": n.value,
-                "phases_ms": {k: ph[i] for i, k in enumerate(names)}}
+                "phases_ms": {k: ph[i] for i, k in enumerate(names)},
+                "drive_kernel_ms": dr.value, "step_kernel_ms": rk.value, "step_kernel_launches": nl.value}

@@ -231,8 +231,9 @@ void layout(Net& net) {
 
 // Connectivity.  Rows: connections in declaration order; within a
 // connection REF_BERNOULLI by ascending target, FIXED_OUTDEGREE by draw k,
-// FIXED_INDEGREE by ascending (target, k).  Two passes: per-(connection,
-// source) counts, then the fill at prefix-sum offsets.
+// FIXED_INDEGREE by ascending (target, k); then a stable partition puts the
+// delay-1 synapses first.  Two passes: per-(connection, source) counts, then
+// the fill at prefix-sum offsets.
 void build_csr(Net& net) {
     const size_t nc = net.conns.size();
     std::vector<std::vector<uint32_t>> cnt(nc);
@@ -333,6 +334,27 @@ void build_csr(Net& net) {
                 }
         }
         for (uint32_t s = 0; s < sp.size; ++s) cur[sb + s] += cnt[ci][s];
+    }
+    // Canonical row order: a stable partition that puts the synapses of
+    // delay 1 (the ones the next step needs) before the others.
+    std::vector<uint32_t> tt;
+    std::vector<float> ww;
+    std::vector<uint8_t> dd;
+    for (uint32_t i = 0; i < net.n; ++i) {
+        const uint64_t b = net.row_ptr[i], e = net.row_ptr[i + 1];
+        tt.clear();
+        ww.clear();
+        dd.clear();
+        for (int pass = 0; pass < 2; ++pass)
+            for (uint64_t j = b; j < e; ++j)
+                if ((net.dly[j] == 1) == (pass == 0)) {
+                    tt.push_back(net.tgt[j]);
+                    ww.push_back(net.w[j]);
+                    dd.push_back(net.dly[j]);
+                }
+        std::copy(tt.begin(), tt.end(), net.tgt.begin() + b);
+        std::copy(ww.begin(), ww.end(), net.w.begin() + b);
+        std::copy(dd.begin(), dd.end(), net.dly.begin() + b);
     }
 }
 

@@ -116,10 +116,16 @@ def test_csr_rules(oracle_mod, rule):
         # each E target appears 7 times among the Poisson rows
         rows = tg[rp[base[0]]:rp[base[0] + 50]]
         assert np.all(np.bincount(rows - E0, minlength=120) == 7)
+    # canonical order: delay-1 synapses first (stable partition of the row)
+    for a in range(o.n):
+        dd = d[rp[a]:rp[a + 1]]
+        assert np.all(np.diff((dd != 1).astype(np.int8)) >= 0)
     if rule == capi.CONN_REF_BERNOULLI:
-        # within one connection, targets ascend (network.cl:88-105 in order)
+        # within one connection and delay class, targets ascend (network.cl:88-105 in order)
         for a in range(base[0], base[0] + 50):
-            assert np.all(np.diff(tg[rp[a]:rp[a + 1]].astype(np.int64)) > 0)
+            row_t, row_d = tg[rp[a]:rp[a + 1]].astype(np.int64), d[rp[a]:rp[a + 1]]
+            for cls in (row_d == 1, row_d != 1):
+                assert np.all(np.diff(row_t[cls]) > 0)
         frac = (rp[base[0] + 50] - rp[base[0]]) / (50 * 120)
         assert frac == pytest.approx(0.2, abs=0.03)
     # random weights (weight 0) lie in [wmin, wmax)
