@@ -169,6 +169,23 @@ NAER_API int naer_net_population_base(naer_net* net, uint32_t pop_id, uint32_t* 
  * steps (GRID) or nsteps windows (EVENT) and returns. */
 NAER_API int naer_net_step(naer_net* net, uint64_t nsteps);
 
+/* No counterpart in the reference.  naer_net_step for a network compiled
+ * with NAER_AGG_DETERMINISTIC (same kernels, same results), except that the
+ * step's scratch comes from one fixed 32 MiB device array inside the library,
+ * so the call never allocates or frees device memory.  It serves hosts that
+ * own every byte of device memory through their own pool and must not see a
+ * library call cudaMalloc (which also stalls the whole device) in the middle
+ * of a run.
+ * Limit: the network's worst-case step (all neurons spiking) must fit in the
+ * array; a larger one gets NAER_E_OVERFLOW from the first call, before any
+ * state changes.  NAER_E_STATE for an atomic-aggregation network.
+ * The first call on a network looks up the array's device address and
+ * partitions it; make that call before any stream capture begins.
+ * One array exists per device, shared by all networks on it: calls whose
+ * GPU work overlaps (networks on different streams or host threads) race on
+ * it and must be serialized by the caller. */
+NAER_API int naer_net_step_noalloc(naer_net* net, uint64_t nsteps);
+
 /* Network::finish (Network.cpp:258-265): blocks until the queue drains and
  * reports any device-side error. */
 NAER_API int naer_net_finish(naer_net* net);

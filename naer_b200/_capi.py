@@ -123,6 +123,7 @@ PROTOTYPES = {
     "naer_net_compile": [_vp],
     "naer_net_population_base": [_vp, C.c_uint32, _P(C.c_uint32)],
     "naer_net_step": [_vp, C.c_uint64],
+    "naer_net_step_noalloc": [_vp, C.c_uint64],
     "naer_net_finish": [_vp],
     "naer_net_get_time_us": [_vp, _P(C.c_uint64)],
     "naer_net_get_synapses": [_vp, _P(C.c_uint64)],

@@ -193,6 +193,13 @@ int naer_net_step(naer_net* net, uint64_t nsteps) {
     });
 }
 
+int naer_net_step_noalloc(naer_net* net, uint64_t nsteps) {
+    return guarded([&] {
+        need_compiled(net);
+        net->eng->run_fixed_scratch(nsteps);
+    });
+}
+
 int naer_net_finish(naer_net* net) {
     return guarded([&] {
         need_compiled(net);

@@ -842,6 +842,151 @@ void Engine::run_deterministic_step() {
     ++host_step_;
 }
 
+// ---------------------------------------------------------------------------
+// Deterministic steps with no allocation.  The aggregation's scratch (queue
+// sort, row-size scan, event sort and the CUB temporary storage) is carved
+// from one fixed device array of this library instead of engine-owned
+// buffers that grow with the step's event count.  Its size bounds the
+// networks the call accepts: the worst case of a step (every neuron spiking,
+// so every padded synapse emitting one event) must fit.  One array exists
+// per device and is shared by every engine on that device.
+
+constexpr size_t kFixedScratchBytes = 32ull << 20;  // 32 MiB
+static __device__ __align__(256) unsigned char g_fixed_scratch[kFixedScratchBytes];
+
+namespace {
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+}  // namespace
+
+// Looks up this device's copy of the arena and partitions it for the
+// installed networks.  Rejects a network whose worst-case step does not fit
+// before any of its state changes.
+void Engine::fixed_scratch_setup() {
+    if (aggregation_ != NAER_AGG_DETERMINISTIC)
+        throw Error(NAER_E_STATE, "the fixed-scratch step needs a network compiled with deterministic aggregation");
+    uint64_t neurons = 0, events = 0;
+    for (const NetHost* n : nets_) {
+        neurons += n->n_storage;
+        events += n->synapses_padded;
+    }
+    FixedScratch f;
+    f.q_max = std::max<uint64_t>(1, std::min<uint64_t>(queue_cap_, neurons));
+    f.e_max = std::max<uint64_t>(1, events);
+    f.q_bits = std::min(64, 32 + (int)bit_width(std::max<uint32_t>(eng_.n_nets, 1)));
+    f.e_bits = std::max<int>(1, (int)bit_width(total_ring_cells_));
+    if (f.e_max > 0x7FFFFFFFull)
+        throw Error(NAER_E_OVERFLOW, "network exceeds the fixed scratch: more than 2^31 padded synapses");
+    // partition sizes first, addresses after the fit is known
+    const size_t sizes[11] = {
+        (lif_grid_ + 1) * sizeof(uint32_t),
+        f.q_max * 8, f.q_max * 8, f.q_max * 4, f.q_max * 4, f.q_max * 4, f.q_max * 4,
+        f.e_max * 8, f.e_max * 8, f.e_max * 4, f.e_max * 4};
+    size_t offs[11], used = 0;
+    for (int i = 0; i < 11; ++i) {
+        offs[i] = used;
+        used = align256(used + sizes[i]);
+    }
+    // CUB temporary storage of the four operations (double-buffer sorts:
+    // the sorted copies live in the partitions above)
+    size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
+    {
+        cub::DoubleBuffer<unsigned long long> qk(nullptr, nullptr);
+        cub::DoubleBuffer<uint32_t> qv(nullptr, nullptr);
+        cub::DoubleBuffer<unsigned long long> ek(nullptr, nullptr);
+        cub::DoubleBuffer<float> ev(nullptr, nullptr);
+        NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b1, qk, qv, (int)f.q_max, 0, f.q_bits, stream_));
+        NAER_CK(cub::DeviceScan::ExclusiveSum(nullptr, b2, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                              (int)f.q_max, stream_));
+        NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b3, ek, ev, (int)f.e_max, 0, f.e_bits, stream_));
+        NAER_CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                              (int)(lif_grid_ + 1), stream_));
+    }
+    f.tmp_bytes = std::max({b1, b2, b3, b4});
+    const size_t need = used + f.tmp_bytes;
+    if (need > kFixedScratchBytes)
+        throw Error(NAER_E_OVERFLOW,
+                    "network too large for the fixed-scratch step: its worst-case step (" + std::to_string(neurons) +
+                        " neurons, " + std::to_string(events) + " padded synapses) needs " +
+                        std::to_string(need) + " bytes of scratch; the fixed arena holds " +
+                        std::to_string(kFixedScratchBytes) + " bytes");
+    void* base = nullptr;
+    NAER_CK(cudaGetSymbolAddress(&base, g_fixed_scratch));
+    unsigned char* a = static_cast<unsigned char*>(base);
+    f.prefix = reinterpret_cast<uint32_t*>(a + offs[0]);
+    f.q_keys[0] = reinterpret_cast<unsigned long long*>(a + offs[1]);
+    f.q_keys[1] = reinterpret_cast<unsigned long long*>(a + offs[2]);
+    f.q_vals[0] = reinterpret_cast<uint32_t*>(a + offs[3]);
+    f.q_vals[1] = reinterpret_cast<uint32_t*>(a + offs[4]);
+    f.q_sizes = reinterpret_cast<uint32_t*>(a + offs[5]);
+    f.q_offs = reinterpret_cast<uint32_t*>(a + offs[6]);
+    f.e_keys[0] = reinterpret_cast<unsigned long long*>(a + offs[7]);
+    f.e_keys[1] = reinterpret_cast<unsigned long long*>(a + offs[8]);
+    f.e_vals[0] = reinterpret_cast<float*>(a + offs[9]);
+    f.e_vals[1] = reinterpret_cast<float*>(a + offs[10]);
+    f.tmp = a + used;
+    // No partition has to start at zero: every word a step reads was
+    // written earlier in the same step.
+    f.ready = true;
+    fs_ = f;
+}
+
+void Engine::run_fixed_scratch(uint64_t nsteps) {
+    DeviceGuard g(device_);
+    if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
+    if (!fs_.ready) fixed_scratch_setup();
+    for (uint64_t i = 0; i < nsteps; ++i) run_fixed_scratch_step();
+}
+
+// The deterministic step of run_deterministic_step with the fixed arena's
+// partitions as scratch: same kernels, same order, same results.
+void Engine::run_fixed_scratch_step() {
+    cudaStream_t st = stream_;
+    const FixedScratch& f = fs_;
+    const uint32_t T = 256;
+    const uint32_t dgrid = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 16));
+    k_drive<<<dgrid, kLifThreads, 0, st>>>(eng_, (unsigned long long)host_step_, 1u);
+    k_lif<<<lif_grid_, kLifThreads, 0, st>>>(eng_);
+    const uint32_t qb = (uint32_t)(host_step_ & 1ull);
+    size_t b = f.tmp_bytes;
+    NAER_CK(cub::DeviceScan::ExclusiveSum(f.tmp, b, d_counts_[qb], f.prefix, (int)(lif_grid_ + 1), st));
+    NAER_CK(cudaMemcpyAsync(h_pinned_, f.prefix + lif_grid_, 4, cudaMemcpyDeviceToHost, st));
+    NAER_CK(cudaStreamSynchronize(st));
+    const uint32_t Q = h_pinned_[0];
+    if (Q > f.q_max) throw Error(NAER_E_OVERFLOW, "spike count exceeds the fixed scratch");
+    if (Q > 0) {
+        k_det_queue_keys<<<(Q + T - 1) / T, T, 0, st>>>(eng_, f.prefix, f.q_keys[0], f.q_vals[0], Q);
+        cub::DoubleBuffer<unsigned long long> qk(f.q_keys[0], f.q_keys[1]);
+        cub::DoubleBuffer<uint32_t> qv(f.q_vals[0], f.q_vals[1]);
+        b = f.tmp_bytes;
+        NAER_CK(cub::DeviceRadixSort::SortPairs(f.tmp, b, qk, qv, (int)Q, 0, f.q_bits, st));
+        const uint32_t* order = qv.Current();
+        k_det_row_sizes<<<(Q + T - 1) / T, T, 0, st>>>(eng_, order, Q, f.q_sizes);
+        b = f.tmp_bytes;
+        NAER_CK(cub::DeviceScan::ExclusiveSum(f.tmp, b, f.q_sizes, f.q_offs, (int)Q, st));
+        NAER_CK(cudaMemcpyAsync(h_pinned_, f.q_offs + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
+        NAER_CK(cudaMemcpyAsync(h_pinned_ + 1, f.q_sizes + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
+        NAER_CK(cudaStreamSynchronize(st));
+        const uint64_t E = (uint64_t)h_pinned_[0] + h_pinned_[1];
+        if (E > f.e_max) throw Error(NAER_E_OVERFLOW, "event count exceeds the fixed scratch");
+        k_det_raster<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + T - 1) / T, 1024)), T, 0, st>>>(eng_, order, Q);
+        if (E > 0) {
+            k_det_emit<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + 7) / 8, (uint32_t)sm_count_ * 8)),
+                         kScatterThreads, 0, st>>>(eng_, order, Q, f.q_offs, f.e_keys[0], f.e_vals[0]);
+            cub::DoubleBuffer<unsigned long long> ek(f.e_keys[0], f.e_keys[1]);
+            cub::DoubleBuffer<float> ev(f.e_vals[0], f.e_vals[1]);
+            b = f.tmp_bytes;
+            NAER_CK(cub::DeviceRadixSort::SortPairs(f.tmp, b, ek, ev, (int)E, 0, f.e_bits, st));
+            k_det_fold<<<(uint32_t)((E + T - 1) / T), T, 0, st>>>(d_nets_, eng_.n_nets, ek.Current(),
+                                                                  ev.Current(), (uint32_t)E);
+        }
+    } else {
+        k_det_raster<<<1, 32, 0, st>>>(eng_, nullptr, 0);
+    }
+    k_advance<<<1, 32, 0, st>>>(eng_);
+    NAER_CK(cudaGetLastError());
+    ++host_step_;
+}
+
 void Engine::sync() {
     DeviceGuard g(device_);
     NAER_CK(cudaStreamSynchronize(stream_));

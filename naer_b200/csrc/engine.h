@@ -91,6 +91,9 @@ public:
                  uint32_t aggregation);
 
     void run(uint64_t nsteps);
+    // Deterministic-aggregation steps whose scratch is the library's fixed
+    // device arena: no device memory is allocated or freed by the call.
+    void run_fixed_scratch(uint64_t nsteps);
     void sync();
     Ctl read_ctl();
     uint64_t host_step() const { return host_step_; }
@@ -163,6 +166,26 @@ private:
     void* cub_tmp_ = nullptr;
     size_t cub_tmp_bytes_ = 0;
     uint32_t* h_pinned_ = nullptr;  // small pinned staging
+
+    // partitions of the fixed scratch arena (set up by the first
+    // run_fixed_scratch call on this engine)
+    struct FixedScratch {
+        bool ready = false;
+        uint64_t q_max = 0, e_max = 0;
+        int q_bits = 64, e_bits = 64;
+        uint32_t* prefix = nullptr;
+        unsigned long long* q_keys[2] = {nullptr, nullptr};
+        uint32_t* q_vals[2] = {nullptr, nullptr};
+        uint32_t* q_sizes = nullptr;
+        uint32_t* q_offs = nullptr;
+        unsigned long long* e_keys[2] = {nullptr, nullptr};
+        float* e_vals[2] = {nullptr, nullptr};
+        void* tmp = nullptr;
+        size_t tmp_bytes = 0;
+    };
+    FixedScratch fs_{};
+    void fixed_scratch_setup();
+    void run_fixed_scratch_step();
 
     bool profiling_ = false;
     bool use_smem_state_ = false;
