@@ -332,7 +332,7 @@ def run_ours(args):
                                  + ", ".join(f"{k} {v / ph_tot:.0%}" for k, v in ph.items())},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": 2 * ((chunk + 15) // 16) * args.steps,
+            "gpu_launches": int(st1["kernel_launches"] - st0["kernel_launches"]),
             "clocks": clk,
             "spikes_per_s_sim": spikes / (args.steps * chunk * 1e-4) / args.neurons,
         }

@@ -129,6 +129,7 @@ typedef struct naer_stats {
     uint64_t device_bytes;      /* device memory held by the handle */
     uint32_t neurons;
     uint32_t ring_slots;
+    uint64_t kernel_launches;   /* launches of the library's own step kernels */
 } naer_stats;
 
 typedef struct naer_net naer_net;

@@ -96,6 +96,7 @@ class Stats(C.Structure):
         ("device_bytes", C.c_uint64),
         ("neurons", C.c_uint32),
         ("ring_slots", C.c_uint32),
+        ("kernel_launches", C.c_uint64),
     ]
 
 

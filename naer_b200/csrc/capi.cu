@@ -245,6 +245,7 @@ int naer_net_get_stats(naer_net* net, naer_stats* st) {
         st->device_bytes = net->eng->device_bytes();
         st->neurons = net->net.n_ids;
         st->ring_slots = net->net.ring_slots;
+        st->kernel_launches = net->eng->kernel_launches();
     });
 }
 

@@ -692,6 +692,7 @@ void Engine::launch_run(uint32_t steps) {
     const void* fn = use_smem_state_ ? (const void*)k_run<true> : (const void*)k_run<false>;
     if (profiling_) NAER_CK(cudaEventRecord(timer_event(), stream_));
     NAER_CK(cudaLaunchCooperativeKernel(fn, dim3(lif_grid_), dim3(kLifThreads), args, scatter_smem_, stream_));
+    ++launches_;
     if (profiling_) {
         NAER_CK(cudaEventRecord(timer_event(), stream_));
         timer_kinds_.push_back(1);
@@ -733,6 +734,7 @@ void Engine::launch_drive(uint64_t s_first, uint32_t nsteps) {
     const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 16));
     if (profiling_) NAER_CK(cudaEventRecord(timer_event(), stream_));
     k_drive<<<grid, kLifThreads, 0, stream_>>>(eng_, (unsigned long long)s_first, nsteps);
+    ++launches_;
     if (profiling_) {
         NAER_CK(cudaEventRecord(timer_event(), stream_));
         timer_kinds_.push_back(0);
@@ -798,6 +800,7 @@ void Engine::ensure_det_capacity(uint64_t events) {
 
 void Engine::run_deterministic_step() {
     cudaStream_t st = stream_;
+    uint64_t own_launches = 2;  // LIF, advance (launch_drive counts itself)
     if (!q_keys_[0]) ensure_det_capacity(1);
     const uint32_t T = 256;
     launch_drive(host_step_, 1);
@@ -814,6 +817,7 @@ void Engine::run_deterministic_step() {
         const int qbits = 32 + (int)bit_width(std::max<uint32_t>(eng_.n_nets, 1));
         NAER_CK(cub::DeviceRadixSort::SortPairs(cub_tmp_, b, q_keys_[0], q_keys_[1], q_vals_[0], q_vals_[1],
                                                 (int)Q, 0, std::min(qbits, 64), st));
+        own_launches += 3;  // queue keys, row sizes, raster
         k_det_row_sizes<<<(Q + T - 1) / T, T, 0, st>>>(eng_, q_vals_[1], Q, q_sizes_);
         b = cub_tmp_bytes_;
         NAER_CK(cub::DeviceScan::ExclusiveSum(cub_tmp_, b, q_sizes_, q_offs_, (int)Q, st));
@@ -824,6 +828,7 @@ void Engine::run_deterministic_step() {
         if (E > 0x7FFFFFFFull) throw Error(NAER_E_OVERFLOW, "more than 2^31 events in one step");
         k_det_raster<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + T - 1) / T, 1024)), T, 0, st>>>(eng_, q_vals_[1], Q);
         if (E > 0) {
+            own_launches += 2;  // emit, fold
             ensure_det_capacity(E);
             k_det_emit<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + 7) / 8, (uint32_t)sm_count_ * 8)),
                          kScatterThreads, 0, st>>>(eng_, q_vals_[1], Q, q_offs_, e_keys_[0], e_vals_[0]);
@@ -835,10 +840,12 @@ void Engine::run_deterministic_step() {
                                                                   e_vals_[1], (uint32_t)E);
         }
     } else {
+        ++own_launches;
         k_det_raster<<<1, 32, 0, st>>>(eng_, nullptr, 0);
     }
     k_advance<<<1, 32, 0, st>>>(eng_);
     NAER_CK(cudaGetLastError());
+    launches_ += own_launches;
     ++host_step_;
 }
 
@@ -941,6 +948,7 @@ void Engine::run_fixed_scratch(uint64_t nsteps) {
 // partitions as scratch: same kernels, same order, same results.
 void Engine::run_fixed_scratch_step() {
     cudaStream_t st = stream_;
+    uint64_t own_launches = 3;  // drive, LIF, advance
     const FixedScratch& f = fs_;
     const uint32_t T = 256;
     const uint32_t dgrid = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 16));
@@ -960,6 +968,7 @@ void Engine::run_fixed_scratch_step() {
         b = f.tmp_bytes;
         NAER_CK(cub::DeviceRadixSort::SortPairs(f.tmp, b, qk, qv, (int)Q, 0, f.q_bits, st));
         const uint32_t* order = qv.Current();
+        own_launches += 3;  // queue keys, row sizes, raster
         k_det_row_sizes<<<(Q + T - 1) / T, T, 0, st>>>(eng_, order, Q, f.q_sizes);
         b = f.tmp_bytes;
         NAER_CK(cub::DeviceScan::ExclusiveSum(f.tmp, b, f.q_sizes, f.q_offs, (int)Q, st));
@@ -970,6 +979,7 @@ void Engine::run_fixed_scratch_step() {
         if (E > f.e_max) throw Error(NAER_E_OVERFLOW, "event count exceeds the fixed scratch");
         k_det_raster<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + T - 1) / T, 1024)), T, 0, st>>>(eng_, order, Q);
         if (E > 0) {
+            own_launches += 2;  // emit, fold
             k_det_emit<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + 7) / 8, (uint32_t)sm_count_ * 8)),
                          kScatterThreads, 0, st>>>(eng_, order, Q, f.q_offs, f.e_keys[0], f.e_vals[0]);
             cub::DoubleBuffer<unsigned long long> ek(f.e_keys[0], f.e_keys[1]);
@@ -980,10 +990,12 @@ void Engine::run_fixed_scratch_step() {
                                                                   ev.Current(), (uint32_t)E);
         }
     } else {
+        ++own_launches;
         k_det_raster<<<1, 32, 0, st>>>(eng_, nullptr, 0);
     }
     k_advance<<<1, 32, 0, st>>>(eng_);
     NAER_CK(cudaGetLastError());
+    launches_ += own_launches;
     ++host_step_;
 }
 

@@ -109,6 +109,8 @@ public:
     void get_launch_times(double* drive_ms, double* run_ms, uint64_t* run_launches);
 
     uint64_t device_bytes() const { return bytes_; }
+    // launches of this library's own step kernels since creation
+    uint64_t kernel_launches() const { return launches_; }
     uint64_t events_total();
     uint64_t overflow_total();
 
@@ -152,6 +154,7 @@ private:
     uint32_t aggregation_ = NAER_AGG_ATOMIC;
     uint32_t lif_grid_ = 0, scatter_grid_ = 0;
     uint64_t host_step_ = 0;
+    uint64_t launches_ = 0;
     uint64_t total_ring_cells_ = 0;
 
 

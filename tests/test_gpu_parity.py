@@ -245,9 +245,11 @@ def test_atomic_persistent_path_exact_with_integer_weights(O):
     oracle, bit for bit, where reduction order cannot matter."""
     s = integer_weight_net()
     with S.build(s) as net:
+        l0 = net.stats()["kernel_launches"]
         for chunk in (1, 7, 300, 692):  # several launches of the persistent kernel
             net.run(chunk)
         net.finish()
+        assert net.stats()["kernel_launches"] > l0
         o = O.OracleNet(s, deterministic=True)
         o.run(1000)
         n = assert_same_run(net, o)
