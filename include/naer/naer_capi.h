@@ -142,7 +142,10 @@ NAER_API int naer_pop_params_default(uint32_t neuron_type, naer_pop_params* p);
 
 /* ---- one network: the plain form --------------------------------------- */
 
-/* Network::Network (Network.cpp:14-47): binds a device, creates the queue. */
+/* Network::Network (Network.cpp:14-47): binds a device, creates the queue.
+ * device = -1 makes a description-only handle (no device resources): it
+ * takes populations and connections but cannot be compiled; it is the
+ * input of naer_batch_add and naer_server_submit. */
 NAER_API int naer_net_create(int device, const naer_net_params* params, naer_net** out);
 
 /* Network::~Network (Network.cpp:49-75; the reference releases nothing). */
@@ -237,8 +240,9 @@ NAER_API int naer_net_set_profiling(naer_net* net, int enable);
 NAER_API int naer_net_get_profile(naer_net* net, double* lif_ms, double* scatter_ms,
                                   uint64_t* launches);
 /* Finer split of the same device time (ms): [0] LIF, [1] wait for all LIF
- * blocks, [2] scatter of the delay-1 synapses (whole rows of STDP sources),
- * [3] scatter of the remaining synapses of the previous step, overlapping
+ * blocks, [2] scatter (in the split pipeline, a compile-time option: of the
+ * delay-1 synapses and whole rows of STDP sources), [3] split pipeline
+ * only: scatter of the remaining synapses of the previous step, overlapping
  * the next LIF, [4] wait for all scatter blocks.  Measured by the first
  * block of the step kernel. */
 NAER_API int naer_net_get_phases(naer_net* net, double* phase_ms5);
@@ -246,6 +250,119 @@ NAER_API int naer_net_get_phases(naer_net* net, double* phase_ms5);
  * Poisson-draw kernels and the persistent step kernels (and their count). */
 NAER_API int naer_net_get_launch_times(naer_net* net, double* drive_ms, double* step_kernel_ms,
                                        uint64_t* step_kernel_launches);
+
+/* ---- batched form ------------------------------------------------------
+ * No counterpart in the reference (one Network per device queue there).
+ * Many independent networks of any sizes are packed, with offsets, into one
+ * engine: one set of persistent step launches advances all of them.  Each
+ * member keeps its own parameters, seeds and STDP switch; all start at step
+ * 0.  Deterministic aggregation gives every member the raster it gets
+ * alone, bit for bit. */
+typedef struct naer_batch naer_batch;
+
+/* Launch geometry of the step loop (results do not depend on it). */
+typedef struct naer_tuning {
+    uint32_t blocks_per_sm;   /* resident step-kernel blocks per SM, 0 = most that fit */
+    uint32_t launch_steps;    /* grid steps per persistent launch, 1..16 */
+    uint32_t scatter_split;   /* warps per spike, 0 = enough to cover the longest row */
+    uint32_t graph_launches;  /* persistent launches per CUDA-graph replay, 0 = no graph */
+    double best_us_per_step;  /* autotune: time of the chosen geometry */
+    double default_us_per_step; /* autotune: time of the default geometry */
+    uint32_t trials;          /* autotune: geometries timed */
+    uint32_t pad_;
+} naer_tuning;
+
+NAER_API int naer_batch_create(int device, uint32_t aggregation, uint64_t raster_capacity,
+                               naer_batch** out);
+NAER_API int naer_batch_destroy(naer_batch* batch);
+/* Copies a description-only network (naer_net_create(-1, ...)) into the
+ * batch; *member is its index.  Validates it. */
+NAER_API int naer_batch_add(naer_batch* batch, const naer_net* description, uint32_t* member);
+/* Builds every member on the device (connectivity generated there). */
+NAER_API int naer_batch_compile(naer_batch* batch);
+/* Asynchronous: nsteps grid steps of every member.  In atomic mode the
+ * launch sequence is recorded once as a CUDA graph and replayed. */
+NAER_API int naer_batch_step(naer_batch* batch, uint64_t nsteps);
+NAER_API int naer_batch_finish(naer_batch* batch);
+/* Times candidate geometries on the batch itself, trial_steps grid steps
+ * each (they advance the simulation), and keeps the fastest. */
+NAER_API int naer_batch_autotune(naer_batch* batch, uint32_t trial_steps, naer_tuning* out);
+NAER_API int naer_batch_set_tuning(naer_batch* batch, const naer_tuning* tuning);
+NAER_API int naer_batch_get_tuning(naer_batch* batch, naer_tuning* tuning);
+/* Raster records [first, first + capacity): member index, step, reference
+ * address within the member.  Ordered by step, then member, then address. */
+NAER_API int naer_batch_read_spikes(naer_batch* batch, uint64_t first, uint64_t capacity,
+                                    uint32_t* member, uint32_t* steps, uint32_t* ids, uint64_t* count);
+NAER_API int naer_batch_clear_spikes(naer_batch* batch);
+/* Whole-batch counters (synapses and neurons summed over members). */
+NAER_API int naer_batch_get_stats(naer_batch* batch, naer_stats* st);
+NAER_API int naer_batch_read_state(naer_batch* batch, uint32_t member, float* v, uint32_t* refractory);
+NAER_API int naer_batch_stream(naer_batch* batch, void** stream);
+
+/* ---- served form -------------------------------------------------------
+ * No counterpart in the reference.  A request loop on its own host thread:
+ * jobs (a description, a duration in grid steps) are admitted first come,
+ * first served while the device bytes of the admitted networks stay under
+ * the budget, built on the device and stepped together with the jobs
+ * already running (continuous batching: admission and retirement happen
+ * every chunk_steps grid steps, state stays on the device).  Each job's
+ * raster is collected per chunk and returned when the job ends.  All
+ * functions are thread-safe. */
+typedef struct naer_server naer_server;
+
+typedef struct naer_server_params {
+    uint64_t budget_bytes;     /* device bytes of admitted networks, at most */
+    uint64_t raster_capacity;  /* spike records per chunk (excess is dropped and counted) */
+    uint32_t chunk_steps;      /* grid steps between admission points */
+    uint32_t aggregation;      /* NAER_AGG_* for every job */
+    uint32_t max_jobs;         /* jobs stepped together, at most */
+    uint32_t pad_;
+} naer_server_params;
+
+#define NAER_JOB_QUEUED 0u
+#define NAER_JOB_RUNNING 1u
+#define NAER_JOB_DONE 2u
+#define NAER_JOB_FAILED 3u
+
+typedef struct naer_job_info {
+    uint32_t state;            /* NAER_JOB_* */
+    uint32_t pad_;
+    uint64_t duration;         /* grid steps asked for */
+    uint64_t steps_done;
+    uint64_t spikes;           /* raster records of the job (when done) */
+    uint64_t device_bytes;     /* device memory of its network while running */
+    double submit_s, admit_s, done_s;  /* seconds since the server started */
+} naer_job_info;
+
+typedef struct naer_server_stats {
+    uint64_t submitted, done, failed, running, queued;
+    uint64_t chunks, engine_steps, peak_bytes, bytes_in_use, raster_dropped;
+    double p50_ms, p99_ms, mean_ms;  /* job latency: submit to raster delivered */
+    double sims_per_s;               /* jobs done / (last done - first submit) */
+} naer_server_stats;
+
+NAER_API int naer_server_params_default(naer_server_params* p);
+NAER_API int naer_server_create(int device, const naer_server_params* params, naer_server** out);
+/* Stops the loop after the current chunk; unfinished jobs are abandoned. */
+NAER_API int naer_server_destroy(naer_server* server);
+/* Copies a description-only network; NAER_E_OVERFLOW if its estimated
+ * device bytes exceed the whole budget. */
+NAER_API int naer_server_submit(naer_server* server, const naer_net* description,
+                                uint64_t duration_steps, uint64_t* job);
+NAER_API int naer_server_job_info(naer_server* server, uint64_t job, naer_job_info* info);
+/* Error text of a failed job. */
+NAER_API int naer_server_job_error(naer_server* server, uint64_t job, char* buf, size_t len);
+/* *finished = 1 when the job (all jobs) ended within the timeout. */
+NAER_API int naer_server_wait(naer_server* server, uint64_t job, double timeout_s, int* finished);
+NAER_API int naer_server_drain(naer_server* server, double timeout_s, int* finished);
+/* Raster of a finished job, ordered by (step, address); steps count from
+ * the job's own step 0. */
+NAER_API int naer_server_read_spikes(naer_server* server, uint64_t job, uint64_t first,
+                                     uint64_t capacity, uint32_t* steps, uint32_t* ids,
+                                     uint64_t* count);
+/* Forgets a finished job and its raster. */
+NAER_API int naer_server_release(naer_server* server, uint64_t job);
+NAER_API int naer_server_get_stats(naer_server* server, naer_server_stats* st);
 
 #ifdef __cplusplus
 }

@@ -100,6 +100,53 @@ class Stats(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("blocks_per_sm", C.c_uint32),
+        ("launch_steps", C.c_uint32),
+        ("scatter_split", C.c_uint32),
+        ("graph_launches", C.c_uint32),
+        ("best_us_per_step", C.c_double),
+        ("default_us_per_step", C.c_double),
+        ("trials", C.c_uint32),
+        ("pad_", C.c_uint32),
+    ]
+
+
+class ServerParams(C.Structure):
+    _fields_ = [
+        ("budget_bytes", C.c_uint64),
+        ("raster_capacity", C.c_uint64),
+        ("chunk_steps", C.c_uint32),
+        ("aggregation", C.c_uint32),
+        ("max_jobs", C.c_uint32),
+        ("pad_", C.c_uint32),
+    ]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
+class JobInfo(C.Structure):
+    _fields_ = [
+        ("state", C.c_uint32),
+        ("pad_", C.c_uint32),
+        ("duration", C.c_uint64),
+        ("steps_done", C.c_uint64),
+        ("spikes", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+        ("submit_s", C.c_double),
+        ("admit_s", C.c_double),
+        ("done_s", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "done", "failed", "running", "queued", "chunks",
+                                           "engine_steps", "peak_bytes", "bytes_in_use", "raster_dropped")] + \
+               [(n, C.c_double) for n in ("p50_ms", "p99_ms", "mean_ms", "sims_per_s")]
+
+
 class NaerError(RuntimeError):
     """A non-zero status from the C ABI (message from naer_last_error)."""
 
@@ -141,6 +188,31 @@ PROTOTYPES = {
     "naer_net_get_profile": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
     "naer_net_get_phases": [_vp, _vp],
     "naer_net_get_launch_times": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
+    "naer_batch_create": [C.c_int, C.c_uint32, C.c_uint64, _P(_vp)],
+    "naer_batch_destroy": [_vp],
+    "naer_batch_add": [_vp, _vp, _P(C.c_uint32)],
+    "naer_batch_compile": [_vp],
+    "naer_batch_step": [_vp, C.c_uint64],
+    "naer_batch_finish": [_vp],
+    "naer_batch_autotune": [_vp, C.c_uint32, _P(Tuning)],
+    "naer_batch_set_tuning": [_vp, _P(Tuning)],
+    "naer_batch_get_tuning": [_vp, _P(Tuning)],
+    "naer_batch_read_spikes": [_vp, C.c_uint64, C.c_uint64, _vp, _vp, _vp, _P(C.c_uint64)],
+    "naer_batch_clear_spikes": [_vp],
+    "naer_batch_get_stats": [_vp, _P(Stats)],
+    "naer_batch_read_state": [_vp, C.c_uint32, _vp, _vp],
+    "naer_batch_stream": [_vp, _P(_vp)],
+    "naer_server_params_default": [_P(ServerParams)],
+    "naer_server_create": [C.c_int, _P(ServerParams), _P(_vp)],
+    "naer_server_destroy": [_vp],
+    "naer_server_submit": [_vp, _vp, C.c_uint64, _P(C.c_uint64)],
+    "naer_server_job_info": [_vp, C.c_uint64, _P(JobInfo)],
+    "naer_server_job_error": [_vp, C.c_uint64, C.c_char_p, C.c_size_t],
+    "naer_server_wait": [_vp, C.c_uint64, C.c_double, _P(C.c_int)],
+    "naer_server_drain": [_vp, C.c_double, _P(C.c_int)],
+    "naer_server_read_spikes": [_vp, C.c_uint64, C.c_uint64, C.c_uint64, _vp, _vp, _P(C.c_uint64)],
+    "naer_server_release": [_vp, C.c_uint64],
+    "naer_server_get_stats": [_vp, _P(ServerStats)],
 }
 
 _lib = None

@@ -6,13 +6,23 @@
 
 #include "../../include/naer/naer_capi.h"
 #include "engine.h"
+#include "forms.h"
 
 using naer::Error;
 
 struct naer_net {
-    std::unique_ptr<naer::Engine> eng;
+    std::unique_ptr<naer::Engine> eng;  // null for a description-only handle
     naer::NetHost net;
     uint32_t type_count[3] = {0, 0, 0};
+};
+
+struct naer_batch {
+    std::unique_ptr<naer::Batch> b;
+    uint32_t graph_launches = 16;
+};
+
+struct naer_server {
+    std::unique_ptr<naer::Server> s;
 };
 
 namespace {
@@ -118,9 +128,10 @@ int naer_net_create(int device, const naer_net_params* params, naer_net** out) {
         need(p.dt_us > 0, NAER_E_INVALID, "dt_us must be positive");
         if (p.mode == NAER_MODE_EVENT)
             throw Error(NAER_E_UNSUPPORTED, "event mode is not available in this build");
+        need(device >= -1, NAER_E_INVALID, "device index out of range");
         auto n = std::make_unique<naer_net>();
         n->net.params = p;
-        n->eng = std::make_unique<naer::Engine>(device);
+        if (device >= 0) n->eng = std::make_unique<naer::Engine>(device);
         *out = n.release();
     });
 }
@@ -172,6 +183,8 @@ int naer_net_compile(naer_net* net) {
     return guarded([&] {
         need(net != nullptr, NAER_E_INVALID, "null network handle");
         need(!net->net.compiled, NAER_E_STATE, "network already compiled");
+        need(net->eng != nullptr, NAER_E_STATE,
+             "description-only network (device -1): add it to a batch or submit it to a server");
         net->eng->build(net->net);
         const auto& P = net->net.params;
         net->eng->install({&net->net}, P.raster_capacity, P.record_spikes != 0, P.aggregation);
@@ -281,22 +294,35 @@ int naer_net_clear_spikes(naer_net* net) {
     });
 }
 
+namespace {
+
+void read_state_of(naer::Engine& eng, const naer::NetHost& n, float* v, uint32_t* refractory) {
+    std::vector<float> hv(n.n_storage);
+    std::vector<uint8_t> hr(n.n_storage);
+    eng.sync();
+    int prev = -1;
+    NAER_CK(cudaGetDevice(&prev));
+    NAER_CK(cudaSetDevice(eng.device()));
+    const cudaError_t e1 = cudaMemcpy(hv.data(), n.v, n.n_storage * 4ull, cudaMemcpyDeviceToHost);
+    const cudaError_t e2 = cudaMemcpy(hr.data(), n.refr, n.n_storage, cudaMemcpyDeviceToHost);
+    cudaSetDevice(prev);
+    NAER_CK(e1);
+    NAER_CK(e2);
+    for (const auto& p : n.pops) {
+        const bool lif = p.type != naer::kPOISSON;
+        for (uint32_t k = 0; k < p.size; ++k) {
+            if (v) v[p.id_base + k] = lif ? hv[p.storage_base + k] : 0.0f;
+            if (refractory) refractory[p.id_base + k] = lif ? hr[p.storage_base + k] : 0u;
+        }
+    }
+}
+
+}  // namespace
+
 int naer_net_read_state(naer_net* net, float* v, uint32_t* refractory) {
     return guarded([&] {
         need_compiled(net);
-        const auto& n = net->net;
-        std::vector<float> hv(n.n_storage);
-        std::vector<uint8_t> hr(n.n_storage);
-        net->eng->sync();
-        NAER_CK(cudaMemcpy(hv.data(), n.v, n.n_storage * 4ull, cudaMemcpyDeviceToHost));
-        NAER_CK(cudaMemcpy(hr.data(), n.refr, n.n_storage, cudaMemcpyDeviceToHost));
-        for (const auto& p : n.pops) {
-            const bool lif = p.type != naer::kPOISSON;
-            for (uint32_t k = 0; k < p.size; ++k) {
-                if (v) v[p.id_base + k] = lif ? hv[p.storage_base + k] : 0.0f;
-                if (refractory) refractory[p.id_base + k] = lif ? hr[p.storage_base + k] : 0u;
-            }
-        }
+        read_state_of(*net->eng, net->net, v, refractory);
     });
 }
 
@@ -384,6 +410,279 @@ int naer_net_get_phases(naer_net* net, double* phase_ms5) {
         need_compiled(net);
         need(phase_ms5 != nullptr, NAER_E_INVALID, "null argument");
         net->eng->get_phases(phase_ms5);
+    });
+}
+
+/* ---- batched form ---- */
+
+int naer_batch_create(int device, uint32_t aggregation, uint64_t raster_capacity, naer_batch** out) {
+    return guarded([&] {
+        need(out != nullptr, NAER_E_INVALID, "null output pointer");
+        *out = nullptr;
+        auto b = std::make_unique<naer_batch>();
+        b->b = std::make_unique<naer::Batch>(device, aggregation, raster_capacity, raster_capacity > 0);
+        *out = b.release();
+    });
+}
+
+int naer_batch_destroy(naer_batch* batch) {
+    if (!batch) return NAER_OK;
+    return guarded([&] {
+        naer::Batch& b = *batch->b;
+        if (b.compiled()) {
+            b.engine().sync();
+            for (size_t i = 0; i < b.size(); ++i) b.engine().free_net(b.member((uint32_t)i));
+        }
+        delete batch;
+    });
+}
+
+int naer_batch_add(naer_batch* batch, const naer_net* description, uint32_t* member) {
+    return guarded([&] {
+        need(batch && description, NAER_E_INVALID, "null argument");
+        const uint32_t m = batch->b->add(description->net);
+        if (member) *member = m;
+    });
+}
+
+int naer_batch_compile(naer_batch* batch) {
+    return guarded([&] {
+        need(batch != nullptr, NAER_E_INVALID, "null batch handle");
+        batch->b->compile();
+    });
+}
+
+int naer_batch_step(naer_batch* batch, uint64_t nsteps) {
+    return guarded([&] {
+        need(batch != nullptr, NAER_E_INVALID, "null batch handle");
+        batch->b->step(nsteps, batch->graph_launches);
+    });
+}
+
+int naer_batch_finish(naer_batch* batch) {
+    return guarded([&] {
+        need(batch != nullptr && batch->b->compiled(), NAER_E_STATE, "batch is not compiled");
+        batch->b->engine().sync();
+        const naer::Ctl c = batch->b->engine().read_ctl();
+        if (c.error) throw Error(NAER_E_CUDA, "device reported error flag " + std::to_string(c.error));
+    });
+}
+
+static void fill_tuning(naer_tuning* out, const naer::Tuning& t, uint32_t graph_launches) {
+    std::memset(out, 0, sizeof(*out));
+    out->blocks_per_sm = t.blocks_per_sm;
+    out->launch_steps = t.launch_steps;
+    out->scatter_split = t.scatter_split;
+    out->graph_launches = graph_launches;
+}
+
+int naer_batch_autotune(naer_batch* batch, uint32_t trial_steps, naer_tuning* out) {
+    return guarded([&] {
+        need(batch != nullptr, NAER_E_INVALID, "null batch handle");
+        const naer::TuneResult r = batch->b->autotune(trial_steps);
+        if (out) {
+            fill_tuning(out, r.best, batch->graph_launches);
+            out->best_us_per_step = r.best_us_per_step;
+            out->default_us_per_step = r.default_us_per_step;
+            out->trials = r.trials;
+        }
+    });
+}
+
+int naer_batch_set_tuning(naer_batch* batch, const naer_tuning* tuning) {
+    return guarded([&] {
+        need(batch && tuning, NAER_E_INVALID, "null argument");
+        need(batch->b->compiled(), NAER_E_STATE, "batch is not compiled");
+        naer::Tuning t;
+        t.blocks_per_sm = tuning->blocks_per_sm;
+        t.launch_steps = tuning->launch_steps;
+        t.scatter_split = tuning->scatter_split;
+        batch->b->engine().set_tuning(t);
+        batch->graph_launches = tuning->graph_launches;
+    });
+}
+
+int naer_batch_get_tuning(naer_batch* batch, naer_tuning* tuning) {
+    return guarded([&] {
+        need(batch && tuning, NAER_E_INVALID, "null argument");
+        fill_tuning(tuning, batch->b->engine().tuning(), batch->graph_launches);
+    });
+}
+
+int naer_batch_read_spikes(naer_batch* batch, uint64_t first, uint64_t capacity, uint32_t* member,
+                           uint32_t* steps, uint32_t* ids, uint64_t* count) {
+    return guarded([&] {
+        need(batch && count && (capacity == 0 || (steps && ids)), NAER_E_INVALID, "null argument");
+        *count = batch->b->read_spikes(first, capacity, member, steps, ids);
+    });
+}
+
+int naer_batch_clear_spikes(naer_batch* batch) {
+    return guarded([&] {
+        need(batch != nullptr && batch->b->compiled(), NAER_E_STATE, "batch is not compiled");
+        batch->b->engine().clear_raster();
+    });
+}
+
+int naer_batch_get_stats(naer_batch* batch, naer_stats* st) {
+    return guarded([&] {
+        need(batch && st, NAER_E_INVALID, "null argument");
+        naer::Batch& b = *batch->b;
+        need(b.compiled(), NAER_E_STATE, "batch is not compiled");
+        naer::Engine& eng = b.engine();
+        const naer::Ctl c = eng.read_ctl();
+        std::memset(st, 0, sizeof(*st));
+        st->step = c.step;
+        st->events = eng.events_total();
+        st->spikes = c.raster_next;
+        st->raster_dropped = c.raster_dropped;
+        st->stdp_hist_overflow = eng.overflow_total();
+        st->device_bytes = eng.device_bytes();
+        for (size_t i = 0; i < b.size(); ++i) {
+            st->synapses += b.member((uint32_t)i).synapses;
+            st->neurons += b.member((uint32_t)i).n_ids;
+            st->ring_slots = std::max(st->ring_slots, b.member((uint32_t)i).ring_slots);
+        }
+        st->kernel_launches = eng.kernel_launches();
+    });
+}
+
+int naer_batch_read_state(naer_batch* batch, uint32_t member, float* v, uint32_t* refractory) {
+    return guarded([&] {
+        need(batch != nullptr, NAER_E_INVALID, "null batch handle");
+        need(batch->b->compiled(), NAER_E_STATE, "batch is not compiled");
+        need(member < batch->b->size(), NAER_E_INVALID, "unknown member");
+        read_state_of(batch->b->engine(), batch->b->member(member), v, refractory);
+    });
+}
+
+int naer_batch_stream(naer_batch* batch, void** stream) {
+    return guarded([&] {
+        need(batch && stream, NAER_E_INVALID, "null argument");
+        *stream = (void*)batch->b->engine().stream();
+    });
+}
+
+/* ---- served form ---- */
+
+int naer_server_params_default(naer_server_params* p) {
+    if (!p) return fail(NAER_E_INVALID, "null pointer");
+    std::memset(p, 0, sizeof(*p));
+    p->budget_bytes = 150ull * 1000 * 1000 * 1000;
+    p->raster_capacity = 1ull << 24;
+    p->chunk_steps = 256;
+    p->aggregation = NAER_AGG_ATOMIC;
+    p->max_jobs = 1024;
+    return NAER_OK;
+}
+
+int naer_server_create(int device, const naer_server_params* params, naer_server** out) {
+    return guarded([&] {
+        need(out != nullptr, NAER_E_INVALID, "null output pointer");
+        *out = nullptr;
+        naer_server_params p;
+        if (params) p = *params; else naer_server_params_default(&p);
+        naer::ServerParams sp;
+        sp.budget_bytes = p.budget_bytes;
+        sp.raster_capacity = p.raster_capacity;
+        sp.chunk_steps = p.chunk_steps;
+        sp.aggregation = p.aggregation;
+        sp.max_jobs = p.max_jobs;
+        auto h = std::make_unique<naer_server>();
+        h->s = std::make_unique<naer::Server>(device, sp);
+        *out = h.release();
+    });
+}
+
+int naer_server_destroy(naer_server* server) {
+    if (!server) return NAER_OK;
+    return guarded([&] { delete server; });
+}
+
+int naer_server_submit(naer_server* server, const naer_net* description, uint64_t duration_steps,
+                       uint64_t* job) {
+    return guarded([&] {
+        need(server && description && job, NAER_E_INVALID, "null argument");
+        *job = server->s->submit(description->net, duration_steps);
+    });
+}
+
+int naer_server_job_info(naer_server* server, uint64_t job, naer_job_info* info) {
+    return guarded([&] {
+        need(server && info, NAER_E_INVALID, "null argument");
+        const naer::JobInfo j = server->s->info(job);
+        std::memset(info, 0, sizeof(*info));
+        info->state = j.state;
+        info->duration = j.duration;
+        info->steps_done = j.steps_done;
+        info->spikes = j.spikes;
+        info->device_bytes = j.device_bytes;
+        info->submit_s = j.submit_s;
+        info->admit_s = j.admit_s;
+        info->done_s = j.done_s;
+    });
+}
+
+int naer_server_job_error(naer_server* server, uint64_t job, char* buf, size_t len) {
+    return guarded([&] {
+        need(server && buf && len > 0, NAER_E_INVALID, "null argument");
+        const naer::JobInfo j = server->s->info(job);
+        const size_t n = std::min(len - 1, j.error.size());
+        std::memcpy(buf, j.error.data(), n);
+        buf[n] = '\0';
+    });
+}
+
+int naer_server_wait(naer_server* server, uint64_t job, double timeout_s, int* finished) {
+    return guarded([&] {
+        need(server != nullptr, NAER_E_INVALID, "null server handle");
+        const bool ok = server->s->wait(job, timeout_s);
+        if (finished) *finished = ok ? 1 : 0;
+    });
+}
+
+int naer_server_drain(naer_server* server, double timeout_s, int* finished) {
+    return guarded([&] {
+        need(server != nullptr, NAER_E_INVALID, "null server handle");
+        const bool ok = server->s->drain(timeout_s);
+        if (finished) *finished = ok ? 1 : 0;
+    });
+}
+
+int naer_server_read_spikes(naer_server* server, uint64_t job, uint64_t first, uint64_t capacity,
+                            uint32_t* steps, uint32_t* ids, uint64_t* count) {
+    return guarded([&] {
+        need(server && count && (capacity == 0 || (steps && ids)), NAER_E_INVALID, "null argument");
+        *count = server->s->read_spikes(job, first, capacity, steps, ids);
+    });
+}
+
+int naer_server_release(naer_server* server, uint64_t job) {
+    return guarded([&] {
+        need(server != nullptr, NAER_E_INVALID, "null server handle");
+        server->s->release(job);
+    });
+}
+
+int naer_server_get_stats(naer_server* server, naer_server_stats* st) {
+    return guarded([&] {
+        need(server && st, NAER_E_INVALID, "null argument");
+        const naer::ServerStats s = server->s->stats();
+        std::memset(st, 0, sizeof(*st));
+        st->submitted = s.submitted;
+        st->done = s.done;
+        st->failed = s.failed;
+        st->running = s.running;
+        st->queued = s.queued;
+        st->chunks = s.chunks;
+        st->engine_steps = s.engine_steps;
+        st->peak_bytes = s.peak_bytes;
+        st->bytes_in_use = s.bytes_in_use;
+        st->raster_dropped = s.raster_dropped;
+        st->p50_ms = s.p50_ms;
+        st->p99_ms = s.p99_ms;
+        st->mean_ms = s.mean_ms;
+        st->sims_per_s = s.sims_per_s;
     });
 }
 

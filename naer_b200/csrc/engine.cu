@@ -136,6 +136,7 @@ Engine::~Engine() {
     f(q_sizes_);
     f(q_offs_);
     f(cub_tmp_);
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (h_pinned_) cudaFreeHost(h_pinned_);
     cudaStreamDestroy(stream_);
     if (prev >= 0) cudaSetDevice(prev);
@@ -209,6 +210,44 @@ static void layout(NetHost& n) {
     }
     if (P.stdp_enabled && P.stdp_history == 0)
         throw Error(NAER_E_INVALID, "stdp_history must be at least 1");
+}
+
+// Device bytes of a built network, from its description: padded synapse
+// arrays (each row padded to 4 entries in each of its two delay classes),
+// row pointers, neuron state, ring, drive slots and plasticity state.  The
+// Bernoulli rule's count is its mean plus six standard deviations.
+uint64_t estimate_device_bytes(const NetHost& description) {
+    NetHost n;
+    n.params = description.params;
+    n.pops = description.pops;
+    n.conns = description.conns;
+    layout(n);
+    double syn = 0;
+    uint64_t rows = 0;
+    for (const auto& c : n.conns) {
+        const double src = n.pops[c.src].size, dst = n.pops[c.dst].size;
+        const auto& sp = c.spec;
+        if (sp.rule == NAER_CONN_REF_BERNOULLI) {
+            const double m = sp.probability * src * dst;
+            syn += m + 6.0 * std::sqrt(std::max(m, 1.0));
+        } else if (sp.rule == NAER_CONN_FIXED_OUTDEGREE) {
+            syn += (double)sp.degree * src;
+        } else {
+            syn += (double)sp.degree * dst;
+        }
+        rows += n.pops[c.src].size;
+    }
+    const uint64_t Ns = n.n_storage;
+    uint64_t b = (uint64_t)std::ceil(syn) * 9ull + (rows + Ns) * 6ull * 9ull;  // entries + padding
+    b += (Ns + 1) * 8ull + Ns * 4ull;                                          // row_ptr, row_mid
+    b += Ns * (4ull + 1ull + kDriveSlots + 4ull * n.ring_slots);                // V, refr, drive, ring
+    if (n.params.stdp_enabled && n.n_plastic) {
+        const uint64_t Np = n.n_plastic;
+        b += Np * (16ull + 4ull * n.params.stdp_history);
+        const double tmax = std::max(n.params.tau_plus_ms, n.params.tau_minus_ms) * 1000.0;
+        b += 8ull * (uint64_t)std::min<double>(std::ceil(104.0 * tmax / n.params.dt_us) + 1.0, 1 << 24);
+    }
+    return b;
 }
 
 static ConnBuild make_cb(const NetHost& n, const ConnSpec& c) {
@@ -436,6 +475,7 @@ void Engine::build(NetHost& n) {
     d.e_plus = n.e_plus;
     d.e_minus = n.e_minus;
     d.start_step = 0;
+    d.end_step = ~0ull;
     d.n_storage = Ns;
     d.ring_slots = n.ring_slots;
     d.dt_us = P.dt_us;
@@ -493,13 +533,18 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
                      uint32_t aggregation) {
     DeviceGuard g(device_);
     NAER_CK(cudaStreamSynchronize(stream_));
+    drop_graph();
     nets_ = nets;
     aggregation_ = aggregation;
+    inst_raster_cap_ = raster_capacity;
+    inst_record_ = record;
     std::vector<PopDev> pops;
     std::vector<ChunkDev> chunks;
     h_nets_.clear();
+    id_offsets_.clear();
     uint64_t key_base = 0;
     uint64_t qcap = 0;
+    uint64_t id_off = 0;
     for (uint32_t ni = 0; ni < nets.size(); ++ni) {
         NetHost& n = *nets[ni];
         NetDev d = n.dev;
@@ -507,6 +552,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
         key_base += (uint64_t)n.ring_slots * n.n_storage;
         h_nets_.push_back(d);
         qcap += n.n_storage;
+        id_offsets_.push_back((uint32_t)id_off);
         const auto& P = n.params;
         for (uint32_t pi : n.pop_order) {
             const PopSpec& ps = n.pops[pi];
@@ -516,7 +562,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
             pd.type = ps.type;
             pd.storage_base = ps.storage_base;
             pd.size = ps.size;
-            pd.id_base = ps.id_base;
+            pd.id_base = (uint32_t)id_off + ps.id_base;  // raster ids are engine-global
             if (ps.type == kPOISSON) {
                 pd.rate_hz = (double)ps.prm.rate_hz;
                 pd.rng_seed = P.poisson_seed;
@@ -540,6 +586,8 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
             for (uint32_t f = ps.storage_base; f < ps.storage_base + ps.size; f += kLifChunk)
                 chunks.push_back(ChunkDev{pidx, f, ps.storage_base + ps.size, ni});
         }
+        id_off += n.n_ids;
+        if (id_off > 0xFFFFFFFFull) throw Error(NAER_E_OVERFLOW, "more than 2^32 neuron addresses in one engine");
     }
     total_ring_cells_ = key_base;
     if (qcap > 0xFFFFFFFFull) throw Error(NAER_E_OVERFLOW, "more than 2^32 neurons in one engine");
@@ -578,7 +626,8 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     NAER_CK(cudaFuncSetAttribute(k_run<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_smem_optin));
     use_smem_state_ = false;
     lif_grid_ = 0;
-    for (int bps = 4; bps >= 1 && !use_smem_state_; --bps) {
+    const int bps_hi = tuning_.blocks_per_sm ? (int)std::min<uint32_t>(tuning_.blocks_per_sm, 4) : 4;
+    for (int bps = bps_hi; bps >= 1 && !use_smem_state_; --bps) {
         const uint32_t grid = (uint32_t)bps * sm_count_;
         const uint32_t own = std::max<uint32_t>(1, (eng_.n_chunks + grid - 1) / grid);
         const size_t smem = run_smem_bytes(grid, own, true);
@@ -596,7 +645,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
         const size_t smem_bound = run_smem_bytes((uint32_t)sm_count_ * 4, 1, false);
         NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_run<false>, kLifThreads, smem_bound));
         if (occ < 1) throw Error(NAER_E_CUDA, "the step kernel cannot be resident on this device");
-        lif_grid_ = (uint32_t)std::min(occ, 4) * sm_count_;
+        lif_grid_ = (uint32_t)std::min(occ, bps_hi) * sm_count_;
         scatter_smem_ = run_smem_bytes(lif_grid_, 1, false);
     }
     scatter_grid_ = lif_grid_;
@@ -650,6 +699,25 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     for (NetHost* n : nets) max_row = std::max<uint64_t>(max_row, n->max_row_padded);
     eng_.scatter_split =
         (uint32_t)std::min<uint64_t>(16, std::max<uint64_t>(1, (max_row + kScatterPiece - 1) / kScatterPiece));
+    if (tuning_.scatter_split) eng_.scatter_split = std::min<uint32_t>(tuning_.scatter_split, 64);
+}
+
+void Engine::set_tuning(const Tuning& t) {
+    Tuning v = t;
+    if (v.launch_steps == 0 || v.launch_steps > kDriveSlots)
+        throw Error(NAER_E_INVALID, "launch_steps must be in 1..16");
+    if (v.blocks_per_sm > 4) throw Error(NAER_E_INVALID, "blocks_per_sm must be in 0..4");
+    tuning_ = v;
+    if (!nets_.empty()) install(std::vector<NetHost*>(nets_), inst_raster_cap_, inst_record_, aggregation_);
+}
+
+void Engine::drop_graph() {
+    if (graph_exec_) {
+        NAER_CK(cudaStreamSynchronize(stream_));
+        NAER_CK(cudaGraphExecDestroy(graph_exec_));
+        graph_exec_ = nullptr;
+        graph_launches_ = 0;
+    }
 }
 
 void Engine::regrow(void*& p, size_t& have, size_t need) {
@@ -685,19 +753,38 @@ uint64_t Engine::overflow_total() {
 // ---------------------------------------------------------------------------
 // step loop
 
-void Engine::launch_run(uint32_t steps) {
-    unsigned long long s0 = host_step_;
+void Engine::launch_run(uint32_t steps) { launch_run_ex(steps, false); }
+
+// One persistent launch.  from_ctl: the kernel takes its first step from
+// Ctl::step (launches recorded in a CUDA graph); the cooperative attribute
+// of cudaLaunchKernelEx keeps it capturable.
+void Engine::launch_run_ex(uint32_t steps, bool from_ctl) {
+    unsigned long long s0 = from_ctl ? kStepFromCtl : host_step_;
     NAER_CK(cudaMemsetAsync(&d_ctl_->bar_arrive, 0, sizeof(unsigned long long), stream_));
-    void* args[] = {&eng_, &s0, &steps};
-    const void* fn = use_smem_state_ ? (const void*)k_run<true> : (const void*)k_run<false>;
-    if (profiling_) NAER_CK(cudaEventRecord(timer_event(), stream_));
-    NAER_CK(cudaLaunchCooperativeKernel(fn, dim3(lif_grid_), dim3(kLifThreads), args, scatter_smem_, stream_));
-    ++launches_;
-    if (profiling_) {
+    const bool timed = profiling_ && !from_ctl;
+    if (timed) NAER_CK(cudaEventRecord(timer_event(), stream_));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(lif_grid_);
+    cfg.blockDim = dim3(kLifThreads);
+    cfg.dynamicSmemBytes = scatter_smem_;
+    cfg.stream = stream_;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (use_smem_state_)
+        NAER_CK(cudaLaunchKernelEx(&cfg, k_run<true>, eng_, s0, steps));
+    else
+        NAER_CK(cudaLaunchKernelEx(&cfg, k_run<false>, eng_, s0, steps));
+    if (timed) {
         NAER_CK(cudaEventRecord(timer_event(), stream_));
         timer_kinds_.push_back(1);
     }
-    host_step_ += steps;
+    if (!from_ctl) {
+        ++launches_;
+        host_step_ += steps;
+    }
 }
 
 cudaEvent_t Engine::timer_event() {
@@ -732,10 +819,11 @@ void Engine::resolve_timers() {
 
 void Engine::launch_drive(uint64_t s_first, uint32_t nsteps) {
     const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 16));
-    if (profiling_) NAER_CK(cudaEventRecord(timer_event(), stream_));
+    const bool from_ctl = s_first == kStepFromCtl;
+    if (profiling_ && !from_ctl) NAER_CK(cudaEventRecord(timer_event(), stream_));
     k_drive<<<grid, kLifThreads, 0, stream_>>>(eng_, (unsigned long long)s_first, nsteps);
-    ++launches_;
-    if (profiling_) {
+    if (!from_ctl) ++launches_;
+    if (profiling_ && !from_ctl) {
         NAER_CK(cudaEventRecord(timer_event(), stream_));
         timer_kinds_.push_back(0);
     }
@@ -752,12 +840,56 @@ void Engine::run(uint64_t nsteps) {
     // Poisson counts of a chunk of steps are drawn first (full occupancy),
     // then the persistent kernel simulates the chunk
     while (nsteps > 0) {
-        const uint32_t n = (uint32_t)std::min<uint64_t>(nsteps, kDriveSlots);
+        const uint32_t n = (uint32_t)std::min<uint64_t>(nsteps, tuning_.launch_steps);
         launch_drive(host_step_, n);
         launch_run(n);
         nsteps -= n;
     }
     NAER_CK(cudaGetLastError());
+}
+
+uint64_t Engine::run_graph(uint64_t nsteps, uint32_t graph_launches) {
+    DeviceGuard g(device_);
+    if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
+    if (aggregation_ == NAER_AGG_DETERMINISTIC || graph_launches == 0) {
+        run(nsteps);
+        return 0;
+    }
+    const uint32_t L = tuning_.launch_steps;
+    const uint64_t per = (uint64_t)L * graph_launches;
+    if (graph_exec_ && graph_launches_ != graph_launches) drop_graph();
+    if (!graph_exec_ && nsteps >= per) {
+        // record drive + step launches that read their first step from Ctl
+        NAER_CK(cudaStreamSynchronize(stream_));
+        NAER_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        cudaError_t err = cudaSuccess;
+        try {
+            for (uint32_t i = 0; i < graph_launches; ++i) {
+                launch_drive(kStepFromCtl, L);
+                launch_run_ex(L, true);
+            }
+        } catch (...) {
+            cudaGraph_t gdrop = nullptr;
+            cudaStreamEndCapture(stream_, &gdrop);
+            if (gdrop) cudaGraphDestroy(gdrop);
+            throw;
+        }
+        cudaGraph_t graph = nullptr;
+        err = cudaStreamEndCapture(stream_, &graph);
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&graph_exec_, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        NAER_CK(err);
+        graph_launches_ = graph_launches;
+    }
+    uint64_t done = 0;
+    while (graph_exec_ && nsteps - done >= per) {
+        NAER_CK(cudaGraphLaunch(graph_exec_, stream_));
+        host_step_ += per;
+        launches_ += 2ull * graph_launches;
+        done += per;
+    }
+    run(nsteps - done);
+    return done;
 }
 
 void Engine::ensure_det_capacity(uint64_t events) {

@@ -73,6 +73,19 @@ struct NetHost {
     NetDev dev{};
 };
 
+// Device bytes a network will hold once built (synapse arrays, state, ring,
+// drive slots, plasticity state), from its description alone.  Also
+// validates the description (the checks compile makes).
+uint64_t estimate_device_bytes(const NetHost& description);
+
+// Launch geometry of the persistent step loop (all choices leave the
+// simulated results unchanged).
+struct Tuning {
+    uint32_t blocks_per_sm = 0;            // resident step-kernel blocks per SM (0 = most that fit)
+    uint32_t launch_steps = kDriveSlots;   // grid steps per persistent launch (1..kDriveSlots)
+    uint32_t scatter_split = 0;            // warps per spike (0 = enough to cover the longest row)
+};
+
 class Engine {
 public:
     explicit Engine(int device);
@@ -91,6 +104,18 @@ public:
                  uint32_t aggregation);
 
     void run(uint64_t nsteps);
+    // Atomic mode: the same steps, with the launch sequence of `graph_launches`
+    // persistent launches recorded once in a CUDA graph and replayed (the
+    // remainder runs as plain launches).  Returns the steps run by replays.
+    uint64_t run_graph(uint64_t nsteps, uint32_t graph_launches);
+    void set_tuning(const Tuning& t);
+    const Tuning& tuning() const { return tuning_; }
+    uint32_t lif_grid() const { return lif_grid_; }
+    uint32_t scatter_split() const { return eng_.scatter_split; }
+    uint32_t blocks_per_sm() const { return lif_grid_ / (uint32_t)sm_count_; }
+    // engine-global raster id of each installed net's reference address 0
+    const std::vector<uint32_t>& id_offsets() const { return id_offsets_; }
+    const std::vector<NetHost*>& nets() const { return nets_; }
     // Deterministic-aggregation steps whose scratch is the library's fixed
     // device arena: no device memory is allocated or freed by the call.
     void run_fixed_scratch(uint64_t nsteps);
@@ -155,6 +180,14 @@ private:
     uint32_t lif_grid_ = 0, scatter_grid_ = 0;
     uint64_t host_step_ = 0;
     uint64_t launches_ = 0;
+    Tuning tuning_{};
+    uint64_t inst_raster_cap_ = 0;
+    bool inst_record_ = false;
+    std::vector<uint32_t> id_offsets_;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    uint32_t graph_launches_ = 0;
+    void drop_graph();
+    void launch_run_ex(uint32_t steps, bool from_ctl);
     uint64_t total_ring_cells_ = 0;
 
 

@@ -28,6 +28,9 @@ constexpr uint32_t kScatterPiece = 128 * kScatterUnroll;  // synapses per warp i
 // Steps of Poisson counts drawn ahead (ring of slots); small enough that the
 // counts and the delay ring stay resident in L2 together.
 constexpr uint32_t kDriveSlots = 16;
+// Step argument of k_drive / k_run meaning "the engine step in Ctl::step"
+// (launches recorded once in a CUDA graph and replayed).
+constexpr unsigned long long kStepFromCtl = ~0ull;
 constexpr uint32_t kLifBatch = 4;     // owned chunks whose loads are issued together
 
 struct PopDev {
@@ -70,6 +73,7 @@ struct NetDev {
     const float* e_plus;    // [e_len] exp(-k dt / tau_plus) as float
     const float* e_minus;   // [e_len] exp(-k dt / tau_minus) as float
     uint64_t start_step;    // engine step at which this net's step 0 runs
+    uint64_t end_step;      // first engine step at which this net no longer runs (~0 = never)
     uint64_t ring_key_base; // first ring cell of this net in the deterministic key space
     uint32_t n_storage;     // multiple of 4
     uint32_t ring_slots;    // D = max delay + 1

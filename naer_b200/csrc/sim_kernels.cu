@@ -81,12 +81,14 @@ static __device__ __noinline__ uint32_t poisson_exact_call(double rate, uint32_t
 
 __global__ void __launch_bounds__(kLifThreads, NAER_DRIVE_MIN_BLOCKS)
     k_drive(EngineDev eng, unsigned long long s_first, uint32_t nsteps) {
+    if (s_first == kStepFromCtl) s_first = eng.ctl->step;
     for (uint32_t c = blockIdx.x; c < eng.n_chunks; c += gridDim.x) {
         const ChunkDev ch = eng.chunks[c];
         const PopDev p = eng.pops[ch.pop];
         if (!(p.rate_hz > 0.0)) continue;
         const NetDev* np = eng.nets + ch.net;
         const unsigned long long start = np->start_step;
+        const unsigned long long stop = np->end_step;
         if (!np->active) continue;
         const uint32_t i0 = ch.first + threadIdx.x * kLifPerThread;
         if (i0 >= ch.end) continue;
@@ -97,7 +99,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_DRIVE_MIN_BLOCKS)
         // steps are independent draws: the loop carries no dependence
         for (uint32_t k = 0; k < nsteps; ++k) {
             const unsigned long long s = s_first + k;
-            if (s < start) continue;
+            if (s < start || s >= stop) continue;
             const uint32_t tl = (uint32_t)(s - start);
             const uint32_t t0 = tl * dt_us, t1 = t0 + dt_us;
             uint32_t z[4];
@@ -139,7 +141,7 @@ __device__ __forceinline__ void lif_chunk(const EngineDev& eng, uint32_t c, unsi
     const PopDev p = eng.pops[ch.pop];
     const NetDev* np = eng.nets + ch.net;
     const unsigned long long start = np->start_step;
-    if (!np->active || s < start) return;  // uniform over the block
+    if (!np->active || s < start || s >= np->end_step) return;  // uniform over the block
     const uint32_t tl = (uint32_t)(s - start);
     const uint32_t i0 = ch.first + threadIdx.x * kLifPerThread;
     const bool any = i0 < ch.end;
@@ -473,7 +475,7 @@ struct ChunkCache {
     float* v;
     uint8_t* refr;
     uint8_t* drive;
-    unsigned long long start;
+    unsigned long long start, stop;
     uint32_t first, end, net, Ns;
     uint32_t slots, dt_us, active, plastic;
 };
@@ -489,7 +491,7 @@ struct ChunkCache {
 __device__ __forceinline__ void lif_prefetch(const ChunkCache& cc, unsigned long long s, float4& I, uchar4& D) {
     I = make_float4(0.f, 0.f, 0.f, 0.f);
     D = make_uchar4(0, 0, 0, 0);
-    if (!cc.active || s < cc.start) return;
+    if (!cc.active || s < cc.start || s >= cc.stop) return;
     const uint32_t i0 = cc.first + threadIdx.x * kLifPerThread;
     if (i0 >= cc.end) return;
     const uint32_t tl = (uint32_t)(s - cc.start);
@@ -503,7 +505,7 @@ __device__ __forceinline__ void lif_prefetch(const ChunkCache& cc, unsigned long
 }
 
 __device__ __forceinline__ void lif_clear(const ChunkCache& cc, unsigned long long s) {
-    if (!cc.active || s < cc.start || cc.p.type == kPOISSON) return;
+    if (!cc.active || s < cc.start || s >= cc.stop || cc.p.type == kPOISSON) return;
     const uint32_t i0 = cc.first + threadIdx.x * kLifPerThread;
     if (i0 >= cc.end) return;
     const uint32_t tl = (uint32_t)(s - cc.start);
@@ -515,7 +517,7 @@ __device__ __forceinline__ void lif_chunk_smem(const EngineDev& eng, const Chunk
                                                unsigned long long s, float4* sV, uchar4* sR, const float4 I,
                                                const uchar4 D4, SpikeRec* __restrict__ queue,
                                                uint32_t* __restrict__ qid, uint32_t* s_count) {
-    if (!cc.active || s < cc.start) return;  // uniform over the block
+    if (!cc.active || s < cc.start || s >= cc.stop) return;  // uniform over the block
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t tl = (uint32_t)(s - cc.start);
@@ -658,6 +660,9 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
 
     Ctl* ctl = eng.ctl;
     unsigned long long bar_target = 0;
+    // every block reads the engine step before the first grid barrier; block 0
+    // advances it only after the last one
+    if (s0 == kStepFromCtl) s0 = ctl->step;
     unsigned long long rbase = ctl->raster_next;
     unsigned long long dropped = 0;
     const uint32_t region = blockIdx.x * eng.region_cap;
@@ -681,6 +686,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
             c.refr = np->refr;
             c.drive = np->drive;
             c.start = np->start_step;
+            c.stop = np->end_step;
             c.first = ch.first;
             c.end = ch.end;
             c.net = ch.net;

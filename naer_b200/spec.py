@@ -81,6 +81,18 @@ class NetSpec:
 
 def build(spec: NetSpec, device: int = 0) -> Network:
     """Creates and compiles the CUDA network described by ``spec``."""
+    net = describe(spec, device)
+    try:
+        net.compile()
+    except Exception:
+        net.close()
+        raise
+    return net
+
+
+def describe(spec: NetSpec, device: int = -1) -> Network:
+    """The uncompiled network of ``spec``.  With device -1 it is a
+    description-only handle: the input of a batch or a server."""
     net = Network(
         device=device,
         dt_us=spec.dt_us,
@@ -106,7 +118,6 @@ def build(spec: NetSpec, device: int = 0) -> Network:
         for c in spec.conns:
             net.connect(pops[c.src], pops[c.dst], rule=c.rule, weight=c.weight, probability=c.probability,
                         degree=c.degree, wmin=c.wmin, wmax=c.wmax, delay=(c.dmin, c.dmax), seed=c.seed)
-        net.compile()
     except Exception:
         net.close()
         raise
@@ -188,3 +199,47 @@ def _all_targets(s: NetSpec, E: int, I: int, k: int, seed: int) -> NetSpec:
     s.connect(I, E, R, W_I, degree=ke, seed=seed * 7919 + 23, **d)
     s.connect(I, I, R, W_I, degree=ki, seed=seed * 7919 + 24, **d)
     return s
+
+
+def batch_members(count: int = 256, seed: int = 1, n_range=(2000, 50_000), k_range=(100, 1000),
+                  rate_range=(5.0, 30.0), stdp_fraction: float = 0.5) -> list:
+    """Independent networks of uneven sizes for the batched form: neuron
+    counts log-uniform in n_range, in-degree uniform in k_range (80/20
+    E/I), each with its own seed, a per-neuron Poisson drive rate uniform in
+    rate_range and STDP on for a stdp_fraction of them (the plastic_indegree
+    network family)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        k = int(rng.integers(k_range[0], k_range[1] + 1))
+        rate = float(rng.uniform(*rate_range))
+        stdp = bool(rng.random() < stdp_fraction)
+        m = plastic_indegree(n=n, k=k, seed=seed * 100_003 + i, drive_rate_hz=rate, stdp=stdp)
+        m.name = f"member{i}(N={n},K={k},rate={rate:.1f},stdp={int(stdp)})"
+        out.append(m)
+    return out
+
+
+def served_jobs(count: int = 2000, seed: int = 1, arrivals_per_s: float = 50.0, n_range=(1000, 200_000),
+                k_range=(100, 1000), duration_ms=(100.0, 2000.0), stdp_fraction: float = 0.3,
+                rate_hz: float = 10.0, dt_us: int = 100) -> list:
+    """Simulation jobs for the served form: (arrival time in s, NetSpec,
+    duration in grid steps), Poisson arrivals at arrivals_per_s, neuron
+    counts log-uniform in n_range, in-degree uniform in k_range, durations
+    uniform in duration_ms, STDP on for a stdp_fraction of the jobs."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += float(rng.exponential(1.0 / arrivals_per_s))
+        n = int(round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        k = int(rng.integers(k_range[0], k_range[1] + 1))
+        dur = float(rng.uniform(*duration_ms))
+        stdp = bool(rng.random() < stdp_fraction)
+        m = plastic_indegree(n=n, k=k, seed=seed * 200_003 + i, drive_rate_hz=rate_hz, stdp=stdp)
+        m.name = f"job{i}(N={n},K={k},stdp={int(stdp)})"
+        out.append((t, m, max(1, int(round(dur * 1000.0 / dt_us)))))
+    return out

@@ -34,3 +34,18 @@ def reference_brunel(n_syn: float = 2e5) -> S.NetSpec:
                         (I, E, -10.0 / N), (I, I, -10.0 / N)]:
         s.connect(src, dst, R, w, probability=0.1, **d)
     return s
+
+
+def integer_weight_net(n=6000, k=300, seed=3, stdp=False) -> S.NetSpec:
+    """Fixed out-degree network whose weights and drive weight are integers
+    (mV): every ring sum is exact in fp32, so the order of the atomic
+    reductions cannot change any result."""
+    s = S.NetSpec(name="integer_weights", stdp_enabled=stdp, poisson_seed=seed)
+    ne = n * 4 // 5
+    E = s.add_pop(S.NOP, ne, drive_rate_hz=40.0, drive_weight=21.0, drive_seed=7 + seed)
+    I = s.add_pop(S.NOP, n - ne, drive_rate_hz=40.0, drive_weight=21.0, drive_seed=8 + seed)
+    R = capi.CONN_FIXED_OUTDEGREE
+    for src, w, sd in [(E, 1.0, 1), (I, -3.0, 2)]:
+        s.connect(src, E, R, w, degree=k * 4 // 5, dmin=1, dmax=12, seed=seed * 100 + sd)
+        s.connect(src, I, R, w, degree=k // 5, dmin=1, dmax=12, seed=seed * 100 + sd + 10)
+    return s

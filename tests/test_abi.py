@@ -48,7 +48,9 @@ def test_struct_layout_matches_header(lib, tmp_path):
     from naer_b200 import _capi as capi
     src = tmp_path / "probe.c"
     structs = {"naer_net_params": capi.NetParams, "naer_pop_params": capi.PopParams,
-               "naer_conn_spec": capi.ConnSpecC, "naer_stats": capi.Stats}
+               "naer_conn_spec": capi.ConnSpecC, "naer_stats": capi.Stats, "naer_tuning": capi.Tuning,
+               "naer_server_params": capi.ServerParams, "naer_job_info": capi.JobInfo,
+               "naer_server_stats": capi.ServerStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "naer/naer_capi.h"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
@@ -104,3 +106,41 @@ def test_create_without_gpu_fails_cleanly(lib):
     assert st in (capi.NAER_E_CUDA, capi.NAER_E_INVALID)
     assert not h.value
     assert capi.last_error()
+
+
+def test_description_only_network(lib):
+    """device -1: a description without device resources (the input of the
+    batched and served forms); compiling it is refused."""
+    from naer_b200 import _capi as capi
+    from naer_b200 import spec as S
+    d = S.describe(S.brunel_small(), -1)
+    try:
+        assert lib.naer_net_compile(d.handle) == capi.NAER_E_STATE
+        assert "description-only" in capi.last_error()
+        st = capi.Stats()
+        assert lib.naer_net_get_stats(d.handle, C.byref(st)) == capi.NAER_E_STATE
+    finally:
+        d.close()
+    h = C.c_void_p()
+    assert lib.naer_net_create(-2, None, C.byref(h)) == capi.NAER_E_INVALID
+
+
+def test_server_defaults(lib):
+    from naer_b200 import _capi as capi
+    p = capi.ServerParams()
+    assert lib.naer_server_params_default(C.byref(p)) == 0
+    assert p.budget_bytes == 150 * 10**9 and p.chunk_steps == 256 and p.aggregation == capi.AGG_ATOMIC
+
+
+def test_forms_workloads():
+    """The batched and served workload generators follow their stated ranges."""
+    from naer_b200 import spec as S
+    m = S.batch_members(count=64, seed=5)
+    ns = [sum(p.size for p in x.pops) for x in m]
+    assert min(ns) >= 2000 and max(ns) <= 50_000 and len(set(ns)) > 50
+    assert any(x.stdp_enabled for x in m) and not all(x.stdp_enabled for x in m)
+    jobs = S.served_jobs(count=200, seed=5)
+    t = [j[0] for j in jobs]
+    assert all(b > a for a, b in zip(t, t[1:]))
+    assert 2.5 < t[-1] < 6.0  # 200 arrivals at 50/s
+    assert all(1000 <= j[2] <= 20000 for j in jobs)

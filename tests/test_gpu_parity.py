@@ -11,7 +11,7 @@ from naer_b200 import _capi as capi
 from naer_b200 import spec as S
 from naer_b200.network import NeuronType
 
-from nets import mixed_rules, reference_brunel
+from nets import integer_weight_net, mixed_rules, reference_brunel
 
 pytestmark = pytest.mark.gpu
 
@@ -223,21 +223,6 @@ def test_state_roundtrip(lib):
         net.write_state(v2, r)
         v3, r3 = net.read_state()
         assert np.array_equal(v3, v2) and np.array_equal(r3, r)
-
-
-def integer_weight_net(n=6000, k=300, seed=3):
-    """Fixed out-degree network whose weights and drive weight are integers
-    (mV): every ring sum is exact in fp32, so the order of the atomic
-    reductions cannot change any result."""
-    s = S.NetSpec(name="integer_weights")
-    ne = n * 4 // 5
-    E = s.add_pop(S.NOP, ne, drive_rate_hz=40.0, drive_weight=21.0, drive_seed=7)
-    I = s.add_pop(S.NOP, n - ne, drive_rate_hz=40.0, drive_weight=21.0, drive_seed=8)
-    R = capi.CONN_FIXED_OUTDEGREE
-    for src, w, sd in [(E, 1.0, 1), (I, -3.0, 2)]:
-        s.connect(src, E, R, w, degree=k * 4 // 5, dmin=1, dmax=12, seed=seed * 100 + sd)
-        s.connect(src, I, R, w, degree=k // 5, dmin=1, dmax=12, seed=seed * 100 + sd + 10)
-    return s
 
 
 def test_atomic_persistent_path_exact_with_integer_weights(O):
