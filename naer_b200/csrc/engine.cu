@@ -208,8 +208,8 @@ static void layout(NetHost& n) {
         if (tr < 0 || tr > 255) throw Error(NAER_E_INVALID, "refractory period must be 0..255 steps");
         if (!(p.prm.tau_m_ms > 0.0f)) throw Error(NAER_E_INVALID, "tau_m_ms must be positive");
     }
-    if (P.stdp_enabled && P.stdp_history == 0)
-        throw Error(NAER_E_INVALID, "stdp_history must be at least 1");
+    if (P.stdp_enabled && (P.stdp_history == 0 || P.stdp_history > kMaxStdpHistory))
+        throw Error(NAER_E_INVALID, "stdp_history must be in 1..16");
 }
 
 // Device bytes of a built network, from its description: padded synapse
@@ -243,7 +243,7 @@ uint64_t estimate_device_bytes(const NetHost& description) {
     b += Ns * (4ull + 1ull + kDriveSlots + 4ull * n.ring_slots);                // V, refr, drive, ring
     if (n.params.stdp_enabled && n.n_plastic) {
         const uint64_t Np = n.n_plastic;
-        b += Np * (16ull + 4ull * n.params.stdp_history);
+        b += Np * (8ull + 4ull * round_up4(2u + n.params.stdp_history));
         const double tmax = std::max(n.params.tau_plus_ms, n.params.tau_minus_ms) * 1000.0;
         b += 8ull * (uint64_t)std::min<double>(std::ceil(104.0 * tmax / n.params.dt_us) + 1.0, 1 << 24);
     }
@@ -430,17 +430,17 @@ void Engine::build(NetHost& n) {
     const auto& P = n.params;
     const bool stdp = P.stdp_enabled && n.n_plastic > 0;
     if (stdp) {
-        const uint32_t Np = n.n_plastic, K = P.stdp_history;
-        n.last_post = static_cast<int32_t*>(dalloc(Np * 4ull));
-        n.y_post = static_cast<float*>(dalloc(Np * 4ull));
-        n.hist = static_cast<int32_t*>(dalloc((uint64_t)Np * K * 4ull));
-        n.last_pre = static_cast<int32_t*>(dalloc(Np * 4ull));
-        n.x_pre = static_cast<float*>(dalloc(Np * 4ull));
-        NAER_CK(cudaMemsetAsync(n.last_post, 0xFF, Np * 4ull, st));
-        NAER_CK(cudaMemsetAsync(n.y_post, 0, Np * 4ull, st));
-        NAER_CK(cudaMemsetAsync(n.hist, 0xFF, (uint64_t)Np * K * 4ull, st));
-        NAER_CK(cudaMemsetAsync(n.last_pre, 0xFF, Np * 4ull, st));
-        NAER_CK(cudaMemsetAsync(n.x_pre, 0, Np * 4ull, st));
+        const uint32_t Np = n.n_plastic;
+        n.post_stride = round_up4(2u + P.stdp_history);
+        n.post = static_cast<int32_t*>(dalloc((uint64_t)Np * n.post_stride * 4ull));
+        n.pre = static_cast<int2*>(dalloc(Np * 8ull));
+        // every word -1, then the post traces (word 1 of each row) 0.0f
+        std::vector<int32_t> row0((uint64_t)Np * n.post_stride, -1);
+        for (uint64_t r = 0; r < Np; ++r) row0[r * n.post_stride + 1] = 0;
+        NAER_CK(cudaMemcpyAsync(n.post, row0.data(), row0.size() * 4ull, cudaMemcpyHostToDevice, st));
+        std::vector<int2> pre0(Np, make_int2(-1, 0));
+        NAER_CK(cudaMemcpyAsync(n.pre, pre0.data(), Np * 8ull, cudaMemcpyHostToDevice, st));
+        NAER_CK(cudaStreamSynchronize(st));  // host staging vectors go out of scope
         // exp(-k dt / tau) as float until it underflows (k dt / tau > 104)
         const double tmax = std::max((double)P.tau_plus_ms, (double)P.tau_minus_ms) * 1000.0;
         n.e_len = (uint32_t)std::min<double>(std::ceil(104.0 * tmax / P.dt_us) + 1.0, 1 << 24);
@@ -467,11 +467,9 @@ void Engine::build(NetHost& n) {
     d.tgt = n.tgt;
     d.w = n.w;
     d.dly = n.dly;
-    d.last_post = n.last_post;
-    d.y_post = n.y_post;
-    d.hist = n.hist;
-    d.last_pre = n.last_pre;
-    d.x_pre = n.x_pre;
+    d.post = n.post;
+    d.pre = n.pre;
+    d.post_stride = n.post_stride;
     d.e_plus = n.e_plus;
     d.e_minus = n.e_minus;
     d.start_step = 0;
@@ -506,12 +504,9 @@ void Engine::free_net(NetHost& n) {
     dfree(n.tgt, std::max<uint64_t>(S, 4) * 4ull);
     dfree(n.w, std::max<uint64_t>(S, 4) * 4ull);
     dfree(n.dly, std::max<uint64_t>(S, 16));
-    const uint32_t Np = n.n_plastic, K = n.params.stdp_history;
-    dfree(n.last_post, Np * 4ull);
-    dfree(n.y_post, Np * 4ull);
-    dfree(n.hist, (uint64_t)Np * K * 4ull);
-    dfree(n.last_pre, Np * 4ull);
-    dfree(n.x_pre, Np * 4ull);
+    const uint32_t Np = n.n_plastic;
+    dfree(n.post, (uint64_t)Np * n.post_stride * 4ull);
+    dfree(n.pre, Np * 8ull);
     dfree(n.e_plus, n.e_len * 4ull);
     dfree(n.e_minus, n.e_len * 4ull);
     n.v = nullptr;
@@ -521,8 +516,9 @@ void Engine::free_net(NetHost& n) {
     n.tgt = nullptr;
     n.w = nullptr;
     n.dly = nullptr;
-    n.last_post = n.last_pre = n.hist = nullptr;
-    n.y_post = n.x_pre = n.e_plus = n.e_minus = nullptr;
+    n.post = nullptr;
+    n.pre = nullptr;
+    n.e_plus = n.e_minus = nullptr;
     n.compiled = false;
 }
 

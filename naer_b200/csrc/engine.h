@@ -60,11 +60,9 @@ struct NetHost {
     uint32_t* tgt = nullptr;
     float* w = nullptr;
     uint8_t* dly = nullptr;
-    int32_t* last_post = nullptr;
-    float* y_post = nullptr;
-    int32_t* hist = nullptr;
-    int32_t* last_pre = nullptr;
-    float* x_pre = nullptr;
+    int32_t* post = nullptr;   // [n_plastic][post_stride] packed post rows
+    int2* pre = nullptr;       // [n_plastic] {last pre step, pre trace bits}
+    uint32_t post_stride = 0;
     float* e_plus = nullptr;
     float* e_minus = nullptr;
     uint32_t e_len = 0;

@@ -28,6 +28,10 @@ constexpr uint32_t kScatterPiece = 128 * kScatterUnroll;  // synapses per warp i
 // Steps of Poisson counts drawn ahead (ring of slots); small enough that the
 // counts and the delay ring stay resident in L2 together.
 constexpr uint32_t kDriveSlots = 16;
+// STDP post-spike history: at most this many entries per plastic neuron, so
+// a packed post row (2 + history words, rounded up to 4) fits kPostWordsMax.
+constexpr uint32_t kMaxStdpHistory = 16;
+constexpr uint32_t kPostWordsMax = 20;
 // Step argument of k_drive / k_run meaning "the engine step in Ctl::step"
 // (launches recorded once in a CUDA graph and replayed).
 constexpr unsigned long long kStepFromCtl = ~0ull;
@@ -65,11 +69,13 @@ struct NetDev {
     float* w;               // [S] weight (written back by STDP)
     const uint8_t* dly;     // [S] delay in steps, 1..ring_slots-1
     // pair-based STDP state, one entry per plastic storage index
-    int32_t* last_post;     // step of the latest post spike, -1 = none
-    float* y_post;          // post trace right after last_post
-    int32_t* hist;          // [n_plastic][hist_len] post spike steps, newest first, -1 = none
-    int32_t* last_pre;      // step of the latest pre spike, -1 = none
-    float* x_pre;           // pre trace right after last_pre
+    // Packed post-synaptic row of each plastic neuron, post_stride int32
+    // words (a multiple of 4, so one row is read with int4 loads): [0] step
+    // of the latest post spike (-1 = none), [1] post trace right after it
+    // (float bits), [2, 2 + hist_len) post spike steps, newest first (-1 =
+    // none).
+    int32_t* post;
+    int2* pre;              // {step of the latest pre spike (-1 = none), pre trace after it (float bits)}
     const float* e_plus;    // [e_len] exp(-k dt / tau_plus) as float
     const float* e_minus;   // [e_len] exp(-k dt / tau_minus) as float
     uint64_t start_step;    // engine step at which this net's step 0 runs
@@ -81,6 +87,7 @@ struct NetDev {
     uint32_t n_plastic;     // storage indices below this are STDP neurons
     uint32_t stdp_on;       // plasticity enabled for this net
     uint32_t hist_len;
+    uint32_t post_stride;   // words per post row
     uint32_t e_len;
     float a_plus;           // A+ * w_max
     float a_minus;          // A- * w_max

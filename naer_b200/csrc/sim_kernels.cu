@@ -199,34 +199,7 @@ __device__ __forceinline__ void lif_chunk(const EngineDev& eng, uint32_t c, unsi
                 v = p.v_reset;
                 rr[j] = p.t_ref_steps;
                 spk[j] = true;
-                if (plastic) {
-                    // rare path: descriptor fields read here, not kept live
-                    int32_t* last_post = np->last_post;
-                    float* y_post = np->y_post;
-                    int32_t* hist = np->hist;
-                    int32_t* last_pre = np->last_pre;
-                    float* x_pre = np->x_pre;
-                    const float* e_plus = np->e_plus;
-                    const float* e_minus = np->e_minus;
-                    const uint32_t hist_len = np->hist_len, e_len = np->e_len;
-                    const int32_t t = (int32_t)tl;
-                    // post trace and post-spike history (newest first)
-                    const int32_t lp = last_post[i];
-                    float y = lp >= 0 ? __fmul_rn(y_post[i], decay_lookup(e_minus, e_len, t - lp)) : 0.0f;
-                    y_post[i] = __fadd_rn(y, 1.0f);
-                    last_post[i] = t;
-                    int32_t* h = hist + (size_t)i * hist_len;
-                    for (int k = (int)hist_len - 1; k > 0; --k) h[k] = h[k - 1];
-                    h[0] = t;
-                    // pre trace: the queue record carries the state before this spike
-                    const int32_t lq = last_pre[i];
-                    const float xo = x_pre[i];
-                    aux0[j] = lq;
-                    aux1[j] = xo;
-                    float x = lq >= 0 ? __fmul_rn(xo, decay_lookup(e_plus, e_len, t - lq)) : 0.0f;
-                    x_pre[i] = __fadd_rn(x, 1.0f);
-                    last_pre[i] = t;
-                }
+                if (plastic) stdp_post_spike(np, i, (int32_t)tl, aux0[j], aux1[j]);  // rare path
             }
             vv[j] = v;
         }
@@ -563,32 +536,7 @@ __device__ __forceinline__ void lif_chunk_smem(const EngineDev& eng, const Chunk
                 v = v_reset;
                 rr[k] = cc.p.t_ref_steps;
                 spk[k] = true;
-                if (cc.plastic) {
-                    const NetDev* np = eng.nets + cc.net;
-                    int32_t* last_post = np->last_post;
-                    float* y_post = np->y_post;
-                    int32_t* hist = np->hist;
-                    int32_t* last_pre = np->last_pre;
-                    float* x_pre = np->x_pre;
-                    const float* e_plus = np->e_plus;
-                    const float* e_minus = np->e_minus;
-                    const uint32_t hist_len = np->hist_len, e_len = np->e_len;
-                    const int32_t t = (int32_t)tl;
-                    const int32_t lp = last_post[i];
-                    float y = lp >= 0 ? __fmul_rn(y_post[i], decay_lookup(e_minus, e_len, t - lp)) : 0.0f;
-                    y_post[i] = __fadd_rn(y, 1.0f);
-                    last_post[i] = t;
-                    int32_t* h = hist + (size_t)i * hist_len;
-                    for (int q = (int)hist_len - 1; q > 0; --q) h[q] = h[q - 1];
-                    h[0] = t;
-                    const int32_t lq = last_pre[i];
-                    const float xo = x_pre[i];
-                    aux0[k] = lq;
-                    aux1[k] = xo;
-                    float x = lq >= 0 ? __fmul_rn(xo, decay_lookup(e_plus, e_len, t - lq)) : 0.0f;
-                    x_pre[i] = __fadd_rn(x, 1.0f);
-                    last_pre[i] = t;
-                }
+                if (cc.plastic) stdp_post_spike(eng.nets + cc.net, i, (int32_t)tl, aux0[k], aux1[k]);
             }
             vv[k] = v;
         }

@@ -58,28 +58,40 @@ __device__ __forceinline__ float decay_lookup(const float* table, uint32_t len, 
 // Register copy of a net's plasticity fields (the kernels copy descriptor
 // fields once per work item so that stores and atomics cannot force reloads).
 struct StdpView {
-    const int32_t* __restrict__ hist;
-    const int32_t* __restrict__ last_post;
-    const float* __restrict__ y_post;
+    const int32_t* __restrict__ post;
     const float* __restrict__ e_plus;
     const float* __restrict__ e_minus;
-    uint32_t hist_len, e_len;
+    uint32_t hist_len, post_stride, e_len;
     float a_plus, a_minus, w_max;
 };
 
 __device__ __forceinline__ StdpView stdp_view(const NetDev& n) {
     StdpView v;
-    v.hist = n.hist;
-    v.last_post = n.last_post;
-    v.y_post = n.y_post;
+    v.post = n.post;
     v.e_plus = n.e_plus;
     v.e_minus = n.e_minus;
     v.hist_len = n.hist_len;
+    v.post_stride = n.post_stride;
     v.e_len = n.e_len;
     v.a_plus = n.a_plus;
     v.a_minus = n.a_minus;
     v.w_max = n.w_max;
     return v;
+}
+
+// A packed post row (stride words, a multiple of 4) into registers with
+// independent int4 loads at L2 (rows are rewritten by other blocks' LIF);
+// words past the stride read as -1.
+__device__ __forceinline__ void load_post_row(const int32_t* row, uint32_t stride, int32_t (&r)[kPostWordsMax]) {
+#pragma unroll
+    for (uint32_t v = 0; v < kPostWordsMax / 4; ++v) {
+        int4 x = make_int4(-1, -1, -1, -1);
+        if (v * 4u < stride) x = __ldcg(reinterpret_cast<const int4*>(row) + v);
+        r[4 * v] = x.x;
+        r[4 * v + 1] = x.y;
+        r[4 * v + 2] = x.z;
+        r[4 * v + 3] = x.w;
+    }
 }
 
 // Pair-based STDP for one plastic synapse at the pre spike of step t
@@ -88,26 +100,73 @@ __device__ __forceinline__ StdpView stdp_view(const NetDev& n) {
 // LTD uses the post trace at t.  Weights are clipped to [0, w_max] after
 // every update, so the sequence equals the online rule's.  Every operation
 // is an explicitly rounded fp32 op so the oracle can repeat it bit for bit.
+// The target's whole post row is loaded at once and every decay-table
+// lookup is issued before the sequential weight updates use them.
 // Plays the role of update_synapse (include/naer/kernels/stdp.cl:8-30).
 __device__ __forceinline__ float stdp_update(const StdpView& n, float w, uint32_t tgt, int32_t t,
                                              int32_t pre_last, float pre_x, uint32_t& overflow) {
+    int32_t r[kPostWordsMax];
+    load_post_row(n.post + (size_t)tgt * n.post_stride, n.post_stride, r);
     if (pre_last >= 0) {
-        const int32_t* h = n.hist + (size_t)tgt * n.hist_len;
+        // history entries newer than pre_last form a prefix (newest first)
         uint32_t c = 0;
-        while (c < n.hist_len && __ldcg(h + c) > pre_last) ++c;
+        bool run = true;
+#pragma unroll
+        for (uint32_t k = 0; k < kMaxStdpHistory; ++k) {
+            run = run && k < n.hist_len && r[2 + k] > pre_last;
+            c += run ? 1u : 0u;
+        }
         if (c == n.hist_len) ++overflow;
-        for (int k = (int)c - 1; k >= 0; --k) {
-            const int32_t s = __ldcg(h + k);
-            const float x = __fmul_rn(pre_x, decay_lookup(n.e_plus, n.e_len, s - pre_last));
-            w = fminf(__fadd_rn(w, __fmul_rn(n.a_plus, x)), n.w_max);
+        float e[kMaxStdpHistory];
+#pragma unroll
+        for (uint32_t k = 0; k < kMaxStdpHistory; ++k)
+            e[k] = k < c ? decay_lookup(n.e_plus, n.e_len, r[2 + k] - pre_last) : 0.0f;
+#pragma unroll
+        for (int k = (int)kMaxStdpHistory - 1; k >= 0; --k) {
+            if ((uint32_t)k < c) {
+                const float x = __fmul_rn(pre_x, e[k]);
+                w = fminf(__fadd_rn(w, __fmul_rn(n.a_plus, x)), n.w_max);
+            }
         }
     }
-    const int32_t lp = __ldcg(n.last_post + tgt);
+    const int32_t lp = r[0];
     if (lp >= 0) {
-        const float y = __fmul_rn(__ldcg(n.y_post + tgt), decay_lookup(n.e_minus, n.e_len, t - lp));
+        const float y = __fmul_rn(__int_as_float(r[1]), decay_lookup(n.e_minus, n.e_len, t - lp));
         w = fmaxf(__fsub_rn(w, __fmul_rn(n.a_minus, y)), 0.0f);
     }
     return w;
+}
+
+// Plasticity bookkeeping of plastic neuron i spiking at local step t: post
+// trace and post history (row rewritten whole), pre trace.  aux0/aux1
+// receive the pre state before this spike (carried by the queue record).
+__device__ __forceinline__ void stdp_post_spike(const NetDev* np, uint32_t i, int32_t t, int32_t& aux0, float& aux1) {
+    const uint32_t stride = np->post_stride, hist_len = np->hist_len, e_len = np->e_len;
+    const float* e_plus = np->e_plus;
+    const float* e_minus = np->e_minus;
+    int32_t* row = np->post + (size_t)i * stride;
+    int2* pre = np->pre + i;
+    int32_t r[kPostWordsMax];
+    load_post_row(row, stride, r);
+    const int2 pq = __ldcg(pre);
+    const int32_t lp = r[0];
+    const float y = lp >= 0 ? __fmul_rn(__int_as_float(r[1]), decay_lookup(e_minus, e_len, t - lp)) : 0.0f;
+    r[0] = t;
+    r[1] = __float_as_int(__fadd_rn(y, 1.0f));
+#pragma unroll
+    for (int q = (int)kMaxStdpHistory - 1; q > 0; --q)
+        if ((uint32_t)q < hist_len) r[2 + q] = r[1 + q];
+    r[2] = t;
+#pragma unroll
+    for (uint32_t v = 0; v < kPostWordsMax / 4; ++v)
+        if (v * 4u < stride)
+            __stcg(reinterpret_cast<int4*>(row) + v, make_int4(r[4 * v], r[4 * v + 1], r[4 * v + 2], r[4 * v + 3]));
+    const int32_t lq = pq.x;
+    const float xo = __int_as_float(pq.y);
+    aux0 = lq;
+    aux1 = xo;
+    const float x = lq >= 0 ? __fmul_rn(xo, decay_lookup(e_plus, e_len, t - lq)) : 0.0f;
+    __stcg(pre, make_int2(t, __float_as_int(__fadd_rn(x, 1.0f))));
 }
 
 __device__ __forceinline__ uint32_t ring_slot(uint32_t t_mod, uint32_t d, uint32_t slots) {
