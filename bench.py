@@ -47,6 +47,11 @@ def parse():
     ap.add_argument("--cpu-warmup", type=int, default=300)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and served forms")
+    ap.add_argument("--batch-members", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=20000, help="grid steps per member (2 s)")
+    ap.add_argument("--served-jobs", type=int, default=2000)
+    ap.add_argument("--plain-sample", type=int, default=6, help="jobs run one at a time for the plain arm")
     return ap.parse_args()
 
 
@@ -210,6 +215,111 @@ def run_reference(args):
     return 0
 
 
+def plain_runs(specs_steps, local):
+    """Each job alone with the plain form, one after another: build, run,
+    read the raster back.  Returns per-job seconds (run only, with build)."""
+    from naer_b200 import spec as S
+    run_s, all_s = [], []
+    for spec, steps in specs_steps:
+        t0 = time.perf_counter()
+        net = S.build(spec, device=local)
+        t1 = time.perf_counter()
+        net.run(steps)
+        net.finish()
+        net.read_spikes()
+        t2 = time.perf_counter()
+        net.close()
+        run_s.append(t2 - t1)
+        all_s.append(t2 - t0)
+    return run_s, all_s
+
+
+def bench_batched(args, local):
+    """Batched form: independent networks of uneven sizes (log-uniform 2k-50k
+    neurons, in-degree 100-1000, own seeds, Poisson 5-30 Hz, STDP on half)
+    packed into one engine, autotuned, CUDA-graph step loop, 2 s simulated
+    each; against one-at-a-time plain runs of a seeded sample of the same
+    members."""
+    import numpy as np
+    from naer_b200 import spec as S
+    from naer_b200.forms import Batch
+    members = S.batch_members(count=args.batch_members, seed=1)
+    for m in members:
+        m.raster_capacity = 1 << 22
+    steps = args.batch_steps
+    t0 = time.perf_counter()
+    b = Batch(members, device=local, raster_capacity=1 << 26).compile()
+    t1 = time.perf_counter()
+    st0 = b.stats()
+    t2 = time.perf_counter()
+    tune = b.autotune(64)  # its trial steps are part of the members' simulated time
+    done = b.stats()["step"]
+    b.run(steps - done)
+    b.finish()
+    t3 = time.perf_counter()
+    st1 = b.stats()
+    b.close()
+    sim_s = t3 - t2
+    rng = np.random.default_rng(7)
+    pick = rng.choice(len(members), min(args.plain_sample, len(members)), replace=False)
+    run_s, all_s = plain_runs([(members[int(i)], steps) for i in pick], local)
+    plain_rate = 1.0 / float(np.mean(run_s))
+    return {
+        "workload": f"{len(members)} networks, {st0['neurons']} neurons, {st0['synapses']} synapses in total; "
+                    f"{steps} grid steps (2 s) each",
+        "sims_per_s": len(members) / sim_s,
+        "sims_per_s_with_build": len(members) / (sim_s + t1 - t0),
+        "events_per_s": (st1["events"] - st0["events"]) / sim_s,
+        "us_per_step": sim_s / steps * 1e6,
+        "build_s": t1 - t0,
+        "autotune": {k: tune[k] for k in ("blocks_per_sm", "launch_steps", "scatter_split", "graph_launches",
+                                          "best_us_per_step", "default_us_per_step", "trials")},
+        "plain_sims_per_s": plain_rate,
+        "plain_sims_per_s_with_build": 1.0 / float(np.mean(all_s)),
+        "plain_sample": f"{len(pick)} members run alone one after another (mean {np.mean(run_s):.3f} s each)",
+        "speedup_vs_plain": (len(members) / sim_s) / plain_rate,
+        "raster_records": int(st1["spikes"]),
+    }
+
+
+def bench_served(args, local):
+    """Served form: a seeded Poisson stream of jobs (50/s; 1k-200k neurons
+    log-uniform, in-degree 100-1000, 100 ms - 2 s, 30 % STDP) submitted on
+    schedule to the continuous-batching server (150 GB budget); p50/p99
+    latency from submission to raster delivered; against the same jobs' plain
+    one-at-a-time runs (a seeded sample)."""
+    import numpy as np
+    from naer_b200 import spec as S
+    from naer_b200.forms import Server
+    jobs = S.served_jobs(count=args.served_jobs, seed=1)
+    srv = Server(device=local, budget_bytes=150 * 10**9, chunk_steps=256)
+    t0 = time.perf_counter()
+    for ta, spec, steps in jobs:
+        now = time.perf_counter() - t0
+        if ta > now:
+            time.sleep(ta - now)
+        srv.submit(spec, steps)
+    ok = srv.drain(1800.0)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    rng = np.random.default_rng(11)
+    pick = rng.choice(len(jobs), min(args.plain_sample, len(jobs)), replace=False)
+    run_s, all_s = plain_runs([(jobs[int(i)][1], jobs[int(i)][2]) for i in pick], local)
+    return {
+        "workload": f"{len(jobs)} jobs, Poisson arrivals at 50/s over {jobs[-1][0]:.1f} s",
+        "sims_per_s": st["sims_per_s"],
+        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+        "drained": ok, "wall_s": wall, "done": st["done"], "failed": st["failed"],
+        "peak_device_gb": st["peak_bytes"] / 1e9, "chunks": st["chunks"], "raster_dropped": st["raster_dropped"],
+        "thread_s": {k: round(st[k], 2) for k in ("build_s", "install_s", "step_s", "drain_s")},
+        "plain_sims_per_s": 1.0 / float(np.mean(all_s)),
+        "plain_latency_ms_mean": 1e3 * float(np.mean(all_s)),
+        "plain_sample": f"{len(pick)} jobs run alone one after another (build + run + raster read)",
+        "speedup_vs_plain": st["sims_per_s"] * float(np.mean(all_s)),
+    }
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -315,6 +425,11 @@ def run_ours(args):
     else:
         net.close()
 
+    forms = {}
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms["batched"] = bench_batched(args, local)
+        forms["served"] = bench_served(args, local)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -336,6 +451,7 @@ def run_ours(args):
             "clocks": clk,
             "spikes_per_s_sim": spikes / (args.steps * chunk * 1e-4) / args.neurons,
         }
+        line.update(forms)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

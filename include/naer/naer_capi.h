@@ -339,6 +339,8 @@ typedef struct naer_server_stats {
     uint64_t chunks, engine_steps, peak_bytes, bytes_in_use, raster_dropped;
     double p50_ms, p99_ms, mean_ms;  /* job latency: submit to raster delivered */
     double sims_per_s;               /* jobs done / (last done - first submit) */
+    double build_s;                  /* builder thread: device builds */
+    double install_s, step_s, drain_s;  /* stepper thread: tables, chunks, rasters */
 } naer_server_stats;
 
 NAER_API int naer_server_params_default(naer_server_params* p);

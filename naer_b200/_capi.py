@@ -144,7 +144,8 @@ class JobInfo(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("submitted", "done", "failed", "running", "queued", "chunks",
                                            "engine_steps", "peak_bytes", "bytes_in_use", "raster_dropped")] + \
-               [(n, C.c_double) for n in ("p50_ms", "p99_ms", "mean_ms", "sims_per_s")]
+               [(n, C.c_double) for n in ("p50_ms", "p99_ms", "mean_ms", "sims_per_s", "build_s", "install_s",
+                                          "step_s", "drain_s")]
 
 
 class NaerError(RuntimeError):

@@ -117,7 +117,11 @@ __global__ void k_indeg_count(ConnBuild cb, uint32_t* cnt) {
     }
 }
 
-__global__ void k_indeg_fill(ConnBuild cb, unsigned long long* cursor, unsigned long long* keys) {
+// Fixed in-degree rows in canonical order without atomics: every draw
+// d = target * K + k gets its source as a sort key and d as the value; a
+// stable radix sort by source then lists each source's draws in ascending
+// (target, k), the order the rows keep.
+__global__ void k_indeg_keys(ConnBuild cb, uint32_t* keys, uint32_t* vals) {
     const uint32_t blocks = (cb.K + 3u) >> 2;
     const uint64_t total = (uint64_t)cb.dst_size * blocks;
     for (uint64_t it = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; it < total;
@@ -129,30 +133,24 @@ __global__ void k_indeg_fill(ConnBuild cb, unsigned long long* cursor, unsigned 
         for (int j = 0; j < 4; ++j) {
             const uint32_t k = b * 4u + j;
             if (k >= cb.K) break;
-            const uint32_t s = conn_pick(r.v[j], cb.src_size);
-            const unsigned long long pos = atomicAdd(cursor + s, 1ull);
-            keys[pos] = (unsigned long long)i * cb.K + k;
+            const uint32_t d = i * cb.K + k;
+            keys[d] = conn_pick(r.v[j], cb.src_size);
+            vals[d] = d;
         }
     }
 }
 
-// After the per-source segments of `keys` are sorted: write entry e of the
-// connection-local order into the source's row.
-__global__ void k_indeg_finalize(ConnBuild cb, const unsigned long long* keys, uint64_t total,
+// Sorted draw e (source s = keys[e], draw d = vals[e]) into its row: entry
+// e - conn_off[s] of the connection's part of row s.
+__global__ void k_indeg_finalize(ConnBuild cb, const uint32_t* keys, const uint32_t* vals, uint64_t total,
                                  const uint64_t* conn_off, const uint64_t* cursor, uint32_t* tgt,
                                  float* w, uint8_t* dly) {
     for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
          e += (uint64_t)gridDim.x * blockDim.x) {
-        // source: last s with conn_off[s] <= e
-        uint32_t lo = 0, hi = cb.src_size;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (conn_off[mid] <= e) lo = mid; else hi = mid;
-        }
-        const uint32_t s = lo;
-        const unsigned long long key = keys[e];
-        const uint32_t i = (uint32_t)(key / cb.K);
-        const uint32_t k = (uint32_t)(key % cb.K);
+        const uint32_t s = keys[e];
+        const uint32_t d = vals[e];
+        const uint32_t i = d / cb.K;
+        const uint32_t k = d - i * cb.K;
         const uint32_t b = k >> 2, j = k & 3u;
         const uint64_t o = cursor[cb.src_storage + s] + (e - conn_off[s]);
         tgt[o] = cb.dst_storage + i;

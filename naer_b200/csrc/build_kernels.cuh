@@ -68,8 +68,8 @@ __global__ void k_bern_fill(ConnBuild cb, const uint64_t* cursor, uint32_t* tgt,
 __global__ void k_outdeg_fill(ConnBuild cb, const uint64_t* cursor, uint32_t* tgt, float* w,
                               uint8_t* dly);
 __global__ void k_indeg_count(ConnBuild cb, uint32_t* cnt);
-__global__ void k_indeg_fill(ConnBuild cb, unsigned long long* cursor, unsigned long long* keys);
-__global__ void k_indeg_finalize(ConnBuild cb, const unsigned long long* keys, uint64_t total,
+__global__ void k_indeg_keys(ConnBuild cb, uint32_t* keys, uint32_t* vals);
+__global__ void k_indeg_finalize(ConnBuild cb, const uint32_t* keys, const uint32_t* vals, uint64_t total,
                                  const uint64_t* conn_off, const uint64_t* cursor, uint32_t* tgt,
                                  float* w, uint8_t* dly);
 __global__ void k_row_len_add(const uint32_t* cnt, uint32_t src_size, uint32_t src_storage,

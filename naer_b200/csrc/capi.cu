@@ -683,6 +683,10 @@ int naer_server_get_stats(naer_server* server, naer_server_stats* st) {
         st->p99_ms = s.p99_ms;
         st->mean_ms = s.mean_ms;
         st->sims_per_s = s.sims_per_s;
+        st->build_s = s.build_s;
+        st->install_s = s.install_s;
+        st->step_s = s.step_s;
+        st->drain_s = s.drain_s;
     });
 }
 

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 
 #include "build_kernels.cuh"
@@ -80,8 +81,7 @@ void with_cub_tmp(Engine& eng, F&& f) {
         eng.dfree(tmp, bytes ? bytes : 16);
         throw;
     }
-    NAER_CK(cudaStreamSynchronize(eng.stream()));
-    eng.dfree(tmp, bytes ? bytes : 16);
+    eng.dfree(tmp, bytes ? bytes : 16);  // ordered after the call's kernels
 }
 
 uint32_t grid_for(uint64_t items, uint32_t threads, uint32_t max_blocks) {
@@ -93,15 +93,22 @@ uint32_t grid_for(uint64_t items, uint32_t threads, uint32_t max_blocks) {
 
 }  // namespace
 
-Engine::Engine(int device) : device_(device) {
+Engine::Engine(int device, int priority) : device_(device) {
     int n = 0;
     NAER_CK(cudaGetDeviceCount(&n));
     if (device < 0 || device >= n) throw Error(NAER_E_INVALID, "device index out of range");
     NAER_CK(cudaSetDevice(device));
     NAER_CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device));
-    NAER_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    NAER_CK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, priority));
+    // keep freed stream-ordered memory in this process's pool (rebuilding
+    // networks reuses it without new mappings); ~Engine trims the pool
+    cudaMemPool_t pool;
+    NAER_CK(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = ~0ull;
+    NAER_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     d_ctl_ = static_cast<Ctl*>(dalloc(sizeof(Ctl)));
-    NAER_CK(cudaMemset(d_ctl_, 0, sizeof(Ctl)));
+    NAER_CK(cudaMemsetAsync(d_ctl_, 0, sizeof(Ctl), stream_));
+    NAER_CK(cudaStreamSynchronize(stream_));
     NAER_CK(cudaMallocHost(&h_pinned_, 256));
 }
 
@@ -139,19 +146,28 @@ Engine::~Engine() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (h_pinned_) cudaFreeHost(h_pinned_);
     cudaStreamDestroy(stream_);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device_) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     if (prev >= 0) cudaSetDevice(prev);
 }
 
+// Stream-ordered allocation: neither call synchronises the device, so an
+// engine that builds networks never stalls another engine's step launches.
+// Memory from dalloc is usable by work queued on this engine's stream at
+// once, and by other streams or the host after this stream is synchronised
+// (every engine entry point that hands memory elsewhere synchronises);
+// dfree is ordered after the work already queued on this stream (callers
+// free memory only when no other stream still uses it).
 void* Engine::dalloc(size_t bytes) {
     void* p = nullptr;
-    NAER_CK(cudaMalloc(&p, bytes ? bytes : 16));
+    NAER_CK(cudaMallocAsync(&p, bytes ? bytes : 16, stream_));
     bytes_ += bytes;
     return p;
 }
 
 void Engine::dfree(void* p, size_t bytes) {
     if (!p) return;
-    NAER_CK(cudaFree(p));
+    NAER_CK(cudaFreeAsync(p, stream_));
     bytes_ -= std::min<uint64_t>(bytes_, bytes);
 }
 
@@ -333,28 +349,28 @@ void Engine::build(NetHost& n) {
             with_cub_tmp(*this, [&](void* tmp, size_t& b) {
                 return cub::DeviceScan::ExclusiveSum(tmp, b, cnt64, off, (int)(cb.src_size + 1), st);
             });
-            uint64_t total = 0;
-            NAER_CK(cudaMemcpyAsync(&total, off + cb.src_size, 8, cudaMemcpyDeviceToHost, st));
-            NAER_CK(cudaStreamSynchronize(st));
+            const uint64_t total = (uint64_t)cb.dst_size * cb.K;  // every draw lands in some row
             if (total > 0x7FFFFFFFull)
                 throw Error(NAER_E_OVERFLOW, "a FIXED_INDEGREE connection exceeds 2^31 synapses");
-            unsigned long long* ccur = reinterpret_cast<unsigned long long*>(cnt64);
-            NAER_CK(cudaMemcpyAsync(ccur, off, cb.src_size * 8ull, cudaMemcpyDeviceToDevice, st));
-            auto* kin = static_cast<unsigned long long*>(dalloc(std::max<uint64_t>(total, 1) * 8ull));
-            auto* kout = static_cast<unsigned long long*>(dalloc(std::max<uint64_t>(total, 1) * 8ull));
+            // stable radix sort of the draws by source (draw order = canonical order)
+            auto* kin = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(total, 1) * 4ull));
+            auto* kout = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(total, 1) * 4ull));
+            auto* vin = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(total, 1) * 4ull));
+            auto* vout = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(total, 1) * 4ull));
             const uint64_t items = (uint64_t)cb.dst_size * ((cb.K + 3) / 4);
-            k_indeg_fill<<<grid_for(items, T, maxb), T, 0, st>>>(cb, ccur, kin);
+            k_indeg_keys<<<grid_for(items, T, maxb), T, 0, st>>>(cb, kin, vin);
             NAER_CK(cudaGetLastError());
+            const int kbits = std::max<int>(1, (int)bit_width(cb.src_size - 1));
             with_cub_tmp(*this, [&](void* tmp, size_t& b) {
-                return cub::DeviceSegmentedSort::SortKeys(tmp, b, kin, kout, (int)total, (int)cb.src_size,
-                                                          off, off + 1, st);
+                return cub::DeviceRadixSort::SortPairs(tmp, b, kin, kout, vin, vout, (int)total, 0, kbits, st);
             });
-            k_indeg_finalize<<<grid_for(total, T, maxb), T, 0, st>>>(cb, kout, total, off, cursor, n.tgt,
+            k_indeg_finalize<<<grid_for(total, T, maxb), T, 0, st>>>(cb, kout, vout, total, off, cursor, n.tgt,
                                                                      n.w, n.dly);
             NAER_CK(cudaGetLastError());
-            NAER_CK(cudaStreamSynchronize(st));
-            dfree(kin, std::max<uint64_t>(total, 1) * 8ull);
-            dfree(kout, std::max<uint64_t>(total, 1) * 8ull);
+            dfree(kin, std::max<uint64_t>(total, 1) * 4ull);
+            dfree(kout, std::max<uint64_t>(total, 1) * 4ull);
+            dfree(vin, std::max<uint64_t>(total, 1) * 4ull);
+            dfree(vout, std::max<uint64_t>(total, 1) * 4ull);
             dfree(off, (cb.src_size + 1) * 8ull);
             dfree(cnt64, (cb.src_size + 1) * 8ull);
         }
@@ -594,7 +610,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
             dst = dalloc(bytes);
             cap_bytes = bytes;
         }
-        if (bytes) NAER_CK(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+        if (bytes) NAER_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
     };
     void* p = d_nets_;
     upload(p, nets_bytes_, h_nets_.data(), h_nets_.size() * sizeof(NetDev));
@@ -659,12 +675,12 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
         regrow(reinterpret_cast<void*&>(d_queue_[i]), queue_bytes_[i], qentries * sizeof(SpikeRec));
         regrow(reinterpret_cast<void*&>(d_qid_[i]), qid_bytes_[i], qentries * sizeof(uint32_t));
         regrow(reinterpret_cast<void*&>(d_counts_[i]), counts_bytes_[i], (lif_grid_ + 1) * sizeof(uint32_t));
-        NAER_CK(cudaMemset(d_counts_[i], 0, (lif_grid_ + 1) * sizeof(uint32_t)));
+        NAER_CK(cudaMemsetAsync(d_counts_[i], 0, (lif_grid_ + 1) * sizeof(uint32_t), stream_));
     }
     regrow(reinterpret_cast<void*&>(d_ev_part_), ev_part_bytes_, scatter_grid_ * sizeof(unsigned long long));
     regrow(reinterpret_cast<void*&>(d_ovf_part_), ovf_part_bytes_, scatter_grid_ * sizeof(unsigned long long));
-    NAER_CK(cudaMemset(d_ev_part_, 0, scatter_grid_ * sizeof(unsigned long long)));
-    NAER_CK(cudaMemset(d_ovf_part_, 0, scatter_grid_ * sizeof(unsigned long long)));
+    NAER_CK(cudaMemsetAsync(d_ev_part_, 0, scatter_grid_ * sizeof(unsigned long long), stream_));
+    NAER_CK(cudaMemsetAsync(d_ovf_part_, 0, scatter_grid_ * sizeof(unsigned long long), stream_));
     ev_part_n_ = scatter_grid_;
     queue_cap_ = (uint32_t)qentries;
     const size_t rbytes = std::max<uint64_t>(raster_capacity, 1) * sizeof(uint2);
@@ -696,6 +712,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     eng_.scatter_split =
         (uint32_t)std::min<uint64_t>(16, std::max<uint64_t>(1, (max_row + kScatterPiece - 1) / kScatterPiece));
     if (tuning_.scatter_split) eng_.scatter_split = std::min<uint32_t>(tuning_.scatter_split, 64);
+    NAER_CK(cudaStreamSynchronize(stream_));  // tables and buffers complete for every stream
 }
 
 void Engine::set_tuning(const Tuning& t) {
@@ -1179,13 +1196,23 @@ uint64_t Engine::read_raster_raw(uint64_t first, uint64_t cap, uint32_t* records
     return n;
 }
 
+uint64_t Engine::harvest_raster(uint2* dst, cudaEvent_t copied, uint64_t* dropped) {
+    const Ctl c = read_ctl();
+    const uint64_t n = std::min<uint64_t>(c.raster_next, eng_.raster_cap);
+    if (dropped) *dropped = c.raster_dropped;
+    DeviceGuard g(device_);
+    if (n) NAER_CK(cudaMemcpyAsync(dst, d_raster_, n * sizeof(uint2), cudaMemcpyDeviceToHost, stream_));
+    NAER_CK(cudaEventRecord(copied, stream_));
+    clear_raster();
+    return n;
+}
+
 void Engine::clear_raster() {
     DeviceGuard g(device_);
-    NAER_CK(cudaStreamSynchronize(stream_));
-    const unsigned long long z = 0;
-    NAER_CK(cudaMemcpy(&d_ctl_->raster_base, &z, 8, cudaMemcpyHostToDevice));
-    NAER_CK(cudaMemcpy(&d_ctl_->raster_next, &z, 8, cudaMemcpyHostToDevice));
-    NAER_CK(cudaMemcpy(&d_ctl_->raster_dropped, &z, 8, cudaMemcpyHostToDevice));
+    // raster_base, raster_next, raster_dropped: three adjacent words, reset
+    // in stream order
+    static_assert(offsetof(Ctl, raster_dropped) == offsetof(Ctl, raster_base) + 16, "Ctl layout");
+    NAER_CK(cudaMemsetAsync(&d_ctl_->raster_base, 0, 24, stream_));
 }
 
 void Engine::set_profiling(bool on) {

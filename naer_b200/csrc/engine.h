@@ -86,7 +86,8 @@ struct Tuning {
 
 class Engine {
 public:
-    explicit Engine(int device);
+    // priority: CUDA stream priority of the engine's stream (lower = higher)
+    explicit Engine(int device, int priority = 0);
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
@@ -124,6 +125,12 @@ public:
     // raster records [first, first+cap) -> (step, id); returns count copied
     uint64_t read_raster(uint64_t first, uint64_t cap, uint32_t* steps, uint32_t* ids);
     uint64_t read_raster_raw(uint64_t first, uint64_t cap, uint32_t* records);
+    // Waits for the queued steps, then queues the copy of all raster records
+    // into `dst` (pinned, >= raster capacity), records `copied` after it and
+    // clears the raster, all in stream order, so that further steps may be
+    // queued before the host reads `dst` (after `copied`).  Returns the
+    // record count; *dropped receives the records lost to a full raster.
+    uint64_t harvest_raster(uint2* dst, cudaEvent_t copied, uint64_t* dropped);
     void clear_raster();
 
     void set_profiling(bool on);

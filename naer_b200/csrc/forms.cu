@@ -153,6 +153,7 @@ Server::Server(int device, const ServerParams& p) : device_(device), prm_(p), t0
     int n = 0;
     NAER_CK(cudaGetDeviceCount(&n));
     if (device < 0 || device >= n) throw Error(NAER_E_INVALID, "device index out of range");
+    builder_ = std::thread([this] { build_loop(); });
     worker_ = std::thread([this] { loop(); });
 }
 
@@ -162,7 +163,10 @@ Server::~Server() {
         stop_ = true;
     }
     cv_work_.notify_all();
+    cv_build_.notify_all();
     if (worker_.joinable()) worker_.join();
+    cv_build_.notify_all();
+    if (builder_.joinable()) builder_.join();
 }
 
 double Server::now_s() const {
@@ -189,21 +193,21 @@ uint64_t Server::submit(const NetHost& description, uint64_t duration_steps) {
     jobs_[id] = std::move(j);
     pending_.push_back(id);
     ++st_.submitted;
-    cv_work_.notify_all();
+    cv_build_.notify_all();
     return id;
 }
 
 JobInfo Server::info(uint64_t job) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = jobs_.find(job);
-    if (it == jobs_.end()) throw Error(NAER_E_INVALID, "unknown job");
+    if (it == jobs_.end() || it->second->released) throw Error(NAER_E_INVALID, "unknown job");
     return it->second->info;
 }
 
 uint64_t Server::read_spikes(uint64_t job, uint64_t first, uint64_t cap, uint32_t* steps, uint32_t* ids) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = jobs_.find(job);
-    if (it == jobs_.end()) throw Error(NAER_E_INVALID, "unknown job");
+    if (it == jobs_.end() || it->second->released) throw Error(NAER_E_INVALID, "unknown job");
     const Job& j = *it->second;
     if (j.info.state != kJobDone) throw Error(NAER_E_STATE, "job has not finished");
     const uint64_t total = j.steps.size();
@@ -217,7 +221,7 @@ uint64_t Server::read_spikes(uint64_t job, uint64_t first, uint64_t cap, uint32_
 bool Server::wait(uint64_t job, double timeout_s) {
     std::unique_lock<std::mutex> lk(mu_);
     auto it = jobs_.find(job);
-    if (it == jobs_.end()) throw Error(NAER_E_INVALID, "unknown job");
+    if (it == jobs_.end() || it->second->released) throw Error(NAER_E_INVALID, "unknown job");
     Job* j = it->second.get();
     return cv_done_.wait_for(lk, std::chrono::duration<double>(timeout_s),
                              [&] { return j->info.state >= kJobDone; });
@@ -235,15 +239,16 @@ bool Server::drain(double timeout_s) {
 void Server::release(uint64_t job) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = jobs_.find(job);
-    if (it == jobs_.end()) throw Error(NAER_E_INVALID, "unknown job");
+    if (it == jobs_.end() || it->second->released) throw Error(NAER_E_INVALID, "unknown job");
     if (it->second->info.state < kJobDone) throw Error(NAER_E_STATE, "job has not finished");
-    jobs_.erase(it);
+    if (it->second->freed) jobs_.erase(it); else it->second->released = true;  // the builder erases it
 }
 
 ServerStats Server::stats() {
     std::lock_guard<std::mutex> lk(mu_);
     ServerStats s = st_;
-    s.queued = pending_.size();
+    s.queued = pending_.size() + ready_.size();
+    s.bytes_in_use = used_;
     std::vector<double> l = latencies_ms_;
     if (!l.empty()) {
         std::sort(l.begin(), l.end());
@@ -259,149 +264,276 @@ ServerStats Server::stats() {
     return s;
 }
 
-// Worker: admit -> build -> (re)install -> one chunk of steps -> hand the
-// chunk's raster to its jobs -> retire finished jobs.
-void Server::loop() {
+// Builder: admission by memory and job slots (first come, first served),
+// device build on its own engine and stream, and the frees of retired jobs.
+void Server::build_loop() {
     std::unique_ptr<Engine> eng;
-    std::vector<Job*> running;
-    uint64_t used = 0;
-    bool changed = false;
-    std::vector<uint2> rec;
-    auto fail_all = [&](const std::string& why) {
+    try {
+        NAER_CK(cudaSetDevice(device_));
+        int lo = 0, hi = 0;
+        NAER_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        eng = std::make_unique<Engine>(device_, hi);
+        for (;;) {
+            Job* j = nullptr;
+            std::vector<Job*> frees;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                auto head_fits = [&] {
+                    if (stop_ || pending_.empty() || live_ >= prm_.max_jobs) return false;
+                    return used_ + jobs_.at(pending_.front())->est_bytes <= prm_.budget_bytes;
+                };
+                cv_build_.wait(lk, [&] { return (stop_ && stepper_done_) || !to_free_.empty() || head_fits(); });
+                frees.assign(to_free_.begin(), to_free_.end());
+                to_free_.clear();
+                if (frees.empty()) {
+                    if (stop_ && stepper_done_) break;
+                    if (head_fits()) {
+                        j = jobs_.at(pending_.front()).get();
+                        pending_.pop_front();
+                        used_ += j->est_bytes;
+                        ++live_;
+                    }
+                }
+            }
+            for (Job* f : frees) {
+                eng->free_net(*f->net);
+                std::lock_guard<std::mutex> lk(mu_);
+                used_ -= f->est_bytes;
+                --live_;
+                f->freed = true;
+                if (f->released) jobs_.erase(f->id);
+            }
+            if (!j) continue;
+            const double t = now_s();
+            try {
+                eng->build(*j->net);
+                eng->sync();  // complete before another stream uses it
+            } catch (const Error& e) {
+                if (e.code == NAER_E_CUDA) throw;
+                if (j->net->compiled) eng->free_net(*j->net);
+                std::lock_guard<std::mutex> lk(mu_);
+                used_ -= j->est_bytes;
+                --live_;
+                j->freed = true;
+                j->info.state = kJobFailed;
+                j->info.error = e.what();
+                ++st_.failed;
+                cv_done_.notify_all();
+                continue;
+            }
+            std::lock_guard<std::mutex> lk(mu_);
+            st_.build_s += now_s() - t;
+            st_.peak_bytes = std::max<uint64_t>(st_.peak_bytes, eng->device_bytes());
+            ready_.push_back(j);
+            cv_work_.notify_all();
+        }
+        // shutting down: whatever was built but never stepped
+        std::vector<Job*> rest;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            rest.assign(ready_.begin(), ready_.end());
+            ready_.clear();
+        }
+        for (Job* j : rest) eng->free_net(*j->net);
+    } catch (const std::exception& e) {
         std::lock_guard<std::mutex> lk(mu_);
-        fatal_ = why;
+        fatal_ = e.what();
         for (auto& kv : jobs_) {
             if (kv.second->info.state < kJobDone) {
                 kv.second->info.state = kJobFailed;
-                kv.second->info.error = why;
+                kv.second->info.error = fatal_;
                 ++st_.failed;
             }
         }
         pending_.clear();
-        st_.running = 0;
+        stop_ = true;
         cv_done_.notify_all();
-    };
+        cv_work_.notify_all();
+    }
+}
+
+// Stepper: one iteration per chunk of steps.  It takes built jobs in,
+// collects the raster of the chunk in flight (waiting for it), retires the
+// jobs whose last step that chunk ran, re-installs the tables if the set
+// changed, queues the next chunk and only then hands the collected records
+// to their jobs on the host, while the device runs the next chunk.
+void Server::loop() {
+    std::unique_ptr<Engine> eng;
+    std::vector<Job*> running;        // set of the next chunk
+    std::vector<Job*> inflight_set;   // set of the chunk in flight
+    std::vector<uint32_t> inflight_off;
+    bool inflight = false;
+    bool changed = false;
+    uint2* rec = nullptr;  // pinned staging of one chunk's raster
+    cudaEvent_t copied = nullptr;
+    std::vector<uint32_t> owner, count;
     try {
         NAER_CK(cudaSetDevice(device_));
         eng = std::make_unique<Engine>(device_);
+        // short persistent launches: the builder's kernels get the device
+        // between them (its stream has the higher priority)
+        Tuning tn;
+        tn.launch_steps = 4;
+        eng->set_tuning(tn);
+        NAER_CK(cudaHostAlloc(reinterpret_cast<void**>(&rec), prm_.raster_capacity * sizeof(uint2),
+                              cudaHostAllocDefault));
+        NAER_CK(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
         for (;;) {
             std::vector<Job*> admit;
             {
                 std::unique_lock<std::mutex> lk(mu_);
-                if (running.empty()) cv_work_.wait(lk, [&] { return stop_ || !pending_.empty(); });
+                if (running.empty() && !inflight) cv_work_.wait(lk, [&] { return stop_ || !ready_.empty(); });
                 if (stop_) break;
-                // first come, first served: the queue head waits for memory
-                while (!pending_.empty() && running.size() + admit.size() < prm_.max_jobs) {
-                    Job* j = jobs_.at(pending_.front()).get();
-                    if (used + j->est_bytes > prm_.budget_bytes) break;
-                    pending_.pop_front();
-                    admit.push_back(j);
-                    used += j->est_bytes;
+                admit.assign(ready_.begin(), ready_.end());
+                ready_.clear();
+                const double t = now_s();
+                for (Job* j : admit) {
+                    j->info.state = kJobRunning;
+                    j->info.admit_s = t;
+                    j->info.device_bytes = j->net->device_bytes;
                 }
             }
+            double t = now_s();
+            // the chunk in flight: wait, queue its raster copy
+            uint64_t nrec = 0, dropped = 0;
+            if (inflight) nrec = eng->harvest_raster(rec, copied, &dropped);
+            const double t_step = inflight ? now_s() - t : 0.0;
+            const uint64_t hs = eng->host_step();
+            // jobs whose last step has run
+            std::vector<Job*> keep, finished;
+            for (Job* j : running) {
+                if (hs >= j->net->dev.end_step) finished.push_back(j); else keep.push_back(j);
+            }
+            if (!finished.empty()) changed = true;
+            running.swap(keep);
             for (Job* j : admit) {
-                try {
-                    eng->build(*j->net);
-                } catch (const Error& e) {
-                    if (e.code == NAER_E_CUDA) throw;
-                    if (j->net->compiled) eng->free_net(*j->net);
-                    used -= j->est_bytes;
-                    std::lock_guard<std::mutex> lk(mu_);
-                    j->info.state = kJobFailed;
-                    j->info.error = e.what();
-                    ++st_.failed;
-                    cv_done_.notify_all();
-                    continue;
-                }
-                j->net->dev.start_step = eng->host_step();
-                j->net->dev.end_step = eng->host_step() + j->info.duration;
+                j->net->dev.start_step = hs;
+                j->net->dev.end_step = hs + j->info.duration;
                 running.push_back(j);
                 changed = true;
-                std::lock_guard<std::mutex> lk(mu_);
-                j->info.state = kJobRunning;
-                j->info.admit_s = now_s();
-                j->info.device_bytes = j->net->device_bytes;
             }
-            if (running.empty()) continue;
-            if (changed) {
+            t = now_s();
+            double t_install = 0;
+            if (changed && !running.empty()) {
                 std::vector<NetHost*> nets;
                 for (Job* j : running) nets.push_back(j->net.get());
                 eng->install(nets, prm_.raster_capacity, true, prm_.aggregation);
                 changed = false;
+                t_install = now_s() - t;
             }
-            const uint64_t hs = eng->host_step();
-            uint64_t last_end = hs;
-            for (Job* j : running) last_end = std::max<uint64_t>(last_end, j->net->dev.end_step);
-            eng->run(std::min<uint64_t>(prm_.chunk_steps, last_end - hs));
-
-            // the chunk's raster, handed to the jobs it belongs to
-            const Ctl c = eng->read_ctl();
-            const uint64_t nrec = std::min<uint64_t>(c.raster_next, prm_.raster_capacity);
-            rec.resize(nrec);
-            if (nrec) eng->read_raster_raw(0, nrec, reinterpret_cast<uint32_t*>(rec.data()));
-            eng->clear_raster();
-            const auto& off = eng->id_offsets();
-            for (const uint2& r : rec) {
-                const uint32_t m = member_of(off, r.y);
-                Job* j = running[m];
-                j->steps.push_back((uint32_t)(r.x - j->net->dev.start_step));
-                j->ids.push_back(r.y - off[m]);
+            // queue the next chunk
+            std::vector<Job*> prev_set;
+            std::vector<uint32_t> prev_off;
+            prev_set.swap(inflight_set);
+            prev_off.swap(inflight_off);
+            if (!running.empty()) {
+                uint64_t last_end = hs;
+                for (Job* j : running) last_end = std::max<uint64_t>(last_end, j->net->dev.end_step);
+                eng->run(std::min<uint64_t>(prm_.chunk_steps, last_end - hs));
+                inflight = true;
+                inflight_set = running;
+                inflight_off = eng->id_offsets();
+            } else {
+                inflight = false;
             }
-            const uint64_t now_step = eng->host_step();
-            std::vector<Job*> keep;
-            std::vector<Job*> finished;
-            for (Job* j : running) {
-                if (now_step >= j->net->dev.end_step) finished.push_back(j); else keep.push_back(j);
+            // hand the collected records to their jobs while the device runs
+            t = now_s();
+            NAER_CK(cudaEventSynchronize(copied));
+            owner.resize(nrec);
+            count.assign(prev_set.size(), 0);
+            for (uint64_t i = 0; i < nrec; ++i) {
+                owner[i] = member_of(prev_off, rec[i].y);
+                ++count[owner[i]];
+            }
+            std::vector<size_t> at(prev_set.size());
+            for (size_t m = 0; m < prev_set.size(); ++m) {
+                Job* j = prev_set[m];
+                at[m] = j->steps.size();
+                j->steps.resize(at[m] + count[m]);
+                j->ids.resize(at[m] + count[m]);
+            }
+            for (uint64_t i = 0; i < nrec; ++i) {
+                const uint32_t m = owner[i];
+                Job* j = prev_set[m];
+                j->steps[at[m]] = (uint32_t)(rec[i].x - j->net->dev.start_step);
+                j->ids[at[m]] = rec[i].y - prev_off[m];
+                ++at[m];
             }
             for (Job* j : finished) {
-                eng->free_net(*j->net);
-                used -= j->est_bytes;
-                // records of one step arrive unordered: order by (step, id)
-                std::vector<uint64_t> key(j->steps.size());
-                for (size_t i = 0; i < key.size(); ++i) key[i] = ((uint64_t)j->steps[i] << 32) | j->ids[i];
-                std::sort(key.begin(), key.end());
-                for (size_t i = 0; i < key.size(); ++i) {
-                    j->steps[i] = (uint32_t)(key[i] >> 32);
-                    j->ids[i] = (uint32_t)key[i];
+                // records arrive step by step (the raster is appended in step
+                // order), unordered within a step: sort each step's ids
+                size_t a = 0;
+                while (a < j->steps.size()) {
+                    size_t b = a + 1;
+                    while (b < j->steps.size() && j->steps[b] == j->steps[a]) ++b;
+                    std::sort(j->ids.begin() + a, j->ids.begin() + b);
+                    a = b;
                 }
             }
-            if (!finished.empty()) changed = true;
-            running.swap(keep);
+            const double t_drain = now_s() - t;
             {
                 std::lock_guard<std::mutex> lk(mu_);
-                const double t = now_s();
+                const double tn2 = now_s();
                 for (Job* j : finished) {
                     j->info.state = kJobDone;
-                    j->info.done_s = t;
+                    j->info.done_s = tn2;
                     j->info.steps_done = j->info.duration;
                     j->info.spikes = j->steps.size();
-                    latencies_ms_.push_back(1e3 * (t - j->info.submit_s));
-                    last_done_s_ = t;
+                    latencies_ms_.push_back(1e3 * (tn2 - j->info.submit_s));
+                    last_done_s_ = tn2;
                     ++st_.done;
+                    to_free_.push_back(j);  // no queued launch uses it any more
                 }
-                for (Job* j : running) j->info.steps_done = now_step - j->net->dev.start_step;
-                ++st_.chunks;
-                st_.engine_steps = now_step;
-                st_.bytes_in_use = used;
-                st_.peak_bytes = std::max<uint64_t>(st_.peak_bytes, eng->device_bytes());
-                st_.raster_dropped += c.raster_dropped;
+                for (Job* j : running) j->info.steps_done = std::min<uint64_t>(hs - j->net->dev.start_step, j->info.duration);
+                if (inflight) ++st_.chunks;
+                st_.engine_steps = eng->host_step();
+                st_.install_s += t_install;
+                st_.step_s += t_step;
+                st_.drain_s += t_drain;
+                st_.raster_dropped += dropped;
                 st_.running = running.size();
-                if (!finished.empty()) cv_done_.notify_all();
+                if (!finished.empty()) {
+                    cv_done_.notify_all();
+                    cv_build_.notify_all();
+                }
             }
         }
-        // shutting down: abandon what is still running
-        for (Job* j : running) eng->free_net(*j->net);
+        if (inflight) eng->sync();
+    } catch (const std::exception& e) {
         std::lock_guard<std::mutex> lk(mu_);
+        fatal_ = e.what();
         for (auto& kv : jobs_) {
             if (kv.second->info.state < kJobDone) {
                 kv.second->info.state = kJobFailed;
-                kv.second->info.error = "server stopped";
+                kv.second->info.error = fatal_;
+                ++st_.failed;
             }
         }
+        pending_.clear();
+        stop_ = true;
         cv_done_.notify_all();
-    } catch (const std::exception& e) {
-        fail_all(e.what());
     }
+    if (eng) cudaStreamSynchronize(eng->stream());
+    if (rec) cudaFreeHost(rec);
+    if (copied) cudaEventDestroy(copied);
+    // running jobs are abandoned: the builder frees them
+    std::lock_guard<std::mutex> lk(mu_);
+    for (Job* j : running) {
+        if (j->info.state < kJobDone) {
+            j->info.state = kJobFailed;
+            j->info.error = "server stopped";
+        }
+        to_free_.push_back(j);
+    }
+    for (auto& kv : jobs_) {
+        if (kv.second->info.state < kJobDone) {
+            kv.second->info.state = kJobFailed;
+            if (kv.second->info.error.empty()) kv.second->info.error = "server stopped";
+        }
+    }
+    stepper_done_ = true;
+    cv_done_.notify_all();
+    cv_build_.notify_all();
 }
 
 }  // namespace naer

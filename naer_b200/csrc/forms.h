@@ -76,12 +76,21 @@ struct ServerStats {
     uint64_t chunks = 0, engine_steps = 0, peak_bytes = 0, bytes_in_use = 0, raster_dropped = 0;
     double p50_ms = 0, p99_ms = 0, mean_ms = 0;
     double sims_per_s = 0;  // jobs done / (last done - first submit)
+    // host seconds spent by the two server threads
+    double build_s = 0;     // builder: networks built on the device
+    double install_s = 0, step_s = 0, drain_s = 0;  // stepper: tables, chunks, rasters
 };
 
 // Served form: jobs (description, duration) are admitted as device memory
 // and slots free up, stepped together with the jobs already running (their
 // state stays on the device), and retired when their duration is reached.
-// A worker thread owns the engine; the public methods are thread-safe.
+// Two threads: the builder admits queued jobs first come, first served
+// while their estimated bytes fit the budget, builds them on its own engine
+// and stream (build kernels interleave with the step launches), and frees
+// retired jobs; the stepper owns the step engine, takes built jobs in at
+// every chunk boundary, runs the chunk, hands its raster to the jobs and
+// retires those that reached their duration.  Public methods are
+// thread-safe.
 class Server {
 public:
     Server(int device, const ServerParams& p);
@@ -102,24 +111,32 @@ private:
         JobInfo info;
         uint64_t est_bytes = 0;
         std::vector<uint32_t> steps, ids;
+        bool freed = false;     // holds no device memory
+        bool released = false;  // forgotten by the caller: erase once freed
     };
     void loop();
+    void build_loop();
     double now_s() const;
 
     int device_;
     ServerParams prm_;
     std::chrono::steady_clock::time_point t0_;
     std::mutex mu_;
-    std::condition_variable cv_work_, cv_done_;
+    std::condition_variable cv_work_, cv_done_, cv_build_;
     std::map<uint64_t, std::unique_ptr<Job>> jobs_;
-    std::deque<uint64_t> pending_;
+    std::deque<uint64_t> pending_;   // submitted, not yet built
+    std::deque<Job*> ready_;         // built, not yet stepping
+    std::deque<Job*> to_free_;       // retired, device memory still held
+    uint64_t used_ = 0;              // estimated bytes of built, unfreed jobs
+    uint32_t live_ = 0;              // built, unfreed jobs
     uint64_t next_id_ = 1;
     bool stop_ = false;
+    bool stepper_done_ = false;
     std::string fatal_;
     ServerStats st_{};
     std::vector<double> latencies_ms_;
     double first_submit_s_ = -1, last_done_s_ = 0;
-    std::thread worker_;
+    std::thread worker_, builder_;
 };
 
 }  // namespace naer
