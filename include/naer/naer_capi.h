@@ -313,10 +313,11 @@ typedef struct naer_server naer_server;
 typedef struct naer_server_params {
     uint64_t budget_bytes;     /* device bytes of admitted networks, at most */
     uint64_t raster_capacity;  /* spike records per chunk (excess is dropped and counted) */
-    uint32_t chunk_steps;      /* grid steps between admission points */
+    uint32_t chunk_steps;      /* grid steps between admission points, at most */
     uint32_t aggregation;      /* NAER_AGG_* for every job */
     uint32_t max_jobs;         /* jobs stepped together, at most */
-    uint32_t pad_;
+    uint32_t blocks_per_sm;    /* step-kernel blocks per SM (0 = most that fit) */
+    double chunk_ms;           /* target device time of a chunk: fewer steps when many jobs run */
 } naer_server_params;
 
 #define NAER_JOB_QUEUED 0u

@@ -120,7 +120,8 @@ class ServerParams(C.Structure):
         ("chunk_steps", C.c_uint32),
         ("aggregation", C.c_uint32),
         ("max_jobs", C.c_uint32),
-        ("pad_", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("chunk_ms", C.c_double),
     ]
 
 

@@ -573,6 +573,8 @@ int naer_server_params_default(naer_server_params* p) {
     p->chunk_steps = 256;
     p->aggregation = NAER_AGG_ATOMIC;
     p->max_jobs = 1024;
+    p->blocks_per_sm = 0;
+    p->chunk_ms = 10.0;
     return NAER_OK;
 }
 
@@ -588,6 +590,8 @@ int naer_server_create(int device, const naer_server_params* params, naer_server
         sp.chunk_steps = p.chunk_steps;
         sp.aggregation = p.aggregation;
         sp.max_jobs = p.max_jobs;
+        sp.blocks_per_sm = p.blocks_per_sm;
+        sp.chunk_ms = p.chunk_ms;
         auto h = std::make_unique<naer_server>();
         h->s = std::make_unique<naer::Server>(device, sp);
         *out = h.release();

@@ -295,6 +295,8 @@ void Engine::build(NetHost& n) {
     cudaStream_t st = stream_;
     const uint64_t bytes0 = bytes_;
 
+    unsigned long long* stats = nullptr;  // [synapses, longest padded row, padded size]
+
     // --- connectivity: counts per (connection, source)
     uint64_t* len = static_cast<uint64_t*>(dalloc(Ns * 8ull));
     NAER_CK(cudaMemsetAsync(len, 0, Ns * 8ull, st));
@@ -316,14 +318,30 @@ void Engine::build(NetHost& n) {
                                                                     cb.src_storage, len);
         NAER_CK(cudaGetLastError());
     }
+    // Fixed-degree rules: the synapse count is known here, so the arrays are
+    // sized by a bound (each row padded by at most 3 per padding) and the
+    // whole build is queued without waiting for the device; a Bernoulli
+    // connection needs the device's count first.
+    bool exact = true;
+    uint64_t syn_exact = 0;
+    for (const auto& c : n.conns) {
+        const auto& sp = c.spec;
+        if (sp.rule == NAER_CONN_REF_BERNOULLI) exact = false;
+        else if (sp.rule == NAER_CONN_FIXED_OUTDEGREE) syn_exact += (uint64_t)sp.degree * n.pops[c.src].size;
+        else syn_exact += (uint64_t)sp.degree * n.pops[c.dst].size;
+    }
     uint64_t* padded = static_cast<uint64_t*>(dalloc((Ns + 1) * 8ull));
     k_row_pad<<<grid_for(Ns + 1, T, maxb), T, 0, st>>>(len, Ns, padded);
     n.row_ptr = static_cast<uint64_t*>(dalloc((Ns + 1) * 8ull));
     with_cub_tmp(*this, [&](void* tmp, size_t& b) {
         return cub::DeviceScan::ExclusiveSum(tmp, b, padded, n.row_ptr, (int)(Ns + 1), st);
     });
-    NAER_CK(cudaMemcpyAsync(&n.synapses_padded, n.row_ptr + Ns, 8, cudaMemcpyDeviceToHost, st));
-    NAER_CK(cudaStreamSynchronize(st));
+    if (exact) {
+        n.synapses_padded = syn_exact + 3ull * Ns;
+    } else {
+        NAER_CK(cudaMemcpyAsync(&n.synapses_padded, n.row_ptr + Ns, 8, cudaMemcpyDeviceToHost, st));
+        NAER_CK(cudaStreamSynchronize(st));
+    }
     const uint64_t S = n.synapses_padded;
     n.tgt = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(S, 4) * 4ull));
     n.w = static_cast<float*>(dalloc(std::max<uint64_t>(S, 4) * 4ull));
@@ -392,8 +410,12 @@ void Engine::build(NetHost& n) {
             return cub::DeviceScan::ExclusiveSum(tmp, b, padded2, row_ptr2, (int)(Ns + 1), st);
         });
         uint64_t S2 = 0;
-        NAER_CK(cudaMemcpyAsync(&S2, row_ptr2 + Ns, 8, cudaMemcpyDeviceToHost, st));
-        NAER_CK(cudaStreamSynchronize(st));
+        if (exact) {
+            S2 = syn_exact + 6ull * Ns;  // two padded parts per row
+        } else {
+            NAER_CK(cudaMemcpyAsync(&S2, row_ptr2 + Ns, 8, cudaMemcpyDeviceToHost, st));
+            NAER_CK(cudaStreamSynchronize(st));
+        }
         uint32_t* tgt2 = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(S2, 4) * 4ull));
         float* w2 = static_cast<float*>(dalloc(std::max<uint64_t>(S2, 4) * 4ull));
         uint8_t* dly2 = static_cast<uint8_t*>(dalloc(std::max<uint64_t>(S2, 16)));
@@ -401,9 +423,13 @@ void Engine::build(NetHost& n) {
         k_partition_d1<<<grid_for((uint64_t)Ns * 32, T, maxb), T, 0, st>>>(
             n.row_ptr, len, n1, Ns, row_ptr2, n.tgt, n.w, n.dly, tgt2, w2, dly2, n.row_mid);
         NAER_CK(cudaGetLastError());
-        std::vector<uint64_t> hpad(Ns);
-        NAER_CK(cudaMemcpyAsync(hpad.data(), padded2, Ns * 8ull, cudaMemcpyDeviceToHost, st));
-        NAER_CK(cudaStreamSynchronize(st));
+        // synapse count, longest padded row and the final padded size, read
+        // back with the build's one synchronisation (below)
+        stats = static_cast<unsigned long long*>(dalloc(3 * 8ull));
+        NAER_CK(cudaMemsetAsync(stats, 0, 3 * 8ull, st));
+        k_row_stats<<<grid_for(Ns, T, maxb), T, 0, st>>>(len, padded2, Ns, stats);
+        NAER_CK(cudaMemcpyAsync(stats + 2, row_ptr2 + Ns, 8, cudaMemcpyDeviceToDevice, st));
+        NAER_CK(cudaGetLastError());
         dfree(n.tgt, std::max<uint64_t>(S, 4) * 4ull);
         dfree(n.w, std::max<uint64_t>(S, 4) * 4ull);
         dfree(n.dly, std::max<uint64_t>(S, 16));
@@ -414,15 +440,8 @@ void Engine::build(NetHost& n) {
         n.w = w2;
         n.dly = dly2;
         n.row_ptr = row_ptr2;
-        n.synapses_padded = S2;
-        n.max_row_padded = 0;
-        for (uint64_t x : hpad) n.max_row_padded = std::max<uint64_t>(n.max_row_padded, x);
+        n.syn_capacity = S2;
     }
-    std::vector<uint64_t> hlen(Ns);
-    NAER_CK(cudaMemcpyAsync(hlen.data(), len, Ns * 8ull, cudaMemcpyDeviceToHost, st));
-    NAER_CK(cudaStreamSynchronize(st));
-    n.synapses = 0;
-    for (uint64_t x : hlen) n.synapses += x;
     for (size_t ci = 0; ci < cnt.size(); ++ci)
         dfree(cnt[ci], std::max<uint64_t>(n.pops[n.conns[ci].src].size, 1) * 4ull);
     dfree(len, Ns * 8ull);
@@ -470,7 +489,13 @@ void Engine::build(NetHost& n) {
         NAER_CK(cudaMemcpyAsync(n.e_plus, ep.data(), n.e_len * 4ull, cudaMemcpyHostToDevice, st));
         NAER_CK(cudaMemcpyAsync(n.e_minus, em.data(), n.e_len * 4ull, cudaMemcpyHostToDevice, st));
     }
+    unsigned long long hstats[3] = {0, 0, 0};
+    NAER_CK(cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, st));
+    dfree(stats, 3 * 8ull);
     NAER_CK(cudaStreamSynchronize(st));
+    n.synapses = hstats[0];
+    n.max_row_padded = hstats[1];
+    n.synapses_padded = hstats[2];
 
     NetDev& d = n.dev;
     d = NetDev{};
@@ -508,7 +533,7 @@ void Engine::build(NetHost& n) {
 void Engine::free_net(NetHost& n) {
     DeviceGuard g(device_);
     const uint32_t Ns = n.n_storage;
-    const uint64_t S = n.synapses_padded;
+    const uint64_t S = n.syn_capacity ? n.syn_capacity : n.synapses_padded;  // entries allocated
     dfree(n.v, Ns * 4ull);
     dfree(n.refr, Ns);
     dfree(n.ring, (uint64_t)n.ring_slots * Ns * 4ull);

@@ -47,6 +47,7 @@ struct NetHost {
     uint32_t n_ids = 0, n_storage = 0, n_plastic = 0, ring_slots = 0;
     uint32_t n_poisson = 0;
     uint64_t synapses = 0, synapses_padded = 0, max_row_padded = 0;
+    uint64_t syn_capacity = 0;  // entries allocated for tgt / w / dly (>= synapses_padded)
     std::vector<int32_t> id_of_storage;   // -1 for padding
     std::vector<uint32_t> storage_of_id;
 

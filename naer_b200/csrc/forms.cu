@@ -273,6 +273,21 @@ void Server::build_loop() {
         int lo = 0, hi = 0;
         NAER_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
         eng = std::make_unique<Engine>(device_, hi);
+        // Reserve the budget in the stream-ordered pool up front (allocate
+        // and free: the pool keeps it): later builds then reuse mapped memory
+        // instead of growing the pool while step kernels run.
+        {
+            size_t free_b = 0, total_b = 0;
+            NAER_CK(cudaMemGetInfo(&free_b, &total_b));
+            const uint64_t margin = 8ull << 30;
+            const uint64_t warm = std::min<uint64_t>(prm_.budget_bytes, free_b > margin ? free_b - margin : 0);
+            if (warm) {
+                void* p = nullptr;
+                if (cudaMallocAsync(&p, warm, eng->stream()) == cudaSuccess) NAER_CK(cudaFreeAsync(p, eng->stream()));
+                else (void)cudaGetLastError();
+                eng->sync();
+            }
+        }
         for (;;) {
             Job* j = nullptr;
             std::vector<Job*> frees;
@@ -367,17 +382,27 @@ void Server::loop() {
     uint2* rec = nullptr;  // pinned staging of one chunk's raster
     cudaEvent_t copied = nullptr;
     std::vector<uint32_t> owner, count;
+    // Chunks are bounded in device time, not only in steps: a chunk's step
+    // count follows the measured time per step, so a large running set does
+    // not stretch the interval between admission points (which would let
+    // more jobs queue up and stretch it further).
+    double ms_per_step = 0.0;
+    uint64_t chunk_len = 0;
+    cudaEvent_t c0 = nullptr, c1 = nullptr;  // device time of the chunk in flight
     try {
         NAER_CK(cudaSetDevice(device_));
         eng = std::make_unique<Engine>(device_);
-        // short persistent launches: the builder's kernels get the device
-        // between them (its stream has the higher priority)
+        // short persistent launches: the builder's kernels (higher-priority
+        // stream) get the device between them instead of after whole chunks
         Tuning tn;
         tn.launch_steps = 4;
+        tn.blocks_per_sm = prm_.blocks_per_sm;
         eng->set_tuning(tn);
         NAER_CK(cudaHostAlloc(reinterpret_cast<void**>(&rec), prm_.raster_capacity * sizeof(uint2),
                               cudaHostAllocDefault));
         NAER_CK(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+        NAER_CK(cudaEventCreate(&c0));
+        NAER_CK(cudaEventCreate(&c1));
         for (;;) {
             std::vector<Job*> admit;
             {
@@ -398,6 +423,12 @@ void Server::loop() {
             uint64_t nrec = 0, dropped = 0;
             if (inflight) nrec = eng->harvest_raster(rec, copied, &dropped);
             const double t_step = inflight ? now_s() - t : 0.0;
+            if (inflight && chunk_len > 0) {
+                float ms = 0.0f;
+                NAER_CK(cudaEventElapsedTime(&ms, c0, c1));
+                const double m = (double)ms / (double)chunk_len;
+                ms_per_step = ms_per_step > 0.0 ? 0.5 * (ms_per_step + m) : m;
+            }
             const uint64_t hs = eng->host_step();
             // jobs whose last step has run
             std::vector<Job*> keep, finished;
@@ -429,7 +460,13 @@ void Server::loop() {
             if (!running.empty()) {
                 uint64_t last_end = hs;
                 for (Job* j : running) last_end = std::max<uint64_t>(last_end, j->net->dev.end_step);
-                eng->run(std::min<uint64_t>(prm_.chunk_steps, last_end - hs));
+                uint64_t len = prm_.chunk_steps;
+                if (ms_per_step > 0.0 && prm_.chunk_ms > 0.0)
+                    len = std::min<uint64_t>(len, std::max<uint64_t>(16, (uint64_t)(prm_.chunk_ms / ms_per_step)));
+                chunk_len = std::min<uint64_t>(len, last_end - hs);
+                NAER_CK(cudaEventRecord(c0, eng->stream()));
+                eng->run(chunk_len);
+                NAER_CK(cudaEventRecord(c1, eng->stream()));
                 inflight = true;
                 inflight_set = running;
                 inflight_off = eng->id_offsets();
@@ -516,6 +553,8 @@ void Server::loop() {
     if (eng) cudaStreamSynchronize(eng->stream());
     if (rec) cudaFreeHost(rec);
     if (copied) cudaEventDestroy(copied);
+    if (c0) cudaEventDestroy(c0);
+    if (c1) cudaEventDestroy(c1);
     // running jobs are abandoned: the builder frees them
     std::lock_guard<std::mutex> lk(mu_);
     for (Job* j : running) {

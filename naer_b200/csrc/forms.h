@@ -59,6 +59,8 @@ struct ServerParams {
     uint32_t aggregation = 0;      // NAER_AGG_*
     uint32_t max_jobs = 1024;      // networks stepped together at most
     uint64_t raster_capacity = 1ull << 24;  // spike records per chunk
+    uint32_t blocks_per_sm = 0;    // step-kernel blocks per SM (0 = most that fit)
+    double chunk_ms = 10.0;        // target device time per chunk (sets its step count)
 };
 
 enum JobState : uint32_t { kJobQueued = 0, kJobRunning = 1, kJobDone = 2, kJobFailed = 3 };
