@@ -146,12 +146,15 @@ def dist_init():
 
 
 def reduce_max_sum(world, tmax, esum):
+    """Max of the ranks' times and sum of their events (every rank gets both):
+    the job's time is its slowest replica's, its work the sum of all."""
     if world == 1:
         return tmax, esum
     import torch
     import torch.distributed as dist
-    t = torch.tensor([tmax], dtype=torch.float64, device="cuda")
-    e = torch.tensor([esum], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([tmax], dtype=torch.float64, device=dev)
+    e = torch.tensor([esum], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     dist.all_reduce(e, op=dist.ReduceOp.SUM)
     return float(t.item()), float(e.item())
