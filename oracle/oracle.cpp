@@ -683,4 +683,144 @@ int oracle_max_threads() {
 #endif
 }
 
+// ---------------------------------------------------------------------------
+// FP64 re-integration of a finished run.  The network restarts from its
+// initial state and every arithmetic step is done in double, with exact
+// exp() decay factors, but the spike times are the run's own (its raster),
+// not recomputed from thresholds: this is the trajectory the run's fp32
+// arithmetic approximates for the same spike inputs.  A POISSON source's
+// multiplicity and every drive count come from the same Poisson windows.
+// Outputs the final membrane potentials (address order) and the final
+// weights (address-order CSR, as oracle_net_copy_weights); *mismatch counts
+// (step, neuron) pairs where the double trajectory's threshold test
+// disagrees with the raster (V > V_th without a recorded spike, or a
+// recorded spike while refractory), a diagnostic only.
+int oracle_reintegrate_fp64(void* h, uint64_t nsteps, const uint32_t* sp_step, const uint32_t* sp_id, uint64_t nsp,
+                            double* v_out, double* w_out, uint64_t* mismatch) {
+    const Net& net = *static_cast<Net*>(h);
+    const OrParams& P = net.prm;
+    const uint32_t n = net.n, D = net.D;
+    std::vector<double> v(n, 0.0), ring((size_t)D * n, 0.0), w(net.w.begin(), net.w.end());
+    std::vector<uint32_t> refr(n, 0);
+    for (size_t p = 0; p < net.pops.size(); ++p)
+        if (net.pops[p].type != 2)
+            for (uint32_t k = 0; k < net.pops[p].size; ++k) v[net.base[p] + k] = net.pops[p].v_init;
+    uint32_t n_stdp = 0;
+    for (const auto& p : net.pops)
+        if (p.type == 0) n_stdp += p.size;
+    const bool plastic = P.stdp_enabled && n_stdp > 0;
+    std::vector<int32_t> last_post(n, -1), last_pre(n, -1), hist(plastic ? (size_t)n * P.stdp_history : 0, -1);
+    std::vector<double> y_post(n, 0.0), x_pre(n, 0.0);
+    const double tau_p = (double)P.tau_plus_ms * 1000.0, tau_m = (double)P.tau_minus_ms * 1000.0;
+    const double ap = (double)P.a_plus * P.w_max, am = (double)P.a_minus * P.w_max, wmax = P.w_max;
+    std::vector<double> prop(net.pops.size());
+    std::vector<uint32_t> tref(net.pops.size());
+    for (size_t p = 0; p < net.pops.size(); ++p) {
+        prop[p] = std::exp(-(double)P.dt_us / ((double)net.pops[p].tau_m_ms * 1000.0));
+        tref[p] = (uint32_t)std::llround((double)net.pops[p].t_ref_ms * 1000.0 / P.dt_us);
+    }
+    std::vector<uint8_t> fired(n, 0);
+    uint64_t mis = 0, k = 0;
+    for (uint64_t t = 0; t < nsteps; ++t) {
+        const uint32_t t0 = (uint32_t)t * P.dt_us, t1 = t0 + P.dt_us;
+        const uint32_t slot = (uint32_t)(t % D);
+        std::vector<uint32_t> spk;
+        while (k < nsp && sp_step[k] < t) ++k;
+        while (k < nsp && sp_step[k] == t) {
+            if (sp_id[k] < n) {
+                fired[sp_id[k]] = 1;
+                spk.push_back(sp_id[k]);
+            }
+            ++k;
+        }
+        std::vector<uint32_t> mult(spk.size(), 1);
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t pi = net.pop_of[i];
+            const OrPop& pop = net.pops[pi];
+            if (pop.type == 2) continue;
+            const double I = ring[(size_t)slot * n + i];
+            ring[(size_t)slot * n + i] = 0.0;
+            if (refr[i] > 0) {
+                refr[i] -= 1;
+                if (fired[i]) ++mis;
+                continue;
+            }
+            double x = v[i] * prop[pi] + I;
+            if (pop.drive_rate_hz > 0.0f) {
+                const uint32_t m = poisson_window(i - net.base[pi], pop.size, pop.drive_seed,
+                                                  (double)pop.drive_rate_hz, t0, t1, nullptr);
+                x += (double)m * (double)pop.drive_weight;
+            }
+            if (fired[i]) {
+                x = pop.v_reset;
+                refr[i] = tref[pi];
+                if (plastic && pop.type == 0) {
+                    const int32_t ts = (int32_t)t;
+                    const int32_t lp = last_post[i];
+                    const double y = lp >= 0 ? y_post[i] * std::exp(-(double)(ts - lp) * P.dt_us / tau_m) : 0.0;
+                    y_post[i] = y + 1.0;
+                    last_post[i] = ts;
+                    int32_t* hh = &hist[(size_t)i * P.stdp_history];
+                    for (int q = (int)P.stdp_history - 1; q > 0; --q) hh[q] = hh[q - 1];
+                    hh[0] = ts;
+                }
+            } else if (x > (double)pop.v_th) {
+                ++mis;
+            }
+            v[i] = x;
+        }
+        // pre state before this step's spikes, for the lazy STDP of their rows
+        std::vector<int32_t> pre_last(spk.size(), -1);
+        std::vector<double> pre_x(spk.size(), 0.0);
+        for (size_t a = 0; a < spk.size(); ++a) {
+            const uint32_t i = spk[a];
+            const OrPop& pop = net.pops[net.pop_of[i]];
+            if (pop.type == 2) {
+                const uint32_t idx = net.type_addr[net.pop_of[i]] + (i - net.base[net.pop_of[i]]);
+                mult[a] = poisson_window(idx, net.n_poisson, P.poisson_seed, (double)pop.rate_hz, t0, t1, nullptr);
+            } else if (plastic && pop.type == 0) {
+                const int32_t ts = (int32_t)t;
+                pre_last[a] = last_pre[i];
+                pre_x[a] = x_pre[i];
+                const double x = last_pre[i] >= 0 ? x_pre[i] * std::exp(-(double)(ts - last_pre[i]) * P.dt_us / tau_p) : 0.0;
+                x_pre[i] = x + 1.0;
+                last_pre[i] = ts;
+            }
+        }
+        for (size_t a = 0; a < spk.size(); ++a) {
+            const uint32_t src = spk[a];
+            const bool src_plastic = plastic && net.kind[src] == 0;
+            for (uint64_t j = net.row_ptr[src]; j < net.row_ptr[src + 1]; ++j) {
+                const uint32_t tg = net.tgt[j];
+                double wv = w[j];
+                if (src_plastic && net.kind[tg] == 0) {
+                    if (pre_last[a] >= 0) {
+                        const int32_t* hh = &hist[(size_t)tg * P.stdp_history];
+                        uint32_t c = 0;
+                        while (c < P.stdp_history && hh[c] > pre_last[a]) ++c;
+                        for (int q = (int)c - 1; q >= 0; --q) {
+                            const double xx = pre_x[a] * std::exp(-(double)(hh[q] - pre_last[a]) * P.dt_us / tau_p);
+                            wv = std::min(wv + ap * xx, wmax);
+                        }
+                    }
+                    if (last_post[tg] >= 0) {
+                        const double y = y_post[tg] * std::exp(-(double)((int32_t)t - last_post[tg]) * P.dt_us / tau_m);
+                        wv = std::max(wv - am * y, 0.0);
+                    }
+                    w[j] = wv;
+                }
+                const double dv = src_plastic ? wv : wv * (double)mult[a];
+                uint32_t sl = slot + net.dly[j];
+                if (sl >= D) sl -= D;
+                ring[(size_t)sl * n + tg] += dv;
+            }
+        }
+        for (uint32_t i : spk) fired[i] = 0;
+    }
+    if (v_out) std::copy(v.begin(), v.end(), v_out);
+    if (w_out) std::copy(w.begin(), w.end(), w_out);
+    if (mismatch) *mismatch = mis;
+    return 0;
+}
+
 }  // extern "C"

@@ -80,6 +80,8 @@ def load() -> C.CDLL:
             "oracle_net_copy_ring": (None, [_vp, _vp]),
             "oracle_net_copy_weights": (None, [_vp, _vp]),
             "oracle_max_threads": (C.c_int, []),
+            "oracle_reintegrate_fp64": (C.c_int, [_vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp, _vp,
+                                                  C.POINTER(C.c_uint64)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -191,6 +193,20 @@ class OracleNet:
         w = np.empty(self.S, dtype=np.float32)
         self._lib.oracle_net_copy_weights(self._h, _ptr(w))
         return w
+
+    def reintegrate_fp64(self, steps: np.ndarray, ids: np.ndarray, nsteps: int):
+        """FP64 re-integration from the initial state (use a network that has
+        not been run) with the spike times of a raster (steps, ids), raster
+        ordered by step.  Returns (V float64 per address, weights float64 in
+        address-order CSR, threshold mismatches)."""
+        st = np.ascontiguousarray(steps, dtype=np.uint32)
+        ii = np.ascontiguousarray(ids, dtype=np.uint32)
+        v = np.empty(self.n, dtype=np.float64)
+        w = np.empty(self.S, dtype=np.float64)
+        mis = C.c_uint64()
+        self._lib.oracle_reintegrate_fp64(self._h, int(nsteps), _ptr(st), _ptr(ii), len(st), _ptr(v), _ptr(w),
+                                          C.byref(mis))
+        return v, w, mis.value
 
 
 def max_threads() -> int:

@@ -239,3 +239,45 @@ def test_atomic_persistent_path_exact_with_integer_weights(O):
         o.run(1000)
         n = assert_same_run(net, o)
         assert n > 2000
+
+
+# Membrane potentials and STDP weights of the CUDA runs against an FP64
+# re-integration (the oracle, double arithmetic, exact exp) driven by the
+# run's own raster: |x32 - x64| <= 1e-5 * max(|x64|, floor), floor 1 mV for
+# V and 1e-3 * w_max for weights.
+FP64_RTOL = 1e-5
+
+
+def assert_fp64(x32, x64, floor):
+    x64 = np.asarray(x64, dtype=np.float64)
+    err = np.abs(np.asarray(x32, dtype=np.float64) - x64) / np.maximum(np.abs(x64), floor)
+    assert err.max() <= FP64_RTOL, err.max()
+
+
+@pytest.mark.parametrize("deterministic", [True, False])
+def test_fp64_reintegration_membrane_and_weights(O, deterministic):
+    s = S.plastic_indegree(n=2000, k=200, drive_weight=21.0).with_(deterministic=deterministic)
+    steps = 1500
+    with S.build(s) as net:
+        net.run(steps)
+        net.finish()
+        st, ids = net.read_spikes()
+        v, _ = net.read_state()
+        _, _, w, _ = net.read_csr()
+    assert len(ids) > 1000
+    v64, w64, _ = O.OracleNet(s).reintegrate_fp64(st, ids, steps)
+    assert_fp64(v, v64, 1.0)
+    assert_fp64(w, w64, 1e-3 * s.w_max)
+
+
+def test_fp64_reintegration_atomic_brunel(O):
+    """Atomic aggregation (unordered fp32 sums), 2 s of the driven workload."""
+    s = S.brunel_small(poisson_weight=1.0)
+    steps = 20000
+    with S.build(s) as net:
+        net.run(steps)
+        net.finish()
+        st, ids = net.read_spikes()
+        v, _ = net.read_state()
+    v64, _, _ = O.OracleNet(s).reintegrate_fp64(st, ids, steps)
+    assert_fp64(v, v64, 1.0)

@@ -224,3 +224,31 @@ def test_golden_oracle_fixture(oracle_mod):
     st, ids = o.spikes()
     assert np.array_equal(st, g["spike_steps"]) and np.array_equal(ids, g["spike_ids"])
     assert np.array_equal(o.state()[0], g["v"])
+
+
+# FP64 re-integration: the fp32 trajectory against double arithmetic with the
+# same spike times.  Tolerance: |x32 - x64| <= 1e-5 * max(|x64|, floor), the
+# floor being 1 mV for membrane potentials and 1e-3 * w_max for weights.
+FP64_RTOL = 1e-5
+
+
+def within_fp64(x32, x64, floor):
+    x64 = np.asarray(x64, dtype=np.float64)
+    return np.abs(np.asarray(x32, dtype=np.float64) - x64) <= FP64_RTOL * np.maximum(np.abs(x64), floor)
+
+
+@pytest.mark.parametrize("make,steps", [(lambda: S.brunel_small(poisson_weight=1.0), 2000),
+                                        (lambda: S.plastic_indegree(n=2000, k=200, drive_weight=21.0), 1000)])
+def test_oracle_fp32_within_fp64_reintegration(oracle_mod, make, steps):
+    O = oracle_mod
+    s = make()
+    o = O.OracleNet(s, deterministic=True)
+    o.run(steps)
+    st, ids = o.spikes()
+    v, _ = o.state()
+    w = o.weights()
+    v64, w64, mismatch = O.OracleNet(s).reintegrate_fp64(st, ids, steps)
+    assert len(ids) > 1000
+    assert within_fp64(v, v64, 1.0).all()
+    assert within_fp64(w, w64, 1e-3 * s.w_max).all()
+    assert mismatch == 0
