@@ -856,7 +856,13 @@ void Engine::resolve_timers() {
 }
 
 void Engine::launch_drive(uint64_t s_first, uint32_t nsteps) {
-    const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 16));
+    if (drive_grid_ == 0) {
+        int occ = 0;
+        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_drive, kLifThreads, 0));
+        drive_grid_ = (uint32_t)std::max(1, occ) * (uint32_t)sm_count_;
+    }
+    // resident blocks only, each with an equal share of (chunk, step) items
+    const uint32_t grid = std::max<uint32_t>(1, std::min<uint64_t>(drive_grid_, (uint64_t)eng_.n_chunks * nsteps));
     const bool from_ctl = s_first == kStepFromCtl;
     if (profiling_ && !from_ctl) NAER_CK(cudaEventRecord(timer_event(), stream_));
     k_drive<<<grid, kLifThreads, 0, stream_>>>(eng_, (unsigned long long)s_first, nsteps);

@@ -184,6 +184,7 @@ private:
     uint32_t queue_cap_ = 0;
     uint32_t aggregation_ = NAER_AGG_ATOMIC;
     uint32_t lif_grid_ = 0, scatter_grid_ = 0;
+    uint32_t drive_grid_ = 0;  // resident blocks of k_drive
     uint64_t host_step_ = 0;
     uint64_t launches_ = 0;
     Tuning tuning_{};

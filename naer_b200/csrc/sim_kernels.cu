@@ -82,38 +82,52 @@ static __device__ __noinline__ uint32_t poisson_exact_call(double rate, uint32_t
 __global__ void __launch_bounds__(kLifThreads, NAER_DRIVE_MIN_BLOCKS)
     k_drive(EngineDev eng, unsigned long long s_first, uint32_t nsteps) {
     if (s_first == kStepFromCtl) s_first = eng.ctl->step;
-    for (uint32_t c = blockIdx.x; c < eng.n_chunks; c += gridDim.x) {
-        const ChunkDev ch = eng.chunks[c];
-        const PopDev p = eng.pops[ch.pop];
-        if (!(p.rate_hz > 0.0)) continue;
-        const NetDev* np = eng.nets + ch.net;
-        const unsigned long long start = np->start_step;
-        const unsigned long long stop = np->end_step;
-        if (!np->active) continue;
-        const uint32_t i0 = ch.first + threadIdx.x * kLifPerThread;
-        if (i0 >= ch.end) continue;
-        const uint32_t dt_us = np->dt_us;
-        const uint32_t Ns = np->n_storage;
-        uint8_t* drive = np->drive;
-        const uint32_t idx0 = (p.type == kPOISSON ? p.rng_idx_base : 0u) + (i0 - p.storage_base);
-        // steps are independent draws: the loop carries no dependence
-        for (uint32_t k = 0; k < nsteps; ++k) {
-            const unsigned long long s = s_first + k;
-            if (s < start || s >= stop) continue;
-            const uint32_t tl = (uint32_t)(s - start);
-            const uint32_t t0 = tl * dt_us, t1 = t0 + dt_us;
-            uint32_t z[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) z[j] = poisson_z0(p, idx0 + j, t0);
-            uint32_t cnt[4] = {0, 0, 0, 0};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (!poisson_quiet(p, z[j], t0) && i0 + j < ch.end)
-                    cnt[j] = poisson_exact_call(p.rate_hz, p.rng_seed, p.rng_n, idx0 + j, z[j], t0, t1);
-            }
-            __stcg(reinterpret_cast<unsigned int*>(drive + (size_t)(s % kDriveSlots) * Ns + i0),
-                   cnt[0] | (cnt[1] << 8) | (cnt[2] << 16) | (cnt[3] << 24));
+    // (chunk, step) items in chunk-major order, an equal contiguous share per
+    // block (the grid is the number of resident blocks): no partial last
+    // wave, and a block reloads descriptors only when its chunk changes
+    const uint64_t total = (uint64_t)eng.n_chunks * nsteps;
+    const uint64_t per = (total + gridDim.x - 1) / gridDim.x;
+    const uint64_t it_end = min(total, (uint64_t)(blockIdx.x + 1) * per);
+    uint32_t cur = 0xFFFFFFFFu;
+    PopDev p{};
+    bool live = false;
+    uint32_t i0 = 0, cend = 0, dt_us = 0, Ns = 0, idx0 = 0;
+    unsigned long long start = 0, stop = 0;
+    uint8_t* drive = nullptr;
+    for (uint64_t it = (uint64_t)blockIdx.x * per; it < it_end; ++it) {
+        const uint32_t c = (uint32_t)(it / nsteps);
+        const uint32_t k = (uint32_t)(it - (uint64_t)c * nsteps);
+        if (c != cur) {
+            cur = c;
+            const ChunkDev ch = eng.chunks[c];
+            p = eng.pops[ch.pop];
+            const NetDev* np = eng.nets + ch.net;
+            start = np->start_step;
+            stop = np->end_step;
+            i0 = ch.first + threadIdx.x * kLifPerThread;
+            cend = ch.end;
+            live = p.rate_hz > 0.0 && np->active && i0 < cend;
+            dt_us = np->dt_us;
+            Ns = np->n_storage;
+            drive = np->drive;
+            idx0 = (p.type == kPOISSON ? p.rng_idx_base : 0u) + (i0 - p.storage_base);
         }
+        if (!live) continue;
+        const unsigned long long s = s_first + k;
+        if (s < start || s >= stop) continue;
+        const uint32_t tl = (uint32_t)(s - start);
+        const uint32_t t0 = tl * dt_us, t1 = t0 + dt_us;
+        uint32_t z[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) z[j] = poisson_z0(p, idx0 + j, t0);
+        uint32_t cnt[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!poisson_quiet(p, z[j], t0) && i0 + j < cend)
+                cnt[j] = poisson_exact_call(p.rate_hz, p.rng_seed, p.rng_n, idx0 + j, z[j], t0, t1);
+        }
+        __stcg(reinterpret_cast<unsigned int*>(drive + (size_t)(s % kDriveSlots) * Ns + i0),
+               cnt[0] | (cnt[1] << 8) | (cnt[2] << 16) | (cnt[3] << 24));
     }
 }
 
