@@ -475,20 +475,18 @@ struct ChunkCache {
 // SMs' reductions wrote it) and the Poisson counts.  Every access names the
 // global space explicitly; the ring slot is cleared by lif_clear after the
 // whole batch of loads has been issued, so no load waits behind a store.
-__device__ __forceinline__ void lif_prefetch(const ChunkCache& cc, unsigned long long s, float4& I, uchar4& D) {
-    I = make_float4(0.f, 0.f, 0.f, 0.f);
-    D = make_uchar4(0, 0, 0, 0);
-    if (!cc.active || s < cc.start || s >= cc.stop) return;
+__device__ __forceinline__ void lif_prefetch(const ChunkCache& cc, unsigned long long s, float4& I, uint32_t& Dw) {
+    // predicated loads, no use of their values here: a chunk's loads never
+    // wait for an earlier chunk's data
     const uint32_t i0 = cc.first + threadIdx.x * kLifPerThread;
-    if (i0 >= cc.end) return;
+    const bool live = cc.active && s >= cc.start && s < cc.stop && i0 < cc.end;
     const uint32_t tl = (uint32_t)(s - cc.start);
-    if (cc.p.rate_hz > 0.0) {
-        const unsigned int w = __ldcg(reinterpret_cast<const unsigned int*>(
-            cc.drive + (size_t)(s % kDriveSlots) * cc.Ns + i0));
-        D = make_uchar4(w & 0xFFu, (w >> 8) & 0xFFu, (w >> 16) & 0xFFu, w >> 24);
-    }
-    if (cc.p.type != kPOISSON)
-        I = __ldcg(reinterpret_cast<const float4*>(cc.ring + (size_t)(tl % cc.slots) * cc.Ns) + (i0 >> 2));
+    const bool want_d = live && cc.p.rate_hz > 0.0;
+    const bool want_i = live && cc.p.type != kPOISSON;
+    Dw = want_d ? __ldcg(reinterpret_cast<const unsigned int*>(cc.drive + (size_t)(s % kDriveSlots) * cc.Ns + i0))
+                : 0u;
+    I = want_i ? __ldcg(reinterpret_cast<const float4*>(cc.ring + (size_t)(tl % cc.slots) * cc.Ns) + (i0 >> 2))
+               : make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 __device__ __forceinline__ void lif_clear(const ChunkCache& cc, unsigned long long s) {
@@ -502,9 +500,10 @@ __device__ __forceinline__ void lif_clear(const ChunkCache& cc, unsigned long lo
 
 __device__ __forceinline__ void lif_chunk_smem(const EngineDev& eng, const ChunkCache& cc, uint32_t j,
                                                unsigned long long s, float4* sV, uchar4* sR, const float4 I,
-                                               const uchar4 D4, SpikeRec* __restrict__ queue,
+                                               const uint32_t Dw, SpikeRec* __restrict__ queue,
                                                uint32_t* __restrict__ qid, uint32_t* s_count) {
     if (!cc.active || s < cc.start || s >= cc.stop) return;  // uniform over the block
+    const uchar4 D4 = make_uchar4(Dw & 0xFFu, (Dw >> 8) & 0xFFu, (Dw >> 16) & 0xFFu, Dw >> 24);
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t tl = (uint32_t)(s - cc.start);
@@ -689,7 +688,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         if (kSmem) {
             for (uint32_t j0 = 0; j0 < own; j0 += kLifBatch) {
                 float4 I[kLifBatch];
-                uchar4 D[kLifBatch];
+                uint32_t D[kLifBatch];
 #pragma unroll
                 for (uint32_t b = 0; b < kLifBatch; ++b)
                     if (j0 + b < own) lif_prefetch(s_cc[j0 + b], s, I[b], D[b]);
