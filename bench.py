@@ -368,7 +368,7 @@ def run_ours(args):
 
     # roofline: CUDA events around every launch on the engine stream; the
     # dominant kernel is the persistent step kernel k_run (LIF + scatter of
-    # 16 grid steps per launch), timed against 9 B per delivered event
+    # up to 64 grid steps per launch), timed against 9 B per delivered event
     net.set_profiling(True)
     p0 = net.stats()["events"]
     net.run(args.profile_steps)

@@ -263,7 +263,7 @@ typedef struct naer_batch naer_batch;
 /* Launch geometry of the step loop (results do not depend on it). */
 typedef struct naer_tuning {
     uint32_t blocks_per_sm;   /* resident step-kernel blocks per SM, 0 = most that fit */
-    uint32_t launch_steps;    /* grid steps per persistent launch, 1..16 */
+    uint32_t launch_steps;    /* grid steps per persistent launch, 1..64 */
     uint32_t scatter_split;   /* warps per spike, 0 = enough to cover the longest row */
     uint32_t graph_launches;  /* persistent launches per CUDA-graph replay, 0 = no graph */
     double best_us_per_step;  /* autotune: time of the chosen geometry */
@@ -298,6 +298,13 @@ NAER_API int naer_batch_clear_spikes(naer_batch* batch);
 NAER_API int naer_batch_get_stats(naer_batch* batch, naer_stats* st);
 NAER_API int naer_batch_read_state(naer_batch* batch, uint32_t member, float* v, uint32_t* refractory);
 NAER_API int naer_batch_stream(naer_batch* batch, void** stream);
+
+/* The same launch-geometry tuning for one network (no counterpart in the
+ * reference): autotune times the candidates on the network itself, each
+ * for trial_steps grid steps, which advance its simulation. */
+NAER_API int naer_net_autotune(naer_net* net, uint32_t trial_steps, naer_tuning* out);
+NAER_API int naer_net_set_tuning(naer_net* net, const naer_tuning* tuning);
+NAER_API int naer_net_get_tuning(naer_net* net, naer_tuning* tuning);
 
 /* ---- served form -------------------------------------------------------
  * No counterpart in the reference.  A request loop on its own host thread:

@@ -190,6 +190,9 @@ PROTOTYPES = {
     "naer_net_get_profile": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
     "naer_net_get_phases": [_vp, _vp],
     "naer_net_get_launch_times": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
+    "naer_net_autotune": [_vp, C.c_uint32, _P(Tuning)],
+    "naer_net_set_tuning": [_vp, _P(Tuning)],
+    "naer_net_get_tuning": [_vp, _P(Tuning)],
     "naer_batch_create": [C.c_int, C.c_uint32, C.c_uint64, _P(_vp)],
     "naer_batch_destroy": [_vp],
     "naer_batch_add": [_vp, _vp, _P(C.c_uint32)],

@@ -489,6 +489,39 @@ int naer_batch_autotune(naer_batch* batch, uint32_t trial_steps, naer_tuning* ou
     });
 }
 
+int naer_net_autotune(naer_net* net, uint32_t trial_steps, naer_tuning* out) {
+    return guarded([&] {
+        need_compiled(net);
+        const naer::TuneResult r = net->eng->autotune(trial_steps);
+        if (out) {
+            fill_tuning(out, r.best, 0);
+            out->best_us_per_step = r.best_us_per_step;
+            out->default_us_per_step = r.default_us_per_step;
+            out->trials = r.trials;
+        }
+    });
+}
+
+int naer_net_set_tuning(naer_net* net, const naer_tuning* tuning) {
+    return guarded([&] {
+        need_compiled(net);
+        need(tuning != nullptr, NAER_E_INVALID, "null argument");
+        naer::Tuning t;
+        t.blocks_per_sm = tuning->blocks_per_sm;
+        t.launch_steps = tuning->launch_steps;
+        t.scatter_split = tuning->scatter_split;
+        net->eng->set_tuning(t);
+    });
+}
+
+int naer_net_get_tuning(naer_net* net, naer_tuning* tuning) {
+    return guarded([&] {
+        need_compiled(net);
+        need(tuning != nullptr, NAER_E_INVALID, "null argument");
+        fill_tuning(tuning, net->eng->tuning(), 0);
+    });
+}
+
 int naer_batch_set_tuning(naer_batch* batch, const naer_tuning* tuning) {
     return guarded([&] {
         need(batch && tuning, NAER_E_INVALID, "null argument");

@@ -743,10 +743,64 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
 void Engine::set_tuning(const Tuning& t) {
     Tuning v = t;
     if (v.launch_steps == 0 || v.launch_steps > kDriveSlots)
-        throw Error(NAER_E_INVALID, "launch_steps must be in 1..16");
+        throw Error(NAER_E_INVALID, "launch_steps must be in 1.." + std::to_string(kDriveSlots));
     if (v.blocks_per_sm > 4) throw Error(NAER_E_INVALID, "blocks_per_sm must be in 0..4");
     tuning_ = v;
     if (!nets_.empty()) install(std::vector<NetHost*>(nets_), inst_raster_cap_, inst_record_, aggregation_);
+}
+
+TuneResult Engine::autotune(uint32_t trial_steps) {
+    if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
+    TuneResult r;
+    r.best = tuning_;
+    if (aggregation_ == NAER_AGG_DETERMINISTIC || trial_steps == 0) return r;
+    DeviceGuard g(device_);
+    cudaEvent_t e0, e1;
+    NAER_CK(cudaEventCreate(&e0));
+    NAER_CK(cudaEventCreate(&e1));
+    auto trial = [&](const Tuning& t) {
+        set_tuning(t);
+        run(t.launch_steps);  // first launch of the new geometry
+        NAER_CK(cudaEventRecord(e0, stream_));
+        run(trial_steps);
+        NAER_CK(cudaEventRecord(e1, stream_));
+        NAER_CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        NAER_CK(cudaEventElapsedTime(&ms, e0, e1));
+        ++r.trials;
+        return 1e3 * ms / trial_steps;
+    };
+    try {
+        const Tuning def{};
+        r.default_us_per_step = trial(def);
+        r.best = def;
+        r.best_us_per_step = r.default_us_per_step;
+        const uint32_t auto_split = eng_.scatter_split;
+        for (uint32_t bps : {0u, 1u}) {
+            for (uint32_t L : {kDriveSlots, kDriveSlots / 2}) {
+                for (uint32_t sp : {0u, std::max<uint32_t>(1, auto_split / 2), std::min<uint32_t>(64, auto_split * 2)}) {
+                    Tuning t;
+                    t.blocks_per_sm = bps;
+                    t.launch_steps = L;
+                    t.scatter_split = sp;
+                    if (bps == 0 && L == kDriveSlots && sp == 0) continue;  // the default, timed above
+                    const double us = trial(t);
+                    if (us < r.best_us_per_step) {
+                        r.best_us_per_step = us;
+                        r.best = t;
+                    }
+                }
+            }
+        }
+        set_tuning(r.best);
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    NAER_CK(cudaEventDestroy(e0));
+    NAER_CK(cudaEventDestroy(e1));
+    return r;
 }
 
 void Engine::drop_graph() {

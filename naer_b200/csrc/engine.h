@@ -85,6 +85,13 @@ struct Tuning {
     uint32_t scatter_split = 0;            // warps per spike (0 = enough to cover the longest row)
 };
 
+struct TuneResult {
+    Tuning best;
+    double best_us_per_step = 0;
+    double default_us_per_step = 0;
+    uint32_t trials = 0;
+};
+
 class Engine {
 public:
     // priority: CUDA stream priority of the engine's stream (lower = higher)
@@ -109,6 +116,10 @@ public:
     // remainder runs as plain launches).  Returns the steps run by replays.
     uint64_t run_graph(uint64_t nsteps, uint32_t graph_launches);
     void set_tuning(const Tuning& t);
+    // Times candidate launch geometries on the installed networks (each
+    // trial advances the simulation by trial_steps grid steps) and keeps
+    // the fastest.  Deterministic aggregation: nothing to tune.
+    TuneResult autotune(uint32_t trial_steps);
     const Tuning& tuning() const { return tuning_; }
     uint32_t lif_grid() const { return lif_grid_; }
     uint32_t scatter_split() const { return eng_.scatter_split; }

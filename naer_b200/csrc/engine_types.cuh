@@ -27,7 +27,10 @@ constexpr uint32_t kScatterUnroll = 2;  // 128-synapse slices in flight per warp
 constexpr uint32_t kScatterPiece = 128 * kScatterUnroll;  // synapses per warp iteration
 // Steps of Poisson counts drawn ahead (ring of slots); small enough that the
 // counts and the delay ring stay resident in L2 together.
-constexpr uint32_t kDriveSlots = 16;
+#ifndef NAER_DRIVE_SLOTS
+#define NAER_DRIVE_SLOTS 64  // 64 measured fastest at 1M / 1e9 (26.5 vs 28.1 us per step with 16)
+#endif
+constexpr uint32_t kDriveSlots = NAER_DRIVE_SLOTS;  // Poisson-count slots = grid steps per launch, at most
 // STDP post-spike history: at most this many entries per plastic neuron, so
 // a packed post row (2 + history words, rounded up to 4) fits kPostWordsMax.
 constexpr uint32_t kMaxStdpHistory = 16;

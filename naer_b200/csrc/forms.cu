@@ -8,18 +8,6 @@ namespace naer {
 
 namespace {
 
-struct CurrentDevice {
-    int prev = -1;
-    explicit CurrentDevice(int dev) {
-        NAER_CK(cudaGetDevice(&prev));
-        if (prev != dev) NAER_CK(cudaSetDevice(dev));
-    }
-    ~CurrentDevice() {
-        int cur = -1;
-        if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) cudaSetDevice(prev);
-    }
-};
-
 std::unique_ptr<NetHost> clone_description(const NetHost& d) {
     if (d.compiled) throw Error(NAER_E_STATE, "a compiled network cannot be used as a description");
     auto n = std::make_unique<NetHost>();
@@ -78,56 +66,7 @@ void Batch::step(uint64_t nsteps, uint32_t graph_launches) {
 
 TuneResult Batch::autotune(uint32_t trial_steps) {
     if (!compiled_) throw Error(NAER_E_STATE, "batch is not compiled");
-    TuneResult r;
-    r.best = eng_->tuning();
-    if (aggregation_ == NAER_AGG_DETERMINISTIC || trial_steps == 0) return r;
-    CurrentDevice g(eng_->device());
-    cudaEvent_t e0, e1;
-    NAER_CK(cudaEventCreate(&e0));
-    NAER_CK(cudaEventCreate(&e1));
-    auto trial = [&](const Tuning& t) {
-        eng_->set_tuning(t);
-        eng_->run(t.launch_steps);  // first launch of the new geometry
-        NAER_CK(cudaEventRecord(e0, eng_->stream()));
-        eng_->run(trial_steps);
-        NAER_CK(cudaEventRecord(e1, eng_->stream()));
-        NAER_CK(cudaEventSynchronize(e1));
-        float ms = 0;
-        NAER_CK(cudaEventElapsedTime(&ms, e0, e1));
-        ++r.trials;
-        return 1e3 * ms / trial_steps;
-    };
-    try {
-        const Tuning def{};
-        r.default_us_per_step = trial(def);
-        r.best = def;
-        r.best_us_per_step = r.default_us_per_step;
-        const uint32_t auto_split = eng_->scatter_split();
-        for (uint32_t bps : {0u, 1u}) {
-            for (uint32_t L : {16u, 8u}) {
-                for (uint32_t sp : {0u, std::max<uint32_t>(1, auto_split / 2), std::min<uint32_t>(64, auto_split * 2)}) {
-                    Tuning t;
-                    t.blocks_per_sm = bps;
-                    t.launch_steps = L;
-                    t.scatter_split = sp;
-                    if (bps == 0 && L == 16 && sp == 0) continue;  // the default, timed above
-                    const double us = trial(t);
-                    if (us < r.best_us_per_step) {
-                        r.best_us_per_step = us;
-                        r.best = t;
-                    }
-                }
-            }
-        }
-        eng_->set_tuning(r.best);
-    } catch (...) {
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        throw;
-    }
-    NAER_CK(cudaEventDestroy(e0));
-    NAER_CK(cudaEventDestroy(e1));
-    return r;
+    return eng_->autotune(trial_steps);
 }
 
 uint64_t Batch::read_spikes(uint64_t first, uint64_t cap, uint32_t* member, uint32_t* steps, uint32_t* ids) {

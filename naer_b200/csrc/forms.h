@@ -15,13 +15,6 @@
 
 namespace naer {
 
-struct TuneResult {
-    Tuning best;
-    double best_us_per_step = 0;
-    double default_us_per_step = 0;
-    uint32_t trials = 0;
-};
-
 // Batched form: members are added as descriptions, built on one engine and
 // stepped together; all start at engine step 0.
 class Batch {

@@ -94,9 +94,10 @@ __global__ void __launch_bounds__(kLifThreads, NAER_DRIVE_MIN_BLOCKS)
     uint32_t i0 = 0, cend = 0, dt_us = 0, Ns = 0, idx0 = 0;
     unsigned long long start = 0, stop = 0;
     uint8_t* drive = nullptr;
-    for (uint64_t it = (uint64_t)blockIdx.x * per; it < it_end; ++it) {
-        const uint32_t c = (uint32_t)(it / nsteps);
-        const uint32_t k = (uint32_t)(it - (uint64_t)c * nsteps);
+    const uint64_t it0 = (uint64_t)blockIdx.x * per;
+    uint32_t c = (uint32_t)(it0 / nsteps);  // one division; then (c, k) advance incrementally
+    uint32_t k = (uint32_t)(it0 - (uint64_t)c * nsteps);
+    for (uint64_t it = it0; it < it_end; ++it, (++k == nsteps ? (k = 0, ++c) : 0)) {
         if (c != cur) {
             cur = c;
             const ChunkDev ch = eng.chunks[c];

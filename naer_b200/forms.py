@@ -52,6 +52,8 @@ class Batch:
         return self
 
     def run(self, nsteps: int) -> None:
+        if nsteps < 0:
+            raise ValueError("nsteps must be >= 0")
         capi.call("naer_batch_step", self._h, int(nsteps))
 
     def finish(self) -> None:
@@ -67,7 +69,7 @@ class Batch:
         capi.call("naer_batch_get_tuning", self._h, C.byref(t))
         return {k: getattr(t, k) for k, _ in capi.Tuning._fields_ if k != "pad_"}
 
-    def set_tuning(self, blocks_per_sm=0, launch_steps=16, scatter_split=0, graph_launches=16) -> None:
+    def set_tuning(self, blocks_per_sm=0, launch_steps=64, scatter_split=0, graph_launches=16) -> None:
         t = capi.Tuning(blocks_per_sm=blocks_per_sm, launch_steps=launch_steps, scatter_split=scatter_split,
                         graph_launches=graph_launches)
         capi.call("naer_batch_set_tuning", self._h, C.byref(t))

@@ -180,10 +180,23 @@ class Network:
 
     def run(self, nsteps: int) -> None:
         """nsteps grid steps, asynchronously."""
+        if nsteps < 0:
+            raise ValueError("nsteps must be >= 0")
         capi.call("naer_net_step", self._h, int(nsteps))
 
     def finish(self) -> None:
         capi.call("naer_net_finish", self._h)
+
+    def autotune(self, trial_steps: int = 64) -> dict:
+        """Picks the launch geometry by timing candidates on this network
+        (each trial advances the simulation by trial_steps grid steps)."""
+        t = capi.Tuning()
+        capi.call("naer_net_autotune", self._h, int(trial_steps), C.byref(t))
+        return {k: getattr(t, k) for k, _ in capi.Tuning._fields_ if k not in ("pad_", "graph_launches")}
+
+    def set_tuning(self, blocks_per_sm: int = 0, launch_steps: int = 64, scatter_split: int = 0) -> None:
+        t = capi.Tuning(blocks_per_sm=blocks_per_sm, launch_steps=launch_steps, scatter_split=scatter_split)
+        capi.call("naer_net_set_tuning", self._h, C.byref(t))
 
     def getTime(self) -> int:
         t = C.c_uint64()

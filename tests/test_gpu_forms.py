@@ -51,15 +51,16 @@ def test_batch_deterministic_matches_alone(lib):
 
 
 def test_batch_graph_atomic_exact_on_integer_weights(lib):
-    """Atomic mode through the CUDA-graph replay (16 launches x 16 steps per
-    replay) plus plain launches for the remainder."""
+    """Atomic mode through the CUDA-graph replay (16 launches per replay)
+    plus plain launches for the remainder."""
     members = [integer_weight_net(n=n, k=k, seed=sd) for n, k, sd in [(3000, 200, 1), (5000, 300, 2), (1500, 100, 3)]]
-    steps = 2 * 256 + 37
     with Batch(members).compile() as b:
+        L = b.tuning()["launch_steps"]
+        steps = 2 * 16 * L + 37  # two replays and a remainder
         l0 = b.stats()["kernel_launches"]
         b.run(steps)
         b.finish()
-        assert b.stats()["kernel_launches"] - l0 == 2 * ((steps + 15) // 16)
+        assert b.stats()["kernel_launches"] - l0 == 2 * ((steps + L - 1) // L)
         sp = b.read_spikes()
         for i, m in enumerate(members):
             st, ids, v, r = alone(m, steps)
@@ -76,12 +77,12 @@ def test_batch_autotune_keeps_results(lib):
         t = b.autotune(trial_steps=32)
         assert t["trials"] >= 2 and t["best_us_per_step"] > 0
         assert t["best_us_per_step"] <= t["default_us_per_step"]
-        done = b.stats()["step"]
-        b.run(600 - done)
+        total = b.stats()["step"] + 200  # the trials advanced the simulation
+        b.run(200)
         b.finish()
         sp = b.read_spikes()
         for i, m in enumerate(members):
-            st, ids, _, _ = alone(m, 600)
+            st, ids, _, _ = alone(m, total)
             bst, bids = b.member_spikes(i, sp)
             assert np.array_equal(st, bst) and np.array_equal(ids, bids)
 
