@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #ifdef _OPENMP
@@ -157,6 +158,15 @@ struct OrParams {
 
 namespace {
 
+// Event-mode state (oracle_net_run_events).
+struct EvState {
+    std::vector<float> v;
+    std::vector<uint32_t> time;
+    std::vector<std::pair<uint32_t, uint32_t>> next;  // events of the next window
+    std::vector<uint32_t> sp_time, sp_id;             // raster: (µs, address)
+    uint64_t window = 0, delivered = 0;
+};
+
 struct Net {
     OrParams prm{};
     std::vector<OrPop> pops;
@@ -187,6 +197,7 @@ struct Net {
     std::vector<float> partial;
     std::vector<uint8_t> touched_flag;
     std::vector<uint64_t> touched;
+    std::unique_ptr<EvState> ev;  // event-mode state (oracle_net_run_events)
 };
 
 inline uint32_t pick(uint32_t word, uint32_t n) { return (uint32_t)(((uint64_t)word * n) >> 32); }
@@ -821,6 +832,116 @@ int oracle_reintegrate_fp64(void* h, uint64_t nsteps, const uint32_t* sp_step, c
     if (w_out) std::copy(w.begin(), w.end(), w_out);
     if (mismatch) *mismatch = mis;
     return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Reference-compatible event mode (the `.cl` kernels' own time model).
+//
+// Time is continuous in µs and advances in windows of 1500 µs
+// (src/Network.cpp:124-127).  Every spike is an event (arrival time, source):
+// a POISSON source's events are its spike times (input_neuron_group.cl:29-38,
+// generated for the window they fall in), a LIF neuron's spike at input time
+// T arrives at its targets at T + 1500 µs (NAER_AXONAL_DELAY, naer_types.h:4;
+// nop.cl:76), i.e. in the next window.  A window's events are applied in
+// time order (ties: ascending source address — the reference's order comes
+// from its scatter and is not defined), each delivering its row to its
+// LIF targets through neuron_dynamics (lif.cl:15-34): dt = T - time; inputs
+// with dt < 0 (refractory) are dropped; V = fp32(fp64(V) * exp(-dt / tau));
+// V += w; time = T; V > V_th -> spike, time += t_ref, V = V_reset.  The
+// per-population tau_m, t_ref, V_th, V_reset replace lif.cl's constants
+// (20 ms, 2 ms, 20 mV, 0).  Connection delays, LIF drive and plasticity do
+// not exist in this model and are ignored (the reference's STDP kernel is
+// partially undefined: NAER_STDP_WEIGHT is never defined, stdp.cl:100).
+//
+// flags bit 0 reproduces nop.cl:54-55: per (spike, 512-neuron NOP group) only
+// the first 96 synapses (the NOP workgroup size, Network.h:115-119) are
+// delivered; STDP targets loop over all synapses (stdp.cl:88-92).
+// Runs nwin more windows of the event model on a built network.  The event
+// state lives beside the grid state of the same handle; the first call
+// starts it from the initial potentials.
+int oracle_net_run_events(void* h, uint64_t nwin, uint32_t flags) {
+    Net& net = *static_cast<Net*>(h);
+    const OrParams& P = net.prm;
+    if (!net.ev) {
+        net.ev = std::make_unique<EvState>();
+        net.ev->v.assign(net.n, 0.0f);
+        net.ev->time.assign(net.n, 0u);
+        for (size_t p = 0; p < net.pops.size(); ++p)
+            if (net.pops[p].type != 2)
+                for (uint32_t k = 0; k < net.pops[p].size; ++k) net.ev->v[net.base[p] + k] = net.pops[p].v_init;
+    }
+    EvState& E = *net.ev;
+    uint32_t count[3] = {0, 0, 0};
+    for (const auto& p : net.pops) count[p.type] += p.size;
+    const uint32_t nop_base = count[0];
+    const uint32_t W = 1500;
+    std::vector<uint32_t> seg_count;
+    for (uint64_t k = 0; k < nwin; ++k) {
+        const uint32_t t0 = (uint32_t)(E.window * W), t1 = t0 + W;
+        std::vector<std::pair<uint32_t, uint32_t>> ev;
+        ev.swap(E.next);
+        uint32_t times[10];
+        for (size_t p = 0; p < net.pops.size(); ++p) {
+            const OrPop& pop = net.pops[p];
+            if (pop.type != 2 || !(pop.rate_hz > 0.0f)) continue;
+            for (uint32_t i = 0; i < pop.size; ++i) {
+                const uint32_t idx = net.type_addr[p] + i;
+                const uint32_t m = poisson_window(idx, net.n_poisson, P.poisson_seed, (double)pop.rate_hz, t0, t1, times);
+                for (uint32_t q = 0; q < m; ++q) {
+                    ev.emplace_back(times[q], net.base[p] + i);
+                    E.sp_time.push_back(times[q]);
+                    E.sp_id.push_back(net.base[p] + i);
+                }
+            }
+        }
+        std::sort(ev.begin(), ev.end());
+        for (const auto& e : ev) {
+            const uint32_t T = e.first, src = e.second;
+            seg_count.clear();
+            for (uint64_t j = net.row_ptr[src]; j < net.row_ptr[src + 1]; ++j) {
+                const uint32_t tg = net.tgt[j];
+                if (net.kind[tg] == 2) continue;
+                if ((flags & 1u) && net.kind[tg] == 1) {
+                    const uint32_t g = (tg - nop_base) / 512u;
+                    if (g >= seg_count.size()) seg_count.resize(g + 1, 0);
+                    if (seg_count[g]++ >= 96u) continue;
+                }
+                const OrPop& pop = net.pops[net.pop_of[tg]];
+                if (T < E.time[tg]) continue;  // dt < 0: refractory
+                const double dt = (double)T - (double)E.time[tg];
+                float v = (float)((double)E.v[tg] * std::exp(-dt / ((double)pop.tau_m_ms * 1000.0)));
+                v = v + net.w[j];
+                E.time[tg] = T;
+                ++E.delivered;
+                if (v > pop.v_th) {
+                    E.time[tg] = T + (uint32_t)std::llround((double)pop.t_ref_ms * 1000.0);
+                    v = pop.v_reset;
+                    E.sp_time.push_back(T);
+                    E.sp_id.push_back(tg);
+                    E.next.emplace_back(T + W, tg);
+                }
+                E.v[tg] = v;
+            }
+        }
+        ++E.window;
+    }
+    return 0;
+}
+
+uint64_t oracle_net_event_spike_count(void* h) {
+    const Net& net = *static_cast<Net*>(h);
+    return net.ev ? net.ev->sp_id.size() : 0;
+}
+
+void oracle_net_event_copy(void* h, uint32_t* times, uint32_t* ids, float* v, uint32_t* last_time,
+                           uint64_t* delivered) {
+    const Net& net = *static_cast<Net*>(h);
+    if (!net.ev) return;
+    if (times) std::copy(net.ev->sp_time.begin(), net.ev->sp_time.end(), times);
+    if (ids) std::copy(net.ev->sp_id.begin(), net.ev->sp_id.end(), ids);
+    if (v) std::copy(net.ev->v.begin(), net.ev->v.end(), v);
+    if (last_time) std::copy(net.ev->time.begin(), net.ev->time.end(), last_time);
+    if (delivered) *delivered = net.ev->delivered;
 }
 
 }  // extern "C"

@@ -82,6 +82,9 @@ def load() -> C.CDLL:
             "oracle_max_threads": (C.c_int, []),
             "oracle_reintegrate_fp64": (C.c_int, [_vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp, _vp,
                                                   C.POINTER(C.c_uint64)]),
+            "oracle_net_run_events": (C.c_int, [_vp, C.c_uint64, C.c_uint32]),
+            "oracle_net_event_spike_count": (C.c_uint64, [_vp]),
+            "oracle_net_event_copy": (None, [_vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -193,6 +196,27 @@ class OracleNet:
         w = np.empty(self.S, dtype=np.float32)
         self._lib.oracle_net_copy_weights(self._h, _ptr(w))
         return w
+
+    def run_events(self, windows: int, truncate96: bool = False) -> None:
+        """Reference-compatible event mode: `windows` windows of 1500 us
+        (see oracle_net_run_events)."""
+        self._lib.oracle_net_run_events(self._h, int(windows), 1 if truncate96 else 0)
+
+    def event_spikes(self):
+        """(time in us, address) of every spike of the event mode so far."""
+        n = self._lib.oracle_net_event_spike_count(self._h)
+        t = np.empty(n, dtype=np.uint32)
+        i = np.empty(n, dtype=np.uint32)
+        self._lib.oracle_net_event_copy(self._h, _ptr(t), _ptr(i), None, None, None)
+        return t, i
+
+    def event_state(self):
+        """(V, last update or refractory end time in us, synapses delivered)."""
+        v = np.empty(self.n, dtype=np.float32)
+        tl = np.empty(self.n, dtype=np.uint32)
+        d = C.c_uint64()
+        self._lib.oracle_net_event_copy(self._h, None, None, _ptr(v), _ptr(tl), C.byref(d))
+        return v, tl, d.value
 
     def reintegrate_fp64(self, steps: np.ndarray, ids: np.ndarray, nsteps: int):
         """FP64 re-integration from the initial state (use a network that has
