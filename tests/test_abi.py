@@ -93,6 +93,41 @@ def test_cpp_wrapper_compiles(tmp_path):
     subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", str(ROOT / "include"), str(src)], check=True)
 
 
+def test_cpp_forms_compile(tmp_path):
+    """include/naer/Forms.h (batched and served forms for C++) compiles."""
+    src = tmp_path / "forms.cpp"
+    src.write_text(textwrap.dedent("""
+        #include "naer/Forms.h"
+        int main() {
+            auto describe = [](Naer::Network& d) {
+                auto P = d.addPopulation(Naer::NeuronType::POISSON, 100);
+                auto E = d.addPopulation(Naer::NeuronType::NOP, 80);
+                d.addConnection(P, E, 0.001f, 0.1);
+            };
+            auto use = [&]() {
+                Naer::Network d(-1);            // description only
+                describe(d);
+                Naer::Batch b(0, true);
+                b.add(d);
+                b.add(d);
+                b.compile();
+                b.autotune(32);
+                b.step(1000);
+                b.finish();
+                auto sp = b.readSpikes();
+                Naer::Server srv(0);
+                uint64_t job = srv.submit(d, 500);
+                srv.wait(job, 60.0);
+                auto js = srv.spikes(job);
+                return sp.size() + js.size() + (size_t)srv.stats().done;
+            };
+            (void)use;
+            return 0;
+        }
+    """))
+    subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", str(ROOT / "include"), str(src)], check=True)
+
+
 def test_create_without_gpu_fails_cleanly(lib):
     from conftest import HAS_GPU
     if HAS_GPU:
