@@ -237,6 +237,36 @@ def plain_runs(specs_steps, local):
     return run_s, all_s
 
 
+def bench_plastic(args, local, stream_of):
+    """The plastic workload: 100k LIF (80 % STDP-excitatory), fixed
+    in-degree 1,000 (1e8 synapses), delays 1-20 steps, 10 Hz drive, pair STDP
+    on E->E; 1 s simulated after 0.1 s of warm-up, CUDA events."""
+    import torch
+    from naer_b200 import spec as S
+    spec = S.plastic_indegree(n=100_000, k=1000)
+    spec.raster_capacity = 1 << 24
+    net = S.build(spec, device=local)
+    stream = stream_of(net)
+    net.run(1000)
+    net.finish()
+    st0 = net.stats()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    net.run(10_000)
+    e1.record(stream)
+    e1.synchronize()
+    st1 = net.stats()
+    ms = e0.elapsed_time(e1)
+    net.close()
+    ev = st1["events"] - st0["events"]
+    return {"workload": "plastic_indegree: 100000 LIF (80/20), fixed in-degree 1000, delays 1-20, 10 Hz drive, "
+                        "pair STDP on E->E; 1 s simulated",
+            "events_per_s": ev / (ms / 1e3), "ms_per_simulated_s": ms, "synapses": int(st1["synapses"]),
+            "spikes_per_s_sim": (st1["spikes"] - st0["spikes"]) / 1.0 / 100_000,
+            "stdp_history_overflows": int(st1["stdp_hist_overflow"])}
+
+
 def bench_batched(args, local):
     """Batched form: independent networks of uneven sizes (log-uniform 2k-50k
     neurons, in-degree 100-1000, own seeds, Poisson 5-30 Hz, STDP on half)
@@ -430,6 +460,8 @@ def run_ours(args):
 
     forms = {}
     if rank == 0 and world == 1 and not args.no_forms:
+        forms["plastic"] = bench_plastic(
+            args, local, lambda n: torch.cuda.ExternalStream(n.stream(), device=torch.device("cuda", local)))
         forms["batched"] = bench_batched(args, local)
         forms["served"] = bench_served(args, local)
 

@@ -240,11 +240,8 @@ NAER_API int naer_net_set_profiling(naer_net* net, int enable);
 NAER_API int naer_net_get_profile(naer_net* net, double* lif_ms, double* scatter_ms,
                                   uint64_t* launches);
 /* Finer split of the same device time (ms): [0] LIF, [1] wait for all LIF
- * blocks, [2] scatter (in the split pipeline, a compile-time option: of the
- * delay-1 synapses and whole rows of STDP sources), [3] split pipeline
- * only: scatter of the remaining synapses of the previous step, overlapping
- * the next LIF, [4] wait for all scatter blocks.  Measured by the first
- * block of the step kernel. */
+ * blocks, [2] scatter, [3] reserved (0), [4] wait for all scatter blocks.
+ * Measured by the first block of the step kernel. */
 NAER_API int naer_net_get_phases(naer_net* net, double* phase_ms5);
 /* CUDA-event durations (ms) of the launches issued while profiling: the
  * Poisson-draw kernels and the persistent step kernels (and their count). */
@@ -269,7 +266,7 @@ typedef struct naer_tuning {
     double best_us_per_step;  /* autotune: time of the chosen geometry */
     double default_us_per_step; /* autotune: time of the default geometry */
     uint32_t trials;          /* autotune: geometries timed */
-    uint32_t pad_;
+    uint32_t scatter_piece;   /* synapses per warp iteration: 128, 256, 0 = 128 for plastic networks else 256 */
 } naer_tuning;
 
 NAER_API int naer_batch_create(int device, uint32_t aggregation, uint64_t raster_capacity,

@@ -109,7 +109,7 @@ class Tuning(C.Structure):
         ("best_us_per_step", C.c_double),
         ("default_us_per_step", C.c_double),
         ("trials", C.c_uint32),
-        ("pad_", C.c_uint32),
+        ("scatter_piece", C.c_uint32),
     ]
 
 

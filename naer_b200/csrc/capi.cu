@@ -473,6 +473,7 @@ static void fill_tuning(naer_tuning* out, const naer::Tuning& t, uint32_t graph_
     out->blocks_per_sm = t.blocks_per_sm;
     out->launch_steps = t.launch_steps;
     out->scatter_split = t.scatter_split;
+    out->scatter_piece = t.scatter_piece;
     out->graph_launches = graph_launches;
 }
 
@@ -510,6 +511,7 @@ int naer_net_set_tuning(naer_net* net, const naer_tuning* tuning) {
         t.blocks_per_sm = tuning->blocks_per_sm;
         t.launch_steps = tuning->launch_steps;
         t.scatter_split = tuning->scatter_split;
+        t.scatter_piece = tuning->scatter_piece;
         net->eng->set_tuning(t);
     });
 }
@@ -530,6 +532,7 @@ int naer_batch_set_tuning(naer_batch* batch, const naer_tuning* tuning) {
         t.blocks_per_sm = tuning->blocks_per_sm;
         t.launch_steps = tuning->launch_steps;
         t.scatter_split = tuning->scatter_split;
+        t.scatter_piece = tuning->scatter_piece;
         batch->b->engine().set_tuning(t);
         batch->graph_launches = tuning->graph_launches;
     });

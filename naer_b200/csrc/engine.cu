@@ -731,11 +731,18 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     eng_.lif_grid = lif_grid_;
     eng_.region_cap = region_cap;
     eng_.record = record ? 1u : 0u;
-    // warps per spike: enough pieces to cover the longest row once
+    // pieces of 128 synapses when some net is plastic (a plastic synapse
+    // costs a dependent post-row load, so more warps per row pay off), else
+    // 256; warps per spike: enough pieces to cover the longest row once
+    bool any_stdp = false;
     uint64_t max_row = 0;
-    for (NetHost* n : nets) max_row = std::max<uint64_t>(max_row, n->max_row_padded);
-    eng_.scatter_split =
-        (uint32_t)std::min<uint64_t>(16, std::max<uint64_t>(1, (max_row + kScatterPiece - 1) / kScatterPiece));
+    for (NetHost* n : nets) {
+        max_row = std::max<uint64_t>(max_row, n->max_row_padded);
+        any_stdp = any_stdp || n->dev.stdp_on;
+    }
+    eng_.scatter_piece = tuning_.scatter_piece ? tuning_.scatter_piece : (any_stdp ? 128u : kScatterPiece);
+    const uint32_t psz = eng_.scatter_piece;
+    eng_.scatter_split = (uint32_t)std::min<uint64_t>(any_stdp ? 32 : 16, std::max<uint64_t>(1, (max_row + psz - 1) / psz));
     if (tuning_.scatter_split) eng_.scatter_split = std::min<uint32_t>(tuning_.scatter_split, 64);
     NAER_CK(cudaStreamSynchronize(stream_));  // tables and buffers complete for every stream
 }
@@ -745,6 +752,8 @@ void Engine::set_tuning(const Tuning& t) {
     if (v.launch_steps == 0 || v.launch_steps > kDriveSlots)
         throw Error(NAER_E_INVALID, "launch_steps must be in 1.." + std::to_string(kDriveSlots));
     if (v.blocks_per_sm > 4) throw Error(NAER_E_INVALID, "blocks_per_sm must be in 0..4");
+    if (v.scatter_piece != 0 && v.scatter_piece != 128 && v.scatter_piece != kScatterPiece)
+        throw Error(NAER_E_INVALID, "scatter_piece must be 0, 128 or 256");
     tuning_ = v;
     if (!nets_.empty()) install(std::vector<NetHost*>(nets_), inst_raster_cap_, inst_record_, aggregation_);
 }
@@ -776,6 +785,7 @@ TuneResult Engine::autotune(uint32_t trial_steps) {
         r.best = def;
         r.best_us_per_step = r.default_us_per_step;
         const uint32_t auto_split = eng_.scatter_split;
+        const uint32_t eng_piece_default = eng_.scatter_piece;
         for (uint32_t bps : {0u, 1u}) {
             for (uint32_t L : {kDriveSlots, kDriveSlots / 2}) {
                 for (uint32_t sp : {0u, std::max<uint32_t>(1, auto_split / 2), std::min<uint32_t>(64, auto_split * 2)}) {
@@ -783,7 +793,11 @@ TuneResult Engine::autotune(uint32_t trial_steps) {
                     t.blocks_per_sm = bps;
                     t.launch_steps = L;
                     t.scatter_split = sp;
-                    if (bps == 0 && L == kDriveSlots && sp == 0) continue;  // the default, timed above
+                    // the other piece width with its own automatic split
+                    t.scatter_piece = 0;
+                    if (bps == 0 && L == kDriveSlots && sp == 0) {
+                        t.scatter_piece = eng_piece_default == 128 ? kScatterPiece : 128u;
+                    }
                     const double us = trial(t);
                     if (us < r.best_us_per_step) {
                         r.best_us_per_step = us;

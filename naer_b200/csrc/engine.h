@@ -83,6 +83,7 @@ struct Tuning {
     uint32_t blocks_per_sm = 0;            // resident step-kernel blocks per SM (0 = most that fit)
     uint32_t launch_steps = kDriveSlots;   // grid steps per persistent launch (1..kDriveSlots)
     uint32_t scatter_split = 0;            // warps per spike (0 = enough to cover the longest row)
+    uint32_t scatter_piece = 0;            // synapses per warp iteration: 128, 256, 0 = 128 with STDP else 256
 };
 
 struct TuneResult {

@@ -164,7 +164,8 @@ struct EngineDev {
     uint32_t lif_grid;
     uint32_t region_cap;
     uint32_t record;                // append spikes to the raster
-    uint32_t scatter_split;         // warps per spike (row pieces of kScatterPiece)
+    uint32_t scatter_split;         // warps per spike (row pieces of scatter_piece)
+    uint32_t scatter_piece;         // synapses per warp iteration: 128 or kScatterPiece
 };
 
 }  // namespace naer

@@ -319,14 +319,6 @@ __device__ __forceinline__ uint32_t block_prefix_counts(const uint32_t* __restri
 // stdp.cl:66-133) and its histogram/scatter/offset passes
 // (spike_aggregation.cl).  The first warp of each spike appends it to the
 // raster at rbase + its queue rank.
-// Which part of each row a scatter pass delivers.
-enum ScatterPart : int {
-    kPartAll = 0,    // the whole row
-    kPartEarly = 1,  // delay-1 part (whole row for STDP sources): needed by the next step
-    kPartLate = 2,   // delay > 1 part of non-STDP sources: may drain while the next step runs
-};
-
-template <int kPart>
 __device__ __forceinline__ void scatter_step(const EngineDev& eng, unsigned long long s, const uint32_t* prefix,
                                              uint32_t Q, unsigned long long rbase, unsigned long long& ev,
                                              uint32_t& ovf, const NetDev* net0) {
@@ -337,6 +329,7 @@ __device__ __forceinline__ void scatter_step(const EngineDev& eng, unsigned long
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t split = eng.scatter_split;
+    const uint32_t psz = eng.scatter_piece;  // 128 or 256 synapses per warp iteration
     const uint32_t items = Q * split;
     const uint32_t G = eng.lif_grid;
 
@@ -352,7 +345,7 @@ __device__ __forceinline__ void scatter_step(const EngineDev& eng, unsigned long
         r.src = (uint32_t)rv.y;
         r.aux0 = rv.z;
         r.aux1 = __int_as_float(rv.w);
-        if (kPart != kPartLate && piece == 0 && lane == 0 && eng.record && rbase + e < eng.raster_cap)
+        if (piece == 0 && lane == 0 && eng.record && rbase + e < eng.raster_cap)
             __stcg(eng.raster + rbase + e, make_uint2((uint32_t)s, __ldcg(qid + qpos)));
         const NetDev* np = (r.net == 0 && net0) ? net0 : eng.nets + r.net;
         const uint32_t tl = (uint32_t)(s - np->start_step);
@@ -364,28 +357,22 @@ __device__ __forceinline__ void scatter_step(const EngineDev& eng, unsigned long
         float* __restrict__ w_a = np->w;
         const uint8_t* __restrict__ d_a = np->dly;
         const ulonglong2 rb = row_bounds(np->row_ptr, r.src);
-        uint64_t beg = rb.x;
-        uint64_t end = rb.y;
+        const uint64_t beg = rb.x;
+        const uint64_t end = rb.y;
         const uint32_t n_plastic = np->n_plastic;
         const bool plastic_src = np->stdp_on && r.src < n_plastic;
-        if (kPart == kPartEarly && !plastic_src) end = beg + __ldg(np->row_mid + r.src);
-        if (kPart == kPartLate) {
-            if (plastic_src) continue;
-            beg += __ldg(np->row_mid + r.src);
-        }
         StdpView sv;
         if (plastic_src) sv = stdp_view(*np);
         const float mult = (!plastic_src && r.aux0 > 1) ? (float)r.aux0 : 1.0f;
 
-        for (uint64_t base = beg + (uint64_t)piece * kScatterPiece; base < end;
-             base += (uint64_t)split * kScatterPiece) {
+        for (uint64_t base = beg + (uint64_t)piece * psz; base < end; base += (uint64_t)split * psz) {
             uint4 tg[kScatterUnroll];
             float4 ww[kScatterUnroll];
             uint32_t dd[kScatterUnroll];
 #pragma unroll
             for (int u = 0; u < (int)kScatterUnroll; ++u) {
                 const uint64_t off = base + (uint64_t)(u * 32 + lane) * 4ull;
-                if (off < end) {
+                if (off < end && (uint32_t)u * 128u < psz) {
                     tg[u] = ld_stream_u4(tgt_a + off);
                     ww[u] = __ldcg(reinterpret_cast<const float4*>(w_a + off));  // STDP may rewrite
                     dd[u] = ld_stream_u32(d_a + off);
@@ -591,12 +578,6 @@ __device__ __forceinline__ void lif_chunk_smem(const EngineDev& eng, const Chunk
 // counters in shared memory for the whole launch (loaded at entry, written
 // back at exit); otherwise they stay in global memory.  Block 0 times the
 // phases with %globaltimer.
-// NAER_SPLIT_DELAY1 selects the split pipeline: only the delay-1 part of
-// each row (whole rows of STDP sources) is scattered before the next LIF,
-// the rest while the next LIF runs.  Measured on B200 at 1M neurons / 1e9
-// synapses it is slower than the single scatter pass (29.4 vs 33.7 us per
-// step), because each spike then pays two dependent-load chains; the
-// default is the single pass.
 #ifndef NAER_RUN_MIN_BLOCKS
 #define NAER_RUN_MIN_BLOCKS 2  // resident blocks per SM the register budget must allow
 #endif
@@ -670,18 +651,10 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         }
     }
     uint32_t k = 0;
-    uint32_t Q_prev = 0;
-    unsigned long long rbase_prev = rbase;
     for (; k < nsteps; ++k) {
         const unsigned long long s = s0 + k;
         const uint32_t qb = (uint32_t)(s & 1ull);
         const unsigned long long ta = timer ? globaltimer_ns() : 0ull;
-        // late part of the previous step first: its reductions (slots >= s + 1)
-        // drain in L2 while this block runs the LIF of step s (slot s)
-#ifdef NAER_SPLIT_DELAY1
-        if (k > 0) scatter_step<kPartLate>(eng, s - 1, s_prefix, Q_prev, rbase_prev, ev, ovf, &s_net0);
-#endif
-        const unsigned long long ta1 = timer ? globaltimer_ns() : 0ull;
         if (threadIdx.x == 0) s_count = 0;
         __syncthreads();
         SpikeRec* queue = (qb ? eng.queue[1] : eng.queue[0]) + region;
@@ -712,36 +685,24 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         const unsigned long long tb = timer ? globaltimer_ns() : 0ull;
 
         const uint32_t Q = block_prefix_counts(qb ? eng.counts[1] : eng.counts[0], G, s_prefix);
-#ifdef NAER_SPLIT_DELAY1
-        scatter_step<kPartEarly>(eng, s, s_prefix, Q, rbase, ev, ovf, &s_net0);
-#else
-        scatter_step<kPartAll>(eng, s, s_prefix, Q, rbase, ev, ovf, &s_net0);
-#endif
+        scatter_step(eng, s, s_prefix, Q, rbase, ev, ovf, &s_net0);
         const unsigned long long tb2 = timer ? globaltimer_ns() : 0ull;
         const unsigned long long cap = eng.record ? eng.raster_cap : 0ull;
         const unsigned long long kept = rbase + Q <= cap ? Q : (rbase >= cap ? 0ull : cap - rbase);
         if (eng.record) dropped += Q - kept;
-        rbase_prev = rbase;
-        Q_prev = Q;
         rbase += kept;
         bar_target += G;
         if (!grid_barrier(ctl, bar_target)) break;
         if (timer) {
             const unsigned long long tc = globaltimer_ns();
-            t_lif += tb - ta1;
-            t_sc += (tc - tb) + (ta1 - ta);
-            t_ph[0] += ta2 - ta1;
+            t_lif += tb - ta;
+            t_sc += tc - tb;
+            t_ph[0] += ta2 - ta;
             t_ph[1] += tb - ta2;
             t_ph[2] += tb2 - tb;
-            t_ph[3] += ta1 - ta;
             t_ph[4] += tc - tb2;
         }
     }
-    // late part of the last step (no step follows inside this launch)
-#ifdef NAER_SPLIT_DELAY1
-    if (k == nsteps && nsteps > 0)
-        scatter_step<kPartLate>(eng, s0 + nsteps - 1, s_prefix, Q_prev, rbase_prev, ev, ovf, &s_net0);
-#endif
     if (kSmem) {
         __syncthreads();
         for (uint32_t j = 0; j < own; ++j) {

@@ -194,8 +194,10 @@ class Network:
         capi.call("naer_net_autotune", self._h, int(trial_steps), C.byref(t))
         return {k: getattr(t, k) for k, _ in capi.Tuning._fields_ if k not in ("pad_", "graph_launches")}
 
-    def set_tuning(self, blocks_per_sm: int = 0, launch_steps: int = 64, scatter_split: int = 0) -> None:
-        t = capi.Tuning(blocks_per_sm=blocks_per_sm, launch_steps=launch_steps, scatter_split=scatter_split)
+    def set_tuning(self, blocks_per_sm: int = 0, launch_steps: int = 64, scatter_split: int = 0,
+                   scatter_piece: int = 0) -> None:
+        t = capi.Tuning(blocks_per_sm=blocks_per_sm, launch_steps=launch_steps, scatter_split=scatter_split,
+                        scatter_piece=scatter_piece)
         capi.call("naer_net_set_tuning", self._h, C.byref(t))
 
     def getTime(self) -> int:
@@ -289,7 +291,7 @@ class Network:
         self.scatter_time = sc.value / 1e3
         ph = (C.c_double * 5)()
         capi.call("naer_net_get_phases", self._h, C.cast(ph, C.c_void_p))
-        names = ["lif", "lif_wait", "scatter_early", "scatter_late", "scatter_wait"]
+        names = ["lif", "lif_wait", "scatter", "reserved", "scatter_wait"]
         dr, rk = C.c_double(), C.c_double()
         nl = C.c_uint64()
         capi.call("naer_net_get_launch_times", self._h, C.byref(dr), C.byref(rk), C.byref(nl))
