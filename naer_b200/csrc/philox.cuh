@@ -14,6 +14,7 @@
 //                                                       word z / 4294967295.0 as double
 //   exprnd        include/naer/kernels/random.cl:26-30  log(1 - x) / (-(rate / 1e6)) microseconds
 #pragma once
+#include <math.h>
 #include <stdint.h>
 
 #if defined(__CUDACC__)
@@ -33,15 +34,13 @@ constexpr uint32_t kPhiloxM1 = 0xCD9E8D57u;
 constexpr uint32_t kPhiloxW0 = 0x9E3779B9u;  // golden ratio
 constexpr uint32_t kPhiloxW1 = 0xBB67AE85u;  // sqrt(3) - 1
 
+// One 32 x 32 -> 64-bit multiply (mul.wide.u32) gives both halves: on the
+// GPU the rounds are bound by the integer-multiply pipe, so hi and lo are
+// not computed by two separate multiplies.
 NAER_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
-#if defined(__CUDA_ARCH__)
-    lo = a * b;
-    hi = __umulhi(a, b);
-#else
-    uint64_t p = (uint64_t)a * (uint64_t)b;
+    const uint64_t p = (uint64_t)a * (uint64_t)b;
     lo = (uint32_t)p;
     hi = (uint32_t)(p >> 32);
-#endif
 }
 
 // Full Philox4x32-10: returns all four output words.
@@ -78,6 +77,46 @@ NAER_HD u32x4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
 // drops the dead words of the last round.
 NAER_HD uint32_t philox_ref_z(uint32_t c0, uint32_t k0, uint32_t k1) {
     return philox4x32_10(c0, 0u, 0u, 0u, k0, k1).v[2];
+}
+
+// philox_ref_z(c0, k0, k1) with the one product that does not depend on
+// the counter supplied by the caller: round 1 leaves key word k0 in counter
+// word 0, so round 2 multiplies M0 by k0.  m_hi:m_lo = M0 * k0 (64-bit).
+// A generator draws for the same neuron (same k0) at every step, so the
+// product is computed once per neuron instead of once per draw.
+NAER_HD uint32_t philox_ref_z_pre(uint32_t c0, uint32_t k0, uint32_t k1, uint32_t m_hi, uint32_t m_lo) {
+    uint32_t h, l;
+    mulhilo32(kPhiloxM0, c0, h, l);  // round 1; counter words 1-3 are zero
+    uint32_t x0 = k0, x1 = 0u, x2 = h ^ k1, x3 = l;
+    k0 += kPhiloxW0;
+    k1 += kPhiloxW1;
+    uint32_t h1, l1;
+    mulhilo32(kPhiloxM1, x2, h1, l1);  // round 2; M0 * x0 is m_hi:m_lo
+    {
+        const uint32_t n0 = h1 ^ x1 ^ k0;
+        const uint32_t n2 = m_hi ^ x3 ^ k1;
+        x0 = n0;
+        x1 = l1;
+        x2 = n2;
+        x3 = m_lo;
+    }
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+    for (int r = 2; r < 10; ++r) {
+        k0 += kPhiloxW0;
+        k1 += kPhiloxW1;
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo32(kPhiloxM0, x0, hi0, lo0);
+        mulhilo32(kPhiloxM1, x2, hi1, lo1);
+        const uint32_t n0 = hi1 ^ x1 ^ k0;
+        const uint32_t n2 = hi0 ^ x3 ^ k1;
+        x0 = n0;
+        x1 = lo1;
+        x2 = n2;
+        x3 = lo0;
+    }
+    return x2;
 }
 
 // Work-item id the reference's kernels see for element `idx` of a type laid

@@ -281,3 +281,47 @@ def test_fp64_reintegration_atomic_brunel(O):
         v, _ = net.read_state()
     v64, _, _ = O.OracleNet(s).reintegrate_fp64(st, ids, steps)
     assert_fp64(v, v64, 1.0)
+
+
+def test_edge_long_rows_long_delays_other_dt(O):
+    """Rows longer than warps-per-spike x piece (the scatter loops over the
+    row), delays up to 254 steps (255 ring slots), a 50 us grid step, a
+    POISSON population of one neuron and populations whose sizes are not
+    multiples of 4."""
+    s = S.NetSpec(dt_us=50, poisson_seed=9)
+    P = s.add_pop(S.POISSON, 1, rate_hz=2000.0)
+    E = s.add_pop(S.NOP, 3001, drive_rate_hz=30.0, drive_weight=21.0, drive_seed=5)
+    I = s.add_pop(S.NOP, 7, drive_rate_hz=30.0, drive_weight=21.0, drive_seed=6)
+    s.connect(P, E, capi.CONN_FIXED_OUTDEGREE, 2.0, degree=6000, dmin=1, dmax=3, seed=21)
+    s.connect(E, E, capi.CONN_FIXED_OUTDEGREE, 1.0, degree=40, dmin=1, dmax=254, seed=22)
+    s.connect(I, E, capi.CONN_FIXED_OUTDEGREE, -2.0, degree=5000, dmin=200, dmax=254, seed=23)
+    s.connect(E, I, capi.CONN_REF_BERNOULLI, 0.5, probability=0.5, dmin=1, dmax=1, seed=24)
+    net, o = run_both(O, s, 1200)
+    with net:
+        assert_same_run(net, o)
+        assert_csr_equal(net, o)
+    # the atomic persistent kernel on the same integer-weight network
+    with S.build(s) as net:
+        net.run(1200)
+        net.finish()
+        o2 = O.OracleNet(s, deterministic=True)
+        o2.run(1200)
+        assert assert_same_run(net, o2) > 100
+
+
+def test_silent_and_empty_networks(O):
+    """No connections; a network whose only population never fires."""
+    s = S.NetSpec()
+    s.add_pop(S.NOP, 5, drive_rate_hz=0.0)
+    net, o = run_both(O, s, 50)
+    with net:
+        assert assert_same_run(net, o) == 0
+        assert net.getSynapses() == 0
+    s2 = S.NetSpec()
+    s2.add_pop(S.POISSON, 3, rate_hz=0.0)
+    s2.add_pop(S.NOP, 9)
+    s2.connect(0, 1, capi.CONN_FIXED_OUTDEGREE, 1.0, degree=2)
+    with S.build(s2) as net:
+        net.run(100)
+        net.finish()
+        assert net.stats()["spikes"] == 0 and net.stats()["events"] == 0

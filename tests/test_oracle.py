@@ -37,6 +37,23 @@ def test_philox_matches_python_restatement(oracle_mod):
         assert list(oracle_mod.philox4x32_10(ctr, key)) == py_philox(ctr, key)
 
 
+# Known-answer vectors published with Random123 for philox4x32-10
+# (counter, key, output), the library behind the reference's philox4x32
+# (include/naer/kernels/random.cl:8-16).
+RANDOM123_KAT = [
+    ([0, 0, 0, 0], [0, 0], [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]),
+    ([M, M, M, M], [M, M], [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]),
+    ([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0],
+     [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]),
+]
+
+
+def test_philox_random123_known_answers(oracle_mod):
+    for ctr, key, out in RANDOM123_KAT:
+        assert list(oracle_mod.philox4x32_10(ctr, key)) == out
+        assert py_philox(ctr, key) == out
+
+
 def test_philox_matches_curand_golden(oracle_mod):
     """cuRAND's Philox4_32_10 outputs (generated on a B200 by
     tests/golden/gen_philox_curand.py) pin the oracle's Philox."""
