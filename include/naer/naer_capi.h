@@ -311,7 +311,13 @@ NAER_API int naer_net_get_tuning(naer_net* net, naer_tuning* tuning);
  * already running (continuous batching: admission and retirement happen
  * every chunk_steps grid steps, state stays on the device).  Each job's
  * raster is collected per chunk and returned when the job ends.  All
- * functions are thread-safe. */
+ * functions are thread-safe.
+ *
+ * Trace: with the environment variable NAER_SERVER_TRACE set to a file
+ * name when the server is created, the stepper writes one CSV row per chunk
+ * (running jobs, device ms, host ms waiting / installing / handing rasters
+ * over, records, queue length, bytes in use) to that file and the builder
+ * one row per build to <name>.build. */
 typedef struct naer_server naer_server;
 
 typedef struct naer_server_params {

@@ -3,6 +3,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
 
 namespace naer {
 
@@ -15,6 +18,16 @@ std::unique_ptr<NetHost> clone_description(const NetHost& d) {
     n->pops = d.pops;
     n->conns = d.conns;
     return n;
+}
+
+// Optional per-chunk and per-build trace of the served form, as CSV: set
+// NAER_SERVER_TRACE to a file name (the builder writes <name>.build).
+FILE* open_trace(const char* suffix, const char* header) {
+    const char* base = std::getenv("NAER_SERVER_TRACE");
+    if (!base || !*base) return nullptr;
+    FILE* f = std::fopen((std::string(base) + suffix).c_str(), "w");
+    if (f) std::fputs(header, f);
+    return f;
 }
 
 // Member of an engine-global raster id (id offsets ascending).
@@ -207,6 +220,7 @@ ServerStats Server::stats() {
 // device build on its own engine and stream, and the frees of retired jobs.
 void Server::build_loop() {
     std::unique_ptr<Engine> eng;
+    FILE* trace = open_trace(".build", "t_s,job,wait_s,build_ms,neurons,synapses,est_bytes,used_bytes,pending\n");
     try {
         NAER_CK(cudaSetDevice(device_));
         int lo = 0, hi = 0;
@@ -277,6 +291,11 @@ void Server::build_loop() {
             }
             std::lock_guard<std::mutex> lk(mu_);
             st_.build_s += now_s() - t;
+            if (trace)
+                std::fprintf(trace, "%.6f,%llu,%.6f,%.3f,%u,%llu,%llu,%llu,%zu\n", t, (unsigned long long)j->id,
+                             t - j->info.submit_s, 1e3 * (now_s() - t), j->net->n_ids,
+                             (unsigned long long)j->net->synapses, (unsigned long long)j->est_bytes,
+                             (unsigned long long)used_, pending_.size());
             st_.peak_bytes = std::max<uint64_t>(st_.peak_bytes, eng->device_bytes());
             ready_.push_back(j);
             cv_work_.notify_all();
@@ -304,6 +323,7 @@ void Server::build_loop() {
         cv_done_.notify_all();
         cv_work_.notify_all();
     }
+    if (trace) std::fclose(trace);
 }
 
 // Stepper: one iteration per chunk of steps.  It takes built jobs in,
@@ -328,6 +348,8 @@ void Server::loop() {
     double ms_per_step = 0.0;
     uint64_t chunk_len = 0;
     cudaEvent_t c0 = nullptr, c1 = nullptr;  // device time of the chunk in flight
+    FILE* trace = open_trace("", "t_s,running,admitted,finished,chunk_steps,chunk_ms,wait_ms,install_ms,drain_ms,"
+                                 "records,pending,used_bytes\n");
     try {
         NAER_CK(cudaSetDevice(device_));
         eng = std::make_unique<Engine>(device_);
@@ -362,9 +384,12 @@ void Server::loop() {
             uint64_t nrec = 0, dropped = 0;
             if (inflight) nrec = eng->harvest_raster(rec, copied, &dropped);
             const double t_step = inflight ? now_s() - t : 0.0;
+            const uint64_t done_len = inflight ? chunk_len : 0;
+            float done_ms = 0.0f;  // device time of the chunk just collected
             if (inflight && chunk_len > 0) {
                 float ms = 0.0f;
                 NAER_CK(cudaEventElapsedTime(&ms, c0, c1));
+                done_ms = ms;
                 const double m = (double)ms / (double)chunk_len;
                 ms_per_step = ms_per_step > 0.0 ? 0.5 * (ms_per_step + m) : m;
             }
@@ -468,6 +493,11 @@ void Server::loop() {
                 st_.drain_s += t_drain;
                 st_.raster_dropped += dropped;
                 st_.running = running.size();
+                if (trace && done_len)
+                    std::fprintf(trace, "%.6f,%zu,%zu,%zu,%llu,%.3f,%.3f,%.3f,%.3f,%llu,%zu,%llu\n", tn2, running.size(),
+                                 admit.size(), finished.size(), (unsigned long long)done_len, done_ms, 1e3 * t_step,
+                                 1e3 * t_install, 1e3 * t_drain, (unsigned long long)nrec, pending_.size(),
+                                 (unsigned long long)used_);
                 if (!finished.empty()) {
                     cv_done_.notify_all();
                     cv_build_.notify_all();
@@ -494,6 +524,7 @@ void Server::loop() {
     if (copied) cudaEventDestroy(copied);
     if (c0) cudaEventDestroy(c0);
     if (c1) cudaEventDestroy(c1);
+    if (trace) std::fclose(trace);
     // running jobs are abandoned: the builder frees them
     std::lock_guard<std::mutex> lk(mu_);
     for (Job* j : running) {
