@@ -328,6 +328,10 @@ typedef struct naer_server_params {
     uint32_t max_jobs;         /* jobs stepped together, at most */
     uint32_t blocks_per_sm;    /* step-kernel blocks per SM (0 = most that fit) */
     double chunk_ms;           /* target device time of a chunk: fewer steps when many jobs run */
+    uint32_t launch_steps;     /* grid steps per persistent step launch, 1..64 (0 = default);
+                                  builds run between launches, so short launches let jobs in sooner
+                                  and long ones pay less launch overhead per step */
+    uint32_t pad_;
 } naer_server_params;
 
 #define NAER_JOB_QUEUED 0u

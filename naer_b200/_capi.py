@@ -122,6 +122,8 @@ class ServerParams(C.Structure):
         ("max_jobs", C.c_uint32),
         ("blocks_per_sm", C.c_uint32),
         ("chunk_ms", C.c_double),
+        ("launch_steps", C.c_uint32),
+        ("pad_", C.c_uint32),
     ]
 
 

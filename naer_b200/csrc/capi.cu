@@ -611,6 +611,7 @@ int naer_server_params_default(naer_server_params* p) {
     p->max_jobs = 1024;
     p->blocks_per_sm = 0;
     p->chunk_ms = 10.0;
+    p->launch_steps = 0;
     return NAER_OK;
 }
 
@@ -628,6 +629,7 @@ int naer_server_create(int device, const naer_server_params* params, naer_server
         sp.max_jobs = p.max_jobs;
         sp.blocks_per_sm = p.blocks_per_sm;
         sp.chunk_ms = p.chunk_ms;
+        if (p.launch_steps) sp.launch_steps = p.launch_steps;
         auto h = std::make_unique<naer_server>();
         h->s = std::make_unique<naer::Server>(device, sp);
         *out = h.release();

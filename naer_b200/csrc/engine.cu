@@ -232,6 +232,44 @@ static void layout(NetHost& n) {
 // arrays (each row padded to 4 entries in each of its two delay classes),
 // row pointers, neuron state, ring, drive slots and plasticity state.  The
 // Bernoulli rule's count is its mean plus six standard deviations.
+uint32_t lif_chunks(const NetHost& description) {
+    uint64_t c = 0;
+    for (const PopSpec& ps : description.pops) c += (ps.size + kLifChunk - 1) / kLifChunk;
+    return (uint32_t)std::min<uint64_t>(c, 0xFFFFFFFFu);
+}
+
+uint32_t Engine::fast_chunk_capacity() {
+    DeviceGuard g(device_);
+    int optin = 0;
+    NAER_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+    cudaFuncAttributes fa{};
+    NAER_CK(cudaFuncGetAttributes(&fa, k_run<true>));
+    optin -= (int)fa.sharedSizeBytes;
+    NAER_CK(cudaFuncSetAttribute(k_run<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    const int bps_hi = tuning_.blocks_per_sm ? (int)std::min<uint32_t>(tuning_.blocks_per_sm, 4) : 4;
+    auto fits = [&](int bps, uint32_t own) {
+        const uint32_t grid = (uint32_t)bps * (uint32_t)sm_count_;
+        const size_t smem = run_smem_bytes(grid, own, true);
+        if (smem > (size_t)optin) return false;
+        int occ = 0;
+        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_run<true>, kLifThreads, smem));
+        return occ >= bps;
+    };
+    for (int bps = bps_hi; bps >= 1; --bps) {
+        if (!fits(bps, 1)) continue;
+        uint32_t lo = 1, hi = 1;  // largest own chunks per block that still fits: doubling, then bisection
+        while (hi < (1u << 16) && fits(bps, hi * 2)) hi *= 2;
+        lo = hi;
+        hi = hi * 2;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (fits(bps, mid)) lo = mid; else hi = mid;
+        }
+        return lo * (uint32_t)bps * (uint32_t)sm_count_;
+    }
+    return 0;
+}
+
 uint64_t estimate_device_bytes(const NetHost& description) {
     NetHost n;
     n.params = description.params;

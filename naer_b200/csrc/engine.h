@@ -77,6 +77,10 @@ struct NetHost {
 // validates the description (the checks compile makes).
 uint64_t estimate_device_bytes(const NetHost& description);
 
+// LIF work items (chunks of up to 1,024 neurons of one population) a
+// network adds to an engine, from its description alone.
+uint32_t lif_chunks(const NetHost& description);
+
 // Launch geometry of the persistent step loop (all choices leave the
 // simulated results unchanged).
 struct Tuning {
@@ -117,6 +121,11 @@ public:
     // remainder runs as plain launches).  Returns the steps run by replays.
     uint64_t run_graph(uint64_t nsteps, uint32_t graph_launches);
     void set_tuning(const Tuning& t);
+    // Most LIF chunks an installation can hold while the step kernel keeps
+    // neuron state in shared memory at the most resident blocks per SM it
+    // can have under the current tuning (its fastest geometry); beyond it
+    // the step runs with fewer blocks or with state in global memory.
+    uint32_t fast_chunk_capacity();
     // Times candidate launch geometries on the installed networks (each
     // trial advances the simulation by trial_steps grid steps) and keeps
     // the fastest.  Deterministic aggregation: nothing to tune.

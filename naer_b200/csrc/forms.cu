@@ -102,6 +102,8 @@ Server::Server(int device, const ServerParams& p) : device_(device), prm_(p), t0
     if (p.chunk_steps == 0) throw Error(NAER_E_INVALID, "chunk_steps must be positive");
     if (p.max_jobs == 0) throw Error(NAER_E_INVALID, "max_jobs must be positive");
     if (p.raster_capacity == 0) throw Error(NAER_E_INVALID, "raster_capacity must be positive");
+    if (p.launch_steps == 0 || p.launch_steps > kDriveSlots)
+        throw Error(NAER_E_INVALID, "launch_steps must be in 1..64");
     int n = 0;
     NAER_CK(cudaGetDeviceCount(&n));
     if (device < 0 || device >= n) throw Error(NAER_E_INVALID, "device index out of range");
@@ -130,6 +132,7 @@ uint64_t Server::submit(const NetHost& description, uint64_t duration_steps) {
     auto j = std::make_unique<Job>();
     j->net = clone_description(description);
     j->est_bytes = estimate_device_bytes(*j->net);
+    j->chunks = lif_chunks(*j->net);
     if (j->est_bytes > prm_.budget_bytes)
         throw Error(NAER_E_OVERFLOW, "job needs about " + std::to_string(j->est_bytes) +
                                          " device bytes, more than the server budget of " +
@@ -349,16 +352,21 @@ void Server::loop() {
     uint64_t chunk_len = 0;
     cudaEvent_t c0 = nullptr, c1 = nullptr;  // device time of the chunk in flight
     FILE* trace = open_trace("", "t_s,running,admitted,finished,chunk_steps,chunk_ms,wait_ms,install_ms,drain_ms,"
-                                 "records,pending,used_bytes\n");
+                                 "records,pending,used_bytes,running_chunks,chunk_cap\n");
     try {
         NAER_CK(cudaSetDevice(device_));
         eng = std::make_unique<Engine>(device_);
         // short persistent launches: the builder's kernels (higher-priority
         // stream) get the device between them instead of after whole chunks
         Tuning tn;
-        tn.launch_steps = 4;
+        tn.launch_steps = prm_.launch_steps;
         tn.blocks_per_sm = prm_.blocks_per_sm;
         eng->set_tuning(tn);
+        // Admission keeps the running set within the step kernel's fastest
+        // geometry (neuron state in shared memory, most blocks per SM).  A
+        // larger set steps more slowly per job, so a backlog that admitted
+        // everything would lower the throughput that has to clear it.
+        const uint64_t chunk_cap = eng->fast_chunk_capacity();
         NAER_CK(cudaHostAlloc(reinterpret_cast<void**>(&rec), prm_.raster_capacity * sizeof(uint2),
                               cudaHostAllocDefault));
         NAER_CK(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
@@ -370,8 +378,18 @@ void Server::loop() {
                 std::unique_lock<std::mutex> lk(mu_);
                 if (running.empty() && !inflight) cv_work_.wait(lk, [&] { return stop_ || !ready_.empty(); });
                 if (stop_) break;
-                admit.assign(ready_.begin(), ready_.end());
-                ready_.clear();
+                uint64_t rc = 0;  // chunks of the jobs that stay after this boundary
+                const uint64_t hs0 = eng->host_step();
+                for (Job* j : running)
+                    if (j->net->dev.end_step > hs0) rc += j->chunks;
+                while (!ready_.empty()) {
+                    Job* j = ready_.front();
+                    const bool alone = rc == 0 && admit.empty();  // a job larger than the cap runs alone
+                    if (!alone && chunk_cap && rc + j->chunks > chunk_cap) break;
+                    admit.push_back(j);
+                    ready_.pop_front();
+                    rc += j->chunks;
+                }
                 const double t = now_s();
                 for (Job* j : admit) {
                     j->info.state = kJobRunning;
@@ -493,11 +511,14 @@ void Server::loop() {
                 st_.drain_s += t_drain;
                 st_.raster_dropped += dropped;
                 st_.running = running.size();
-                if (trace && done_len)
-                    std::fprintf(trace, "%.6f,%zu,%zu,%zu,%llu,%.3f,%.3f,%.3f,%.3f,%llu,%zu,%llu\n", tn2, running.size(),
-                                 admit.size(), finished.size(), (unsigned long long)done_len, done_ms, 1e3 * t_step,
-                                 1e3 * t_install, 1e3 * t_drain, (unsigned long long)nrec, pending_.size(),
-                                 (unsigned long long)used_);
+                if (trace && done_len) {
+                    uint64_t rchunks = 0;
+                    for (Job* j : running) rchunks += j->chunks;
+                    std::fprintf(trace, "%.6f,%zu,%zu,%zu,%llu,%.3f,%.3f,%.3f,%.3f,%llu,%zu,%llu,%llu,%llu\n", tn2,
+                                 running.size(), admit.size(), finished.size(), (unsigned long long)done_len, done_ms,
+                                 1e3 * t_step, 1e3 * t_install, 1e3 * t_drain, (unsigned long long)nrec, pending_.size(),
+                                 (unsigned long long)used_, (unsigned long long)rchunks, (unsigned long long)chunk_cap);
+                }
                 if (!finished.empty()) {
                     cv_done_.notify_all();
                     cv_build_.notify_all();

@@ -54,6 +54,7 @@ struct ServerParams {
     uint64_t raster_capacity = 1ull << 24;  // spike records per chunk
     uint32_t blocks_per_sm = 0;    // step-kernel blocks per SM (0 = most that fit)
     double chunk_ms = 10.0;        // target device time per chunk (sets its step count)
+    uint32_t launch_steps = 4;     // grid steps per persistent step launch (builds run between launches)
 };
 
 enum JobState : uint32_t { kJobQueued = 0, kJobRunning = 1, kJobDone = 2, kJobFailed = 3 };
@@ -105,6 +106,7 @@ private:
         std::unique_ptr<NetHost> net;
         JobInfo info;
         uint64_t est_bytes = 0;
+        uint32_t chunks = 0;    // LIF chunks it adds to the stepping engine
         std::vector<uint32_t> steps, ids;
         bool freed = false;     // holds no device memory
         bool released = false;  // forgotten by the caller: erase once freed

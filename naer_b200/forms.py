@@ -135,7 +135,7 @@ class Server:
 
     def __init__(self, device: int = 0, budget_bytes: int = 150 * 10**9, chunk_steps: int = 256,
                  deterministic: bool = False, max_jobs: int = 1024, raster_capacity: int = 1 << 24,
-                 blocks_per_sm: int = 0, chunk_ms: float = 10.0):
+                 blocks_per_sm: int = 0, chunk_ms: float = 10.0, launch_steps: int = 0):
         capi.load()
         p = capi.ServerParams()
         capi.call("naer_server_params_default", C.byref(p))
@@ -146,6 +146,7 @@ class Server:
         p.raster_capacity = int(raster_capacity)
         p.blocks_per_sm = int(blocks_per_sm)
         p.chunk_ms = float(chunk_ms)
+        p.launch_steps = int(launch_steps)
         h = C.c_void_p()
         capi.call("naer_server_create", int(device), C.byref(p), C.byref(h))
         self._h = h

@@ -165,6 +165,7 @@ def test_server_defaults(lib):
     p = capi.ServerParams()
     assert lib.naer_server_params_default(C.byref(p)) == 0
     assert p.budget_bytes == 150 * 10**9 and p.chunk_steps == 256 and p.aggregation == capi.AGG_ATOMIC
+    assert p.launch_steps == 0  # library default
 
 
 def test_forms_workloads():

@@ -125,10 +125,11 @@ def test_server_deterministic_jobs_match_alone(lib):
             srv.release(jid)
 
 
-def test_server_atomic_integer_weights_exact(lib):
+@pytest.mark.parametrize("launch_steps", [0, 16])
+def test_server_atomic_integer_weights_exact(lib, launch_steps):
     jobs = [(integer_weight_net(n=n, k=150, seed=sd), d) for n, sd, d in [(3000, 11, 400), (2000, 12, 250),
                                                                           (4000, 13, 512)]]
-    with Server(chunk_steps=128) as srv:
+    with Server(chunk_steps=128, launch_steps=launch_steps) as srv:
         ids = [srv.submit(m, d) for m, d in jobs]
         assert srv.drain(300.0)
         for jid, (m, d) in zip(ids, jobs):
@@ -149,3 +150,5 @@ def test_server_rejects_oversize_and_invalid(lib):
         with pytest.raises(NaerError, match="POISSON"):
             srv.submit(s, 10)
         assert srv.stats()["submitted"] == 0
+    with pytest.raises(NaerError, match="launch_steps"):
+        Server(budget_bytes=10**6, launch_steps=65)
