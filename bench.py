@@ -427,6 +427,28 @@ def run_ours(args):
         except Exception:
             traffic = None
 
+    # the device's own ceilings for this path (naer_probe_device): random
+    # fp32 reductions into a ring-sized buffer (one per event), random
+    # stores, streaming read, one grid barrier
+    probe = None
+    try:
+        from naer_b200 import _capi as capi
+        st_ = net.stats()
+        probe = capi.probe_device(local, ring_cells=st_["ring_slots"] * args.neurons,
+                                  small_cells=3 * args.neurons)
+    except Exception as e:  # reported, never fatal to the bench line
+        probe = {"error": str(e)}
+    # scatter phase of k_run alone (block 0's %globaltimer split): the
+    # figure the ring-accumulation and HBM ceilings bound
+    sc_ms = ph.get("scatter", 0.0)
+    scatter_phase = None
+    if sc_ms > 0:
+        sc_rate = pev / (sc_ms / 1e3)
+        scatter_phase = {"ms": sc_ms, "events_per_s": sc_rate, "achieved_gbs": BYTES_PER_EVENT * sc_rate / 1e9,
+                         "frac_hbm": BYTES_PER_EVENT * sc_rate / 1e9 / peak if peak else None,
+                         "frac_of_red_ceiling": (sc_rate / probe["red_ring_per_s"]
+                                                 if probe and probe.get("red_ring_per_s") else None)}
+
     # end to end through the C ABI: step calls + raster readback into pinned host memory
     e2e = None
     if not args.no_e2e:
@@ -480,6 +502,8 @@ def run_ours(args):
                                  f"(CUDA events); Poisson-draw kernel {prof['drive_kernel_ms']:.2f} ms; "
                                  f"phase split of k_run (block 0): "
                                  + ", ".join(f"{k} {v / ph_tot:.0%}" for k, v in ph.items())},
+            "scatter_phase": scatter_phase,
+            "device_probe": probe,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(st1["kernel_launches"] - st0["kernel_launches"]),

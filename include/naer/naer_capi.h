@@ -248,6 +248,43 @@ NAER_API int naer_net_get_phases(naer_net* net, double* phase_ms5);
 NAER_API int naer_net_get_launch_times(naer_net* net, double* drive_ms, double* step_kernel_ms,
                                        uint64_t* step_kernel_launches);
 
+/* Bounded device waits (no counterpart in the reference, whose OpenCL
+ * queue has none).  Every grid barrier of the step kernel gives up after
+ * limit_us microseconds (default 2 s), records NAER_E_TIMEOUT on the device
+ * and ends the launch; naer_net_finish then returns NAER_E_TIMEOUT and the
+ * network refuses further steps (NAER_E_STATE): its state is undefined, the
+ * handle can only be destroyed.  0 restores the default. */
+NAER_API int naer_net_set_wait_limit(naer_net* net, uint64_t limit_us);
+
+/* Fault injection for tests of the bounded wait (no counterpart in the
+ * reference).  A non-zero skew is added to every grid-barrier target of the
+ * following launches, so no barrier can complete and each wait runs out
+ * after the limit above; the kernel then returns normally with the error
+ * recorded.  Nothing else changes on the device.  0 = normal operation. */
+NAER_API int naer_test_set_barrier_skew(naer_net* net, uint64_t skew);
+
+/* ---- device probe ------------------------------------------------------
+ * No counterpart in the reference.  Measures, on `device`, the ceilings the
+ * step kernel is judged against: random-address fp32 reductions
+ * (red.global.add.f32, the atomic mode's ring accumulation) into
+ * ring_cells and small_cells cells, random 4-byte stores into ring_cells
+ * cells, a streaming read of 4 GiB with evict-first 128-bit loads, and one
+ * grid barrier of the step kernel's kind at one and two blocks per SM.
+ * Allocates and frees its own buffers (4 GiB plus 4 B per ring cell). */
+typedef struct naer_device_probe {
+    uint64_t ring_cells, small_cells;
+    double red_ring_per_s;    /* reductions per second into ring_cells cells */
+    double red_small_per_s;   /* reductions per second into small_cells cells */
+    double store_ring_per_s;  /* random stores per second into ring_cells cells */
+    double stream_gbs;        /* streaming read, GB/s */
+    double barrier_us_1;      /* one grid barrier, 1 block per SM, microseconds */
+    double barrier_us_2;      /* one grid barrier, 2 blocks per SM */
+    uint32_t grid;            /* SMs */
+    uint32_t pad_;
+} naer_device_probe;
+
+NAER_API int naer_probe_device(int device, uint64_t ring_cells, uint64_t small_cells, naer_device_probe* out);
+
 /* ---- batched form ------------------------------------------------------
  * No counterpart in the reference (one Network per device queue there).
  * Many independent networks of any sizes are packed, with offsets, into one
@@ -267,7 +304,17 @@ typedef struct naer_tuning {
     double default_us_per_step; /* autotune: time of the default geometry */
     uint32_t trials;          /* autotune: geometries timed */
     uint32_t scatter_piece;   /* synapses per warp iteration: 128, 256, 0 = 128 for plastic networks else 256 */
+    uint32_t neuron_state;    /* NAER_STATE_*: where the step kernel keeps membrane potentials and
+                                 refractory counters during a launch */
+    uint32_t pad_;
 } naer_tuning;
+
+/* naer_tuning.neuron_state.  AUTO: shared memory when the installed chunks
+ * fit it, else global memory.  SHARED: shared memory or NAER_E_INVALID.
+ * GLOBAL: global memory (the path large served sets fall back to). */
+#define NAER_STATE_AUTO 0u
+#define NAER_STATE_SHARED 1u
+#define NAER_STATE_GLOBAL 2u
 
 NAER_API int naer_batch_create(int device, uint32_t aggregation, uint64_t raster_capacity,
                                naer_batch** out);

@@ -110,7 +110,12 @@ class Tuning(C.Structure):
         ("default_us_per_step", C.c_double),
         ("trials", C.c_uint32),
         ("scatter_piece", C.c_uint32),
+        ("neuron_state", C.c_uint32),
+        ("pad_", C.c_uint32),
     ]
+
+
+STATE_AUTO, STATE_SHARED, STATE_GLOBAL = 0, 1, 2
 
 
 class ServerParams(C.Structure):
@@ -123,6 +128,21 @@ class ServerParams(C.Structure):
         ("blocks_per_sm", C.c_uint32),
         ("chunk_ms", C.c_double),
         ("launch_steps", C.c_uint32),
+        ("pad_", C.c_uint32),
+    ]
+
+
+class DeviceProbe(C.Structure):
+    _fields_ = [
+        ("ring_cells", C.c_uint64),
+        ("small_cells", C.c_uint64),
+        ("red_ring_per_s", C.c_double),
+        ("red_small_per_s", C.c_double),
+        ("store_ring_per_s", C.c_double),
+        ("stream_gbs", C.c_double),
+        ("barrier_us_1", C.c_double),
+        ("barrier_us_2", C.c_double),
+        ("grid", C.c_uint32),
         ("pad_", C.c_uint32),
     ]
 
@@ -192,6 +212,9 @@ PROTOTYPES = {
     "naer_net_get_profile": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
     "naer_net_get_phases": [_vp, _vp],
     "naer_net_get_launch_times": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
+    "naer_net_set_wait_limit": [_vp, C.c_uint64],
+    "naer_test_set_barrier_skew": [_vp, C.c_uint64],
+    "naer_probe_device": [C.c_int, C.c_uint64, C.c_uint64, _P(DeviceProbe)],
     "naer_net_autotune": [_vp, C.c_uint32, _P(Tuning)],
     "naer_net_set_tuning": [_vp, _P(Tuning)],
     "naer_net_get_tuning": [_vp, _P(Tuning)],
@@ -241,6 +264,14 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         fn.restype = C.c_int
     _lib = lib
     return lib
+
+
+def probe_device(device: int = 0, ring_cells: int = 17_000_000, small_cells: int = 3_000_000) -> dict:
+    """naer_probe_device: the device's random-reduction, random-store,
+    streaming and grid-barrier figures."""
+    p = DeviceProbe()
+    call("naer_probe_device", int(device), int(ring_cells), int(small_cells), C.byref(p))
+    return {k: getattr(p, k) for k, _ in DeviceProbe._fields_ if k != "pad_"}
 
 
 def last_error() -> str:

@@ -14,7 +14,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libnaer_b200.so"
 
-SOURCES = ["sim_kernels.cu", "build_kernels.cu", "engine.cu", "forms.cu", "capi.cu"]
+SOURCES = ["sim_kernels.cu", "build_kernels.cu", "engine.cu", "forms.cu", "probe.cu", "capi.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -213,12 +213,46 @@ int naer_net_step_noalloc(naer_net* net, uint64_t nsteps) {
     });
 }
 
+namespace {
+void throw_device_status(naer::Engine& eng) {
+    const int st = eng.device_status();
+    if (st == NAER_E_TIMEOUT)
+        throw Error(NAER_E_TIMEOUT, "a grid barrier of the step kernel ran out of its wait limit; the network's "
+                                    "state is undefined");
+    if (st) throw Error(st, "the device reported an error");
+}
+}  // namespace
+
 int naer_net_finish(naer_net* net) {
     return guarded([&] {
         need_compiled(net);
         net->eng->sync();
-        const naer::Ctl c = net->eng->read_ctl();
-        if (c.error) throw Error(NAER_E_CUDA, "device reported error flag " + std::to_string(c.error));
+        throw_device_status(*net->eng);
+    });
+}
+
+int naer_net_set_wait_limit(naer_net* net, uint64_t limit_us) {
+    return guarded([&] {
+        need_compiled(net);
+        need(limit_us <= 3600ull * 1000 * 1000, NAER_E_INVALID, "wait limit above one hour");
+        net->eng->set_barrier_limit(limit_us * 1000ull);
+    });
+}
+
+int naer_test_set_barrier_skew(naer_net* net, uint64_t skew) {
+    return guarded([&] {
+        need_compiled(net);
+        net->eng->set_barrier_skew(skew);
+    });
+}
+
+int naer_probe_device(int device, uint64_t ring_cells, uint64_t small_cells, naer_device_probe* out) {
+    return guarded([&] {
+        need(out != nullptr, NAER_E_INVALID, "null argument");
+        int n = 0;
+        NAER_CK(cudaGetDeviceCount(&n));
+        need(device >= 0 && device < n, NAER_E_INVALID, "device index out of range");
+        naer::probe_device(device, ring_cells, small_cells, out);
     });
 }
 
@@ -463,8 +497,7 @@ int naer_batch_finish(naer_batch* batch) {
     return guarded([&] {
         need(batch != nullptr && batch->b->compiled(), NAER_E_STATE, "batch is not compiled");
         batch->b->engine().sync();
-        const naer::Ctl c = batch->b->engine().read_ctl();
-        if (c.error) throw Error(NAER_E_CUDA, "device reported error flag " + std::to_string(c.error));
+        throw_device_status(batch->b->engine());
     });
 }
 
@@ -474,6 +507,7 @@ static void fill_tuning(naer_tuning* out, const naer::Tuning& t, uint32_t graph_
     out->launch_steps = t.launch_steps;
     out->scatter_split = t.scatter_split;
     out->scatter_piece = t.scatter_piece;
+    out->neuron_state = t.neuron_state;
     out->graph_launches = graph_launches;
 }
 
@@ -512,6 +546,7 @@ int naer_net_set_tuning(naer_net* net, const naer_tuning* tuning) {
         t.launch_steps = tuning->launch_steps;
         t.scatter_split = tuning->scatter_split;
         t.scatter_piece = tuning->scatter_piece;
+        t.neuron_state = tuning->neuron_state;
         net->eng->set_tuning(t);
     });
 }
@@ -533,6 +568,7 @@ int naer_batch_set_tuning(naer_batch* batch, const naer_tuning* tuning) {
         t.launch_steps = tuning->launch_steps;
         t.scatter_split = tuning->scatter_split;
         t.scatter_piece = tuning->scatter_piece;
+        t.neuron_state = tuning->neuron_state;
         batch->b->engine().set_tuning(t);
         batch->graph_launches = tuning->graph_launches;
     });

@@ -109,7 +109,7 @@ Engine::Engine(int device, int priority) : device_(device) {
     d_ctl_ = static_cast<Ctl*>(dalloc(sizeof(Ctl)));
     NAER_CK(cudaMemsetAsync(d_ctl_, 0, sizeof(Ctl), stream_));
     NAER_CK(cudaStreamSynchronize(stream_));
-    NAER_CK(cudaMallocHost(&h_pinned_, 256));
+    NAER_CK(cudaMallocHost(&h_pinned_, 512));  // [0, 256): control block copies; [256, 512): host->device words
 }
 
 Engine::~Engine() {
@@ -609,6 +609,9 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     DeviceGuard g(device_);
     NAER_CK(cudaStreamSynchronize(stream_));
     drop_graph();
+    // the fixed-scratch partition was cut for the previous geometry: the
+    // next fixed-scratch call repartitions and re-checks the fit
+    fs_.ready = false;
     nets_ = nets;
     aggregation_ = aggregation;
     inst_raster_cap_ = raster_capacity;
@@ -702,7 +705,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     use_smem_state_ = false;
     lif_grid_ = 0;
     const int bps_hi = tuning_.blocks_per_sm ? (int)std::min<uint32_t>(tuning_.blocks_per_sm, 4) : 4;
-    for (int bps = bps_hi; bps >= 1 && !use_smem_state_; --bps) {
+    for (int bps = bps_hi; bps >= 1 && !use_smem_state_ && tuning_.neuron_state != NAER_STATE_GLOBAL; --bps) {
         const uint32_t grid = (uint32_t)bps * sm_count_;
         const uint32_t own = std::max<uint32_t>(1, (eng_.n_chunks + grid - 1) / grid);
         const size_t smem = run_smem_bytes(grid, own, true);
@@ -715,6 +718,8 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
             scatter_smem_ = smem;
         }
     }
+    if (!use_smem_state_ && tuning_.neuron_state == NAER_STATE_SHARED)
+        throw Error(NAER_E_INVALID, "neuron state does not fit shared memory at this geometry");
     if (!use_smem_state_) {
         int occ = 0;
         const size_t smem_bound = run_smem_bytes((uint32_t)sm_count_ * 4, 1, false);
@@ -792,6 +797,7 @@ void Engine::set_tuning(const Tuning& t) {
     if (v.blocks_per_sm > 4) throw Error(NAER_E_INVALID, "blocks_per_sm must be in 0..4");
     if (v.scatter_piece != 0 && v.scatter_piece != 128 && v.scatter_piece != kScatterPiece)
         throw Error(NAER_E_INVALID, "scatter_piece must be 0, 128 or 256");
+    if (v.neuron_state > NAER_STATE_GLOBAL) throw Error(NAER_E_INVALID, "unknown neuron_state");
     tuning_ = v;
     if (!nets_.empty()) install(std::vector<NetHost*>(nets_), inst_raster_cap_, inst_record_, aggregation_);
 }
@@ -983,6 +989,7 @@ void Engine::launch_drive(uint64_t s_first, uint32_t nsteps) {
 void Engine::run(uint64_t nsteps) {
     DeviceGuard g(device_);
     if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
+    check_usable();
     if (aggregation_ == NAER_AGG_DETERMINISTIC) {
         for (uint64_t i = 0; i < nsteps; ++i) run_deterministic_step();
         return;
@@ -1001,6 +1008,7 @@ void Engine::run(uint64_t nsteps) {
 uint64_t Engine::run_graph(uint64_t nsteps, uint32_t graph_launches) {
     DeviceGuard g(device_);
     if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
+    check_usable();
     if (aggregation_ == NAER_AGG_DETERMINISTIC || graph_launches == 0) {
         run(nsteps);
         return 0;
@@ -1043,26 +1051,42 @@ uint64_t Engine::run_graph(uint64_t nsteps, uint32_t graph_launches) {
 }
 
 void Engine::ensure_det_capacity(uint64_t events) {
-    if (events <= e_cap_ && q_keys_[0]) return;
-    uint64_t cap = std::max<uint64_t>(events, 1 << 16);
-    if (cap < e_cap_ * 2 && e_cap_) cap = e_cap_ * 2;
-    for (int i = 0; i < 2; ++i) {
-        if (e_keys_[i]) dfree(e_keys_[i], e_cap_ * 8ull);
-        if (e_vals_[i]) dfree(e_vals_[i], e_cap_ * 4ull);
-        e_keys_[i] = static_cast<unsigned long long*>(dalloc(cap * 8ull));
-        e_vals_[i] = static_cast<float*>(dalloc(cap * 4ull));
-    }
-    e_cap_ = cap;
-    if (!q_keys_[0]) {
-        const uint64_t q = std::max<uint32_t>(queue_cap_, 1);
+    // Every buffer is checked against the geometry installed now: install()
+    // may have raised the queue capacity or the LIF grid since the buffers
+    // were sized (the served form reinstalls on every change of its set).
+    const uint64_t q = std::max<uint32_t>(queue_cap_, 1);
+    const uint64_t pre = (uint64_t)lif_grid_ + 1;
+    if (events <= e_cap_ && q <= q_cap_alloc_ && pre <= det_prefix_cap_) return;
+    if (events > e_cap_) {
+        uint64_t cap = std::max<uint64_t>(events, 1 << 16);
+        if (cap < e_cap_ * 2 && e_cap_) cap = e_cap_ * 2;
         for (int i = 0; i < 2; ++i) {
+            if (e_keys_[i]) dfree(e_keys_[i], e_cap_ * 8ull);
+            if (e_vals_[i]) dfree(e_vals_[i], e_cap_ * 4ull);
+            e_keys_[i] = static_cast<unsigned long long*>(dalloc(cap * 8ull));
+            e_vals_[i] = static_cast<float*>(dalloc(cap * 4ull));
+        }
+        e_cap_ = cap;
+    }
+    if (q > q_cap_alloc_) {
+        for (int i = 0; i < 2; ++i) {
+            if (q_keys_[i]) dfree(q_keys_[i], q_cap_alloc_ * 8ull);
+            if (q_vals_[i]) dfree(q_vals_[i], q_cap_alloc_ * 4ull);
             q_keys_[i] = static_cast<unsigned long long*>(dalloc(q * 8ull));
             q_vals_[i] = static_cast<uint32_t*>(dalloc(q * 4ull));
         }
+        if (q_sizes_) dfree(q_sizes_, q_cap_alloc_ * 4ull);
+        if (q_offs_) dfree(q_offs_, q_cap_alloc_ * 4ull);
         q_sizes_ = static_cast<uint32_t*>(dalloc(q * 4ull));
         q_offs_ = static_cast<uint32_t*>(dalloc(q * 4ull));
+        q_cap_alloc_ = q;
     }
-    if (!det_prefix_) det_prefix_ = static_cast<uint32_t*>(dalloc((lif_grid_ + 1) * sizeof(uint32_t)));
+    if (pre > det_prefix_cap_) {
+        if (det_prefix_) dfree(det_prefix_, det_prefix_cap_ * sizeof(uint32_t));
+        det_prefix_ = static_cast<uint32_t*>(dalloc(pre * sizeof(uint32_t)));
+        det_prefix_cap_ = pre;
+    }
+    const uint64_t cap = e_cap_;
     // CUB scratch large enough for every sort/scan of this capacity
     size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
     const int qn = (int)std::max<uint32_t>(queue_cap_, 1);
@@ -1083,7 +1107,7 @@ void Engine::ensure_det_capacity(uint64_t events) {
 void Engine::run_deterministic_step() {
     cudaStream_t st = stream_;
     uint64_t own_launches = 2;  // LIF, advance (launch_drive counts itself)
-    if (!q_keys_[0]) ensure_det_capacity(1);
+    ensure_det_capacity(1);  // buffers follow the installed geometry
     const uint32_t T = 256;
     launch_drive(host_step_, 1);
     k_lif<<<lif_grid_, kLifThreads, 0, st>>>(eng_);
@@ -1108,6 +1132,7 @@ void Engine::run_deterministic_step() {
         NAER_CK(cudaStreamSynchronize(st));
         const uint64_t E = (uint64_t)h_pinned_[0] + h_pinned_[1];
         if (E > 0x7FFFFFFFull) throw Error(NAER_E_OVERFLOW, "more than 2^31 events in one step");
+        if (Q > q_cap_alloc_) throw Error(NAER_E_OVERFLOW, "spike count exceeds the sorted queue");
         k_det_raster<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + T - 1) / T, 1024)), T, 0, st>>>(eng_, q_vals_[1], Q);
         if (E > 0) {
             own_launches += 2;  // emit, fold
@@ -1222,6 +1247,7 @@ void Engine::fixed_scratch_setup() {
 void Engine::run_fixed_scratch(uint64_t nsteps) {
     DeviceGuard g(device_);
     if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
+    check_usable();
     if (!fs_.ready) fixed_scratch_setup();
     for (uint64_t i = 0; i < nsteps; ++i) run_fixed_scratch_step();
 }
@@ -1242,7 +1268,12 @@ void Engine::run_fixed_scratch_step() {
     NAER_CK(cudaMemcpyAsync(h_pinned_, f.prefix + lif_grid_, 4, cudaMemcpyDeviceToHost, st));
     NAER_CK(cudaStreamSynchronize(st));
     const uint32_t Q = h_pinned_[0];
-    if (Q > f.q_max) throw Error(NAER_E_OVERFLOW, "spike count exceeds the fixed scratch");
+    // q_max covers every neuron and e_max every padded synapse, so neither
+    // check below can fire while the partition matches the installed
+    // geometry (install() invalidates it); they guard that invariant.  If
+    // one fired, the LIF of this step would already have run: the network's
+    // state would be undefined.
+    if (Q > f.q_max) throw Error(NAER_E_OVERFLOW, "internal: spike count exceeds the fixed scratch partition");
     if (Q > 0) {
         k_det_queue_keys<<<(Q + T - 1) / T, T, 0, st>>>(eng_, f.prefix, f.q_keys[0], f.q_vals[0], Q);
         cub::DoubleBuffer<unsigned long long> qk(f.q_keys[0], f.q_keys[1]);
@@ -1258,7 +1289,7 @@ void Engine::run_fixed_scratch_step() {
         NAER_CK(cudaMemcpyAsync(h_pinned_ + 1, f.q_sizes + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
         NAER_CK(cudaStreamSynchronize(st));
         const uint64_t E = (uint64_t)h_pinned_[0] + h_pinned_[1];
-        if (E > f.e_max) throw Error(NAER_E_OVERFLOW, "event count exceeds the fixed scratch");
+        if (E > f.e_max) throw Error(NAER_E_OVERFLOW, "internal: event count exceeds the fixed scratch partition");
         k_det_raster<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + T - 1) / T, 1024)), T, 0, st>>>(eng_, order, Q);
         if (E > 0) {
             own_launches += 2;  // emit, fold
@@ -1287,8 +1318,39 @@ void Engine::sync() {
     NAER_CK(cudaGetLastError());
 }
 
+void Engine::set_barrier_limit(uint64_t limit_ns) {
+    DeviceGuard g(device_);
+    const unsigned long long v = limit_ns;
+    std::memcpy(h_pinned_ + 64, &v, 8);
+    NAER_CK(cudaMemcpyAsync(&d_ctl_->bar_limit_ns, h_pinned_ + 64, 8, cudaMemcpyHostToDevice, stream_));
+    NAER_CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::set_barrier_skew(uint64_t skew) {
+    DeviceGuard g(device_);
+    const unsigned long long v = skew;
+    std::memcpy(h_pinned_ + 66, &v, 8);
+    NAER_CK(cudaMemcpyAsync(&d_ctl_->bar_skew, h_pinned_ + 66, 8, cudaMemcpyHostToDevice, stream_));
+    NAER_CK(cudaStreamSynchronize(stream_));
+}
+
+int Engine::device_status() {
+    const Ctl c = read_ctl();
+    if (c.error == 0) return 0;
+    failed_ = true;
+    return c.error == (unsigned int)(-NAER_STATUS_TIMEOUT) ? NAER_E_TIMEOUT : NAER_E_CUDA;
+}
+
+void Engine::check_usable() const {
+    if (failed_)
+        throw Error(NAER_E_STATE,
+                    "a previous launch reported a device error (bounded wait ran out): the network's state is "
+                    "undefined; destroy the handle");
+}
+
 Ctl Engine::read_ctl() {
     DeviceGuard g(device_);
+    static_assert(sizeof(Ctl) <= 256, "control block copy must fit the first half of the pinned staging");
     Ctl c;
     NAER_CK(cudaMemcpyAsync(h_pinned_, d_ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, stream_));
     NAER_CK(cudaStreamSynchronize(stream_));

@@ -81,6 +81,9 @@ uint64_t estimate_device_bytes(const NetHost& description);
 // network adds to an engine, from its description alone.
 uint32_t lif_chunks(const NetHost& description);
 
+// Device probe (probe.cu), see naer_probe_device.
+void probe_device(int device, uint64_t ring_cells, uint64_t small_cells, naer_device_probe* out);
+
 // Launch geometry of the persistent step loop (all choices leave the
 // simulated results unchanged).
 struct Tuning {
@@ -88,6 +91,7 @@ struct Tuning {
     uint32_t launch_steps = kDriveSlots;   // grid steps per persistent launch (1..kDriveSlots)
     uint32_t scatter_split = 0;            // warps per spike (0 = enough to cover the longest row)
     uint32_t scatter_piece = 0;            // synapses per warp iteration: 128, 256, 0 = 128 with STDP else 256
+    uint32_t neuron_state = 0;             // NAER_STATE_AUTO / _SHARED / _GLOBAL: where the step kernel keeps V
 };
 
 struct TuneResult {
@@ -169,6 +173,14 @@ public:
     void* dalloc(size_t bytes);
     void dfree(void* p, size_t bytes);
 
+    // Bounded waits of the step kernel's grid barriers (0 = default) and the
+    // test hook that makes every barrier unsatisfiable (see naer_capi.h).
+    void set_barrier_limit(uint64_t limit_ns);
+    void set_barrier_skew(uint64_t skew);
+    // Device error flag of the control block, as a NAER_E_* status (0 =
+    // none); once non-zero the engine refuses further steps.
+    int device_status();
+
 private:
     void launch_run(uint32_t steps);
     void launch_drive(uint64_t s_first, uint32_t nsteps);
@@ -227,6 +239,8 @@ private:
     unsigned long long* e_keys_[2] = {nullptr, nullptr};
     float* e_vals_[2] = {nullptr, nullptr};
     uint64_t e_cap_ = 0;
+    uint64_t q_cap_alloc_ = 0;     // entries of q_keys_/q_vals_/q_sizes_/q_offs_
+    uint64_t det_prefix_cap_ = 0;  // entries of det_prefix_
     void* cub_tmp_ = nullptr;
     size_t cub_tmp_bytes_ = 0;
     uint32_t* h_pinned_ = nullptr;  // small pinned staging
@@ -251,6 +265,8 @@ private:
     void fixed_scratch_setup();
     void run_fixed_scratch_step();
 
+    bool failed_ = false;  // a launch reported a device error: state undefined
+    void check_usable() const;
     bool profiling_ = false;
     bool use_smem_state_ = false;
     // CUDA-event timing of launches while profiling (pairs in launch order)

@@ -140,7 +140,12 @@ struct Ctl {
     unsigned long long bar_arrive;  // grid barrier arrivals of the running launch
     unsigned int error;
     unsigned int pad_;
+    unsigned long long bar_limit_ns;  // bounded wait of one grid barrier (0 = kBarrierLimitNs)
+    unsigned long long bar_skew;      // added to every barrier target: 0, except when a test makes the
+                                      // wait unsatisfiable to exercise the timeout (naer_test_set_barrier_skew)
 };
+
+constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // 2 s
 
 constexpr int NAER_STATUS_TIMEOUT = -4;  // NAER_E_TIMEOUT of the C ABI
 

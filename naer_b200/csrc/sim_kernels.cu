@@ -8,6 +8,7 @@
 // counter) and publishes one count; each scatter block prefix-sums the
 // counts in shared memory.  The only global atomics are the ring
 // reductions themselves.
+#include "grid_sync.cuh"
 #include "sim_kernels.cuh"
 
 namespace naer {
@@ -463,44 +464,6 @@ __device__ __forceinline__ void scatter_step(const EngineDev& eng, unsigned long
     }
 }
 
-// Grid-wide barrier of the persistent kernel: every block adds one to an
-// arrival counter (zeroed by the host before each launch) with a release
-// reduction and waits until it reaches `target` (barrier number times the
-// grid size).  The wait is bounded: after kBarrierTimeoutNs the block records
-// NAER_E_TIMEOUT in ctl->error and reports failure, and the kernel returns.
-// Co-residency of all blocks is guaranteed by the cooperative launch.
-constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
-
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ bool grid_barrier(Ctl* ctl, unsigned long long target) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        s_ok = 1;
-        __threadfence();  // this block's stores and reductions are visible before it arrives
-        asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(&ctl->bar_arrive) : "memory");
-        const unsigned long long t0 = globaltimer_ns();
-        unsigned long long cur;
-        for (;;) {
-            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(cur) : "l"(&ctl->bar_arrive) : "memory");
-            if (cur >= target) break;
-            if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
-                atomicCAS(&ctl->error, 0u, (unsigned int)(-NAER_STATUS_TIMEOUT));
-                s_ok = 0;
-                break;
-            }
-            __nanosleep(20);
-        }
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
 // Descriptor of one chunk owned by a persistent block, cached in shared
 // memory for the whole launch.
 struct ChunkCache {
@@ -661,6 +624,8 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
     const uint32_t own = blockIdx.x < eng.n_chunks ? (eng.n_chunks - blockIdx.x + G - 1) / G : 0u;
 
     Ctl* ctl = eng.ctl;
+    __shared__ BarrierCfg bcfg;  // read by thread 0 at each barrier; kept out of registers
+    if (threadIdx.x == 0) bcfg = barrier_cfg(ctl);
     unsigned long long bar_target = 0;
     // every block reads the engine step before the first grid barrier; block 0
     // advances it only after the last one
@@ -740,7 +705,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         if (threadIdx.x == 0) (qb ? eng.counts[1] : eng.counts[0])[blockIdx.x] = s_count;
         const unsigned long long ta2 = timer ? globaltimer_ns() : 0ull;
         bar_target += G;
-        if (!grid_barrier(ctl, bar_target)) break;
+        if (!grid_barrier(ctl, bar_target, bcfg)) break;
         const unsigned long long tb = timer ? globaltimer_ns() : 0ull;
 
         const uint32_t Q = block_prefix_counts(qb ? eng.counts[1] : eng.counts[0], G, s_prefix);
@@ -751,7 +716,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         if (eng.record) dropped += Q - kept;
         rbase += kept;
         bar_target += G;
-        if (!grid_barrier(ctl, bar_target)) break;
+        if (!grid_barrier(ctl, bar_target, bcfg)) break;
         if (timer) {
             const unsigned long long tc = globaltimer_ns();
             t_lif += tb - ta;

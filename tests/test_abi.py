@@ -50,7 +50,7 @@ def test_struct_layout_matches_header(lib, tmp_path):
     structs = {"naer_net_params": capi.NetParams, "naer_pop_params": capi.PopParams,
                "naer_conn_spec": capi.ConnSpecC, "naer_stats": capi.Stats, "naer_tuning": capi.Tuning,
                "naer_server_params": capi.ServerParams, "naer_job_info": capi.JobInfo,
-               "naer_server_stats": capi.ServerStats}
+               "naer_server_stats": capi.ServerStats, "naer_device_probe": capi.DeviceProbe}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "naer/naer_capi.h"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

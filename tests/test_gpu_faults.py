@@ -1,0 +1,73 @@
+"""Failure paths on the GPU, made without any fault: every wait of the step
+kernel is bounded, and a test makes one run out on purpose.
+
+naer_test_set_barrier_skew raises every grid-barrier target of the next
+launches, so no barrier can complete; each block's wait gives up after the
+limit set by naer_net_set_wait_limit (here 1 ms), records NAER_E_TIMEOUT in
+the control block and returns.  The host then sees NAER_E_TIMEOUT from
+naer_net_finish, the handle refuses further steps, is destroyed normally,
+and a fresh network on the same device steps bit-exact with the oracle
+(the context is still usable).  The reference reports device failures by
+throwing (src/Network.cpp:21-23, 146-149); here they are status codes.
+"""
+import numpy as np
+import pytest
+
+from naer_b200 import _capi as capi
+from naer_b200 import spec as S
+
+from nets import integer_weight_net
+
+pytestmark = pytest.mark.gpu
+
+
+def test_barrier_wait_runs_out_and_context_survives(oracle_mod, lib):
+    s = integer_weight_net(n=6000, k=300, seed=3)
+    net = S.build(s)
+    try:
+        net.run(5)
+        net.finish()
+        capi.call("naer_net_set_wait_limit", net.handle, 1000)  # 1 ms
+        capi.call("naer_test_set_barrier_skew", net.handle, 1)
+        net.run(130)  # three persistent launches, each ends at its first barrier
+        rc = lib.naer_net_finish(net.handle)
+        assert rc == capi.NAER_E_TIMEOUT, (rc, capi.last_error())
+        assert "wait limit" in capi.last_error()
+        rc = lib.naer_net_step(net.handle, 1)
+        assert rc == capi.NAER_E_STATE
+        assert "undefined" in capi.last_error()
+    finally:
+        net.close()
+    # the device context is intact: a new network runs and matches the oracle
+    with S.build(s) as fresh:
+        fresh.run(300)
+        fresh.finish()
+        st, ids = fresh.read_spikes()
+        v, r = fresh.read_state()
+    o = oracle_mod.OracleNet(s, deterministic=True)
+    o.run(300)
+    ost, oids = o.spikes()
+    ov, orr = o.state()
+    o.close()
+    assert len(ids) > 100
+    assert np.array_equal(st, ost) and np.array_equal(ids, oids)
+    assert np.array_equal(v.view(np.uint32), ov.view(np.uint32)) and np.array_equal(r, orr)
+
+
+def test_wait_limit_validation(lib):
+    with S.build(integer_weight_net(n=2000, k=50)) as net:
+        assert lib.naer_net_set_wait_limit(net.handle, 4_000_000_000) == capi.NAER_E_INVALID
+        capi.call("naer_net_set_wait_limit", net.handle, 0)  # default restored
+        net.run(70)
+        net.finish()
+        assert net.stats()["step"] == 70
+
+
+def test_device_probe_figures(lib):
+    """The ceilings bench.py reports: positive, finite and ordered sensibly."""
+    p = capi.probe_device(0, ring_cells=17_000_000, small_cells=3_000_000)
+    assert p["grid"] >= 100
+    for k in ("red_ring_per_s", "red_small_per_s", "store_ring_per_s"):
+        assert 1e9 < p[k] < 1e14, (k, p[k])
+    assert 500 < p["stream_gbs"] < 20_000
+    assert 0.05 < p["barrier_us_1"] < 100 and 0.05 < p["barrier_us_2"] < 100

@@ -152,3 +152,28 @@ def test_server_rejects_oversize_and_invalid(lib):
         assert srv.stats()["submitted"] == 0
     with pytest.raises(NaerError, match="launch_steps"):
         Server(budget_bytes=10**6, launch_steps=65)
+
+
+def test_server_deterministic_set_outgrows_the_queue(lib):
+    """A deterministic served set whose LIF chunks grow past the step
+    grid's blocks after the first installation (one block per SM, so 148
+    blocks): the queue and sort buffers sized for the first, one-chunk set
+    must grow with the set.  Both jobs still match their runs alone."""
+    small = S.plastic_indegree(n=1500, k=60, seed=21, drive_rate_hz=40.0)
+    big = S.plastic_indegree(n=200_000, k=40, seed=22, drive_rate_hz=20.0, stdp=False)
+    with Server(chunk_steps=32, blocks_per_sm=1, deterministic=True) as srv:
+        a = srv.submit(small, 4000)
+        import time
+        t0 = time.time()
+        while srv.info(a)["state"] != capi.JOB_RUNNING and time.time() - t0 < 60:
+            time.sleep(0.01)  # the small job is installed alone first
+        assert srv.info(a)["state"] == capi.JOB_RUNNING
+        b = srv.submit(big, 120)
+        assert srv.drain(300.0)
+        assert srv.stats()["failed"] == 0
+        assert srv.info(b)["admit_s"] < srv.info(a)["done_s"]  # the two ran together
+        for jid, (m, d) in [(a, (small, 4000)), (b, (big, 120))]:
+            s_st, s_ids = srv.spikes(jid)
+            a_st, a_ids, _, _ = alone(m, d)
+            assert len(a_ids) > 50
+            assert np.array_equal(s_st, a_st) and np.array_equal(s_ids, a_ids), m.name

@@ -77,3 +77,45 @@ def test_noalloc_rejects_atomic_network(lib):
         assert step_noalloc(net, 1) == capi.NAER_E_STATE
         assert "deterministic aggregation" in capi.last_error()
         assert net.stats()["step"] == 0
+
+
+def test_noalloc_follows_a_reinstall(lib):
+    """A reinstall between calls (set_tuning to one block per SM, then back
+    to the default) changes the step grid and the queue; the next call
+    repartitions the arena for it.  Word-for-word equal to naer_net_step."""
+    s = S.brunel_small(poisson_weight=1.0).with_(deterministic=True)
+    with S.build(s) as ref, S.build(s) as net:
+        for bps, n in ((1, 120), (0, 180), (1, 90)):
+            net.set_tuning(blocks_per_sm=bps)
+            ref.run(n)
+            ref.finish()
+            assert step_noalloc(net, n) == capi.NAER_OK, capi.last_error()
+            net.finish()
+            assert_same(ref, net, False)
+        assert net.stats()["step"] == 390
+
+
+def test_noalloc_largest_accepted_network(lib):
+    """The largest fixed out-degree network (degree 100) the arena accepts,
+    found by growing it until the first call is refused, runs word for word
+    like naer_net_step on two calls in a row."""
+    def make(n):
+        return S.scatter_outdegree(n=n, k=100, drive_weight=24.0).with_(deterministic=True)
+    best = None
+    for n in range(4000, 40001, 2000):
+        with S.build(make(n)) as net:
+            rc = step_noalloc(net, 1)
+            if rc == capi.NAER_E_OVERFLOW:
+                assert net.stats()["step"] == 0
+                break
+            assert rc == capi.NAER_OK, capi.last_error()
+            best = n
+    assert best is not None and best < 40000, best
+    s = make(best)
+    with S.build(s) as ref, S.build(s) as net:
+        for n in (200, 300):
+            ref.run(n)
+            ref.finish()
+            assert step_noalloc(net, n) == capi.NAER_OK, capi.last_error()
+            net.finish()
+            assert assert_same(ref, net, False) > 100
