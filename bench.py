@@ -51,7 +51,12 @@ def parse():
     ap.add_argument("--batch-members", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=20000, help="grid steps per member (2 s)")
     ap.add_argument("--served-jobs", type=int, default=2000)
-    ap.add_argument("--plain-sample", type=int, default=6, help="jobs run one at a time for the plain arm")
+    ap.add_argument("--plain-sample", type=int, default=16, help="jobs run one at a time for the plain arm")
+    ap.add_argument("--det-steps", type=int, default=2000, help="timed grid steps of the deterministic plain run")
+    ap.add_argument("--step-kernel", default="split", choices=["split", "two_barrier"],
+                    help="persistent step kernel of the plain runs")
+    ap.add_argument("--no-det", action="store_true", help="skip the deterministic-mode measurements")
+    ap.add_argument("--no-saturated", action="store_true", help="skip the served form's saturation run")
     return ap.parse_args()
 
 
@@ -218,23 +223,30 @@ def run_reference(args):
     return 0
 
 
-def plain_runs(specs_steps, local):
+def plain_runs(specs_steps, local, rasters=False):
     """Each job alone with the plain form, one after another: build, run,
-    read the raster back.  Returns per-job seconds (run only, with build)."""
+    read the raster back.  Returns per-job seconds (run only, with build)
+    and, with rasters=True, each job's (steps, ids)."""
     from naer_b200 import spec as S
-    run_s, all_s = [], []
+    run_s, all_s, out = [], [], []
     for spec, steps in specs_steps:
         t0 = time.perf_counter()
         net = S.build(spec, device=local)
         t1 = time.perf_counter()
         net.run(steps)
         net.finish()
-        net.read_spikes()
+        r = net.read_spikes()
         t2 = time.perf_counter()
         net.close()
         run_s.append(t2 - t1)
         all_s.append(t2 - t0)
-    return run_s, all_s
+        out.append(r)
+    return (run_s, all_s, out) if rasters else (run_s, all_s)
+
+
+def same_raster(a, b):
+    import numpy as np
+    return len(a[1]) == len(b[1]) and bool(np.array_equal(a[0], b[0])) and bool(np.array_equal(a[1], b[1]))
 
 
 def bench_plastic(args, local, stream_of):
@@ -267,21 +279,22 @@ def bench_plastic(args, local, stream_of):
             "stdp_history_overflows": int(st1["stdp_hist_overflow"])}
 
 
-def bench_batched(args, local):
+def bench_batched(args, local, deterministic=False):
     """Batched form: independent networks of uneven sizes (log-uniform 2k-50k
     neurons, in-degree 100-1000, own seeds, Poisson 5-30 Hz, STDP on half)
     packed into one engine, autotuned, CUDA-graph step loop, 2 s simulated
     each; against one-at-a-time plain runs of a seeded sample of the same
-    members."""
+    members (deterministic mode: the sample's rasters must equal their
+    members' rasters in the batch, bit for bit)."""
     import numpy as np
     from naer_b200 import spec as S
     from naer_b200.forms import Batch
-    members = S.batch_members(count=args.batch_members, seed=1)
+    members = [m.with_(deterministic=deterministic) for m in S.batch_members(count=args.batch_members, seed=1)]
     for m in members:
         m.raster_capacity = 1 << 22
     steps = args.batch_steps
     t0 = time.perf_counter()
-    b = Batch(members, device=local, raster_capacity=1 << 26).compile()
+    b = Batch(members, device=local, deterministic=deterministic, raster_capacity=1 << 27).compile()
     t1 = time.perf_counter()
     st0 = b.stats()
     t2 = time.perf_counter()
@@ -291,56 +304,78 @@ def bench_batched(args, local):
     b.finish()
     t3 = time.perf_counter()
     st1 = b.stats()
-    b.close()
-    sim_s = t3 - t2
     rng = np.random.default_rng(7)
     pick = rng.choice(len(members), min(args.plain_sample, len(members)), replace=False)
-    run_s, all_s = plain_runs([(members[int(i)], steps) for i in pick], local)
+    identical = None
+    if deterministic:
+        sp = b.read_spikes()
+        run_s, all_s, alone = plain_runs([(members[int(i)], steps) for i in pick], local, rasters=True)
+        identical = all(same_raster(b.member_spikes(int(i), sp), a) for i, a in zip(pick, alone))
+    else:
+        run_s, all_s = plain_runs([(members[int(i)], steps) for i in pick], local)
+    b.close()
+    sim_s = t3 - t2
     plain_rate = 1.0 / float(np.mean(run_s))
+    sem = float(np.std(run_s, ddof=1) / np.sqrt(len(run_s))) if len(run_s) > 1 else 0.0
     return {
         "workload": f"{len(members)} networks, {st0['neurons']} neurons, {st0['synapses']} synapses in total; "
                     f"{steps} grid steps (2 s) each",
+        "aggregation": "deterministic" if deterministic else "atomic",
         "sims_per_s": len(members) / sim_s,
         "sims_per_s_with_build": len(members) / (sim_s + t1 - t0),
         "events_per_s": (st1["events"] - st0["events"]) / sim_s,
         "us_per_step": sim_s / steps * 1e6,
         "build_s": t1 - t0,
         "autotune": {k: tune[k] for k in ("blocks_per_sm", "launch_steps", "scatter_split", "graph_launches",
-                                          "best_us_per_step", "default_us_per_step", "trials")},
+                                          "step_kernel", "best_us_per_step", "default_us_per_step", "trials")},
         "plain_sims_per_s": plain_rate,
         "plain_sims_per_s_with_build": 1.0 / float(np.mean(all_s)),
-        "plain_sample": f"{len(pick)} members run alone one after another (mean {np.mean(run_s):.3f} s each)",
+        "plain_sample": f"{len(pick)} members run alone one after another (mean {np.mean(run_s):.3f} s each, "
+                        f"standard error {sem:.3f} s)",
         "speedup_vs_plain": (len(members) / sim_s) / plain_rate,
+        "rasters_identical_to_alone": identical,
         "raster_records": int(st1["spikes"]),
     }
 
 
-def bench_served(args, local):
+def bench_served(args, local, deterministic=False, saturate=False):
     """Served form: a seeded Poisson stream of jobs (50/s; 1k-200k neurons
     log-uniform, in-degree 100-1000, 100 ms - 2 s, 30 % STDP) submitted on
     schedule to the continuous-batching server (150 GB budget); p50/p99
     latency from submission to raster delivered; against the same jobs' plain
-    one-at-a-time runs (a seeded sample)."""
+    one-at-a-time runs (a seeded sample).  saturate=True submits every job
+    at once: sims/s is then the server's capacity, not the arrival rate.
+    Deterministic mode: the sample's rasters must equal their jobs' rasters
+    in the mix, bit for bit."""
     import numpy as np
     from naer_b200 import spec as S
     from naer_b200.forms import Server
     jobs = S.served_jobs(count=args.served_jobs, seed=1)
-    srv = Server(device=local, budget_bytes=150 * 10**9, chunk_steps=256)
+    jobs = [(ta, spec.with_(deterministic=deterministic), steps) for ta, spec, steps in jobs]
+    srv = Server(device=local, budget_bytes=150 * 10**9, chunk_steps=256, deterministic=deterministic)
+    ids = []
     t0 = time.perf_counter()
     for ta, spec, steps in jobs:
         now = time.perf_counter() - t0
-        if ta > now:
+        if not saturate and ta > now:
             time.sleep(ta - now)
-        srv.submit(spec, steps)
+        ids.append(srv.submit(spec, steps))
     ok = srv.drain(1800.0)
     wall = time.perf_counter() - t0
     st = srv.stats()
-    srv.close()
     rng = np.random.default_rng(11)
     pick = rng.choice(len(jobs), min(args.plain_sample, len(jobs)), replace=False)
-    run_s, all_s = plain_runs([(jobs[int(i)][1], jobs[int(i)][2]) for i in pick], local)
+    identical = None
+    if deterministic:
+        run_s, all_s, alone = plain_runs([(jobs[int(i)][1], jobs[int(i)][2]) for i in pick], local, rasters=True)
+        identical = all(same_raster(srv.spikes(ids[int(i)]), a) for i, a in zip(pick, alone))
+    else:
+        run_s, all_s = plain_runs([(jobs[int(i)][1], jobs[int(i)][2]) for i in pick], local)
+    srv.close()
     return {
-        "workload": f"{len(jobs)} jobs, Poisson arrivals at 50/s over {jobs[-1][0]:.1f} s",
+        "workload": f"{len(jobs)} jobs, " + ("all submitted at once" if saturate else
+                                            f"Poisson arrivals at 50/s over {jobs[-1][0]:.1f} s"),
+        "aggregation": "deterministic" if deterministic else "atomic",
         "sims_per_s": st["sims_per_s"],
         "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
         "drained": ok, "wall_s": wall, "done": st["done"], "failed": st["failed"],
@@ -350,7 +385,35 @@ def bench_served(args, local):
         "plain_latency_ms_mean": 1e3 * float(np.mean(all_s)),
         "plain_sample": f"{len(pick)} jobs run alone one after another (build + run + raster read)",
         "speedup_vs_plain": st["sims_per_s"] * float(np.mean(all_s)),
+        "rasters_identical_to_alone": identical,
     }
+
+
+def bench_deterministic(args, local, stream_of):
+    """The roofline workload in deterministic aggregation (bit-reproducible
+    rasters): events/s over the timed steps, CUDA events on its stream."""
+    import torch
+    from naer_b200 import spec as S
+    spec = workload(args).with_(deterministic=True)
+    spec.raster_capacity = 1 << 24
+    net = S.build(spec, device=local)
+    stream = stream_of(net)
+    net.run(256)
+    net.finish()
+    st0 = net.stats()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    net.run(args.det_steps)
+    e1.record(stream)
+    e1.synchronize()
+    st1 = net.stats()
+    ms = e0.elapsed_time(e1)
+    net.close()
+    ev = st1["events"] - st0["events"]
+    return {"workload": workload_config(args, int(st1["synapses"]))["workload"],
+            "aggregation": "deterministic", "steps": args.det_steps, "ms": ms,
+            "events_per_s": ev / (ms / 1e3), "ms_per_simulated_s": ms * 1e4 / args.det_steps}
 
 
 def run_ours(args):
@@ -363,6 +426,10 @@ def run_ours(args):
 
     spec = workload(args, seed=1 + rank)
     net = S.build(spec, device=local)
+    from naer_b200 import _capi as capi_
+    kern = capi_.KERNEL_SPLIT if args.step_kernel == "split" else capi_.KERNEL_TWO_BARRIER
+    if kern != capi_.KERNEL_SPLIT:
+        net.set_tuning(step_kernel=kern)
     stream = torch.cuda.ExternalStream(net.stream(), device=torch.device("cuda", local))
     chunk = args.chunk
 
@@ -486,6 +553,14 @@ def run_ours(args):
             args, local, lambda n: torch.cuda.ExternalStream(n.stream(), device=torch.device("cuda", local)))
         forms["batched"] = bench_batched(args, local)
         forms["served"] = bench_served(args, local)
+        if not args.no_saturated:
+            forms["served_saturated"] = bench_served(args, local, saturate=True)
+        if not args.no_det:
+            forms["batched_deterministic"] = bench_batched(args, local, deterministic=True)
+            forms["served_deterministic"] = bench_served(args, local, deterministic=True, saturate=True)
+    if rank == 0 and world == 1 and not args.no_det:
+        forms["deterministic"] = bench_deterministic(
+            args, local, lambda n: torch.cuda.ExternalStream(n.stream(), device=torch.device("cuda", local)))
 
     if rank == 0:
         line = {
@@ -495,10 +570,11 @@ def run_ours(args):
             "config": workload_config(args, int(st1["synapses"])),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
-                         "kernel": "k_run (persistent step kernel: LIF + scatter)",
+                         "kernel": ("k_step" if args.step_kernel == "split" else "k_run")
+                                   + " (persistent step kernel: LIF + scatter)",
                          "peak_source": peak_src,
                          "note": f"{BYTES_PER_EVENT} B x {pev} events over {launches} k_run launches "
-                                 f"({args.profile_steps} grid steps), {prof['step_kernel_ms']:.2f} ms of k_run "
+                                 f"({args.profile_steps} grid steps), {prof['step_kernel_ms']:.2f} ms of the step kernel "
                                  f"(CUDA events); Poisson-draw kernel {prof['drive_kernel_ms']:.2f} ms; "
                                  f"phase split of k_run (block 0): "
                                  + ", ".join(f"{k} {v / ph_tot:.0%}" for k, v in ph.items())},

@@ -175,16 +175,19 @@ NAER_API int naer_net_step(naer_net* net, uint64_t nsteps);
 
 /* No counterpart in the reference.  naer_net_step for a network compiled
  * with NAER_AGG_DETERMINISTIC (same kernels, same results), except that the
- * step's scratch comes from one fixed 32 MiB device array inside the library,
- * so the call never allocates or frees device memory.  It serves hosts that
- * own every byte of device memory through their own pool and must not see a
- * library call cudaMalloc (which also stalls the whole device) in the middle
- * of a run.
- * Limit: the network's worst-case step (all neurons spiking) must fit in the
- * array; a larger one gets NAER_E_OVERFLOW from the first call, before any
- * state changes.  NAER_E_STATE for an atomic-aggregation network.
- * The first call on a network looks up the array's device address and
- * partitions it; make that call before any stream capture begins.
+ * aggregation's scratch (8 bytes per padded synapse and 4 per ring cell)
+ * comes from one fixed 32 MiB device array inside the library instead of
+ * buffers the network allocates on its first deterministic step, so the
+ * call never allocates or frees device memory.  It serves hosts that own
+ * every byte of device memory through their own pool and must not see a
+ * library call cudaMalloc (which also stalls the whole device) in the
+ * middle of a run.
+ * Limit: that scratch must fit in the array; a larger network gets
+ * NAER_E_OVERFLOW from the call, before any state changes.  NAER_E_STATE
+ * for an atomic-aggregation network.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture begins.  Every call clears the parts of the
+ * array that must start empty.
  * One array exists per device, shared by all networks on it: calls whose
  * GPU work overlaps (networks on different streams or host threads) race on
  * it and must be serialized by the caller. */
@@ -306,8 +309,15 @@ typedef struct naer_tuning {
     uint32_t scatter_piece;   /* synapses per warp iteration: 128, 256, 0 = 128 for plastic networks else 256 */
     uint32_t neuron_state;    /* NAER_STATE_*: where the step kernel keeps membrane potentials and
                                  refractory counters during a launch */
-    uint32_t pad_;
+    uint32_t step_kernel;     /* NAER_KERNEL_*: which persistent step kernel runs */
 } naer_tuning;
+
+/* naer_tuning.step_kernel.  SPLIT: one contiguous spike list per step,
+ * delay-1 synapses delivered before the next LIF and the rest of each row
+ * while the grid waits at its barriers.  TWO_BARRIER: per-block spike
+ * regions, the whole scatter between two grid barriers.  Same results. */
+#define NAER_KERNEL_SPLIT 0u
+#define NAER_KERNEL_TWO_BARRIER 1u
 
 /* naer_tuning.neuron_state.  AUTO: shared memory when the installed chunks
  * fit it, else global memory.  SHARED: shared memory or NAER_E_INVALID.

@@ -111,11 +111,12 @@ class Tuning(C.Structure):
         ("trials", C.c_uint32),
         ("scatter_piece", C.c_uint32),
         ("neuron_state", C.c_uint32),
-        ("pad_", C.c_uint32),
+        ("step_kernel", C.c_uint32),
     ]
 
 
 STATE_AUTO, STATE_SHARED, STATE_GLOBAL = 0, 1, 2
+KERNEL_SPLIT, KERNEL_TWO_BARRIER = 0, 1
 
 
 class ServerParams(C.Structure):

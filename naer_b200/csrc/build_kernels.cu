@@ -264,20 +264,28 @@ __global__ void k_partition_d1(const uint64_t* row_ptr, const uint64_t* len, con
 
 // Row statistics of a built network: out[0] += sum of len[0..n) (synapses),
 // out[1] = max of padded[0..n) (longest padded row).
-__global__ void k_row_stats(const uint64_t* len, const uint64_t* padded, uint32_t n, unsigned long long* out) {
-    unsigned long long sum = 0, mx = 0;
+__global__ void k_row_stats(const uint64_t* len, const uint64_t* padded, const uint32_t* n1, uint32_t n,
+                            unsigned long long* out) {
+    unsigned long long sum = 0, mx = 0, mx1 = 0, mx2 = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         sum += len[i];
         mx = max(mx, (unsigned long long)padded[i]);
+        const unsigned long long p1 = (n1[i] + kRowAlign - 1) / kRowAlign * kRowAlign;
+        mx1 = max(mx1, p1);
+        mx2 = max(mx2, (unsigned long long)padded[i] - p1);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
         mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+        mx1 = max(mx1, __shfl_xor_sync(0xFFFFFFFFu, mx1, o));
+        mx2 = max(mx2, __shfl_xor_sync(0xFFFFFFFFu, mx2, o));
     }
     if ((threadIdx.x & 31u) == 0) {
         if (sum) atomicAdd(out, sum);
         if (mx) atomicMax(out + 1, mx);
+        if (mx1) atomicMax(out + 3, mx1);
+        if (mx2) atomicMax(out + 4, mx2);
     }
 }
 

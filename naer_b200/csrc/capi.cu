@@ -508,6 +508,7 @@ static void fill_tuning(naer_tuning* out, const naer::Tuning& t, uint32_t graph_
     out->scatter_split = t.scatter_split;
     out->scatter_piece = t.scatter_piece;
     out->neuron_state = t.neuron_state;
+    out->step_kernel = t.step_kernel;
     out->graph_launches = graph_launches;
 }
 
@@ -547,6 +548,7 @@ int naer_net_set_tuning(naer_net* net, const naer_tuning* tuning) {
         t.scatter_split = tuning->scatter_split;
         t.scatter_piece = tuning->scatter_piece;
         t.neuron_state = tuning->neuron_state;
+        t.step_kernel = tuning->step_kernel;
         net->eng->set_tuning(t);
     });
 }
@@ -569,6 +571,7 @@ int naer_batch_set_tuning(naer_batch* batch, const naer_tuning* tuning) {
         t.scatter_split = tuning->scatter_split;
         t.scatter_piece = tuning->scatter_piece;
         t.neuron_state = tuning->neuron_state;
+        t.step_kernel = tuning->step_kernel;
         batch->b->engine().set_tuning(t);
         batch->graph_launches = tuning->graph_launches;
     });

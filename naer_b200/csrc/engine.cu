@@ -1,6 +1,8 @@
 // Host engine implementation.
 #include <cub/cub.cuh>
 
+#include <mutex>
+
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
@@ -40,6 +42,12 @@ __global__ void k_u32_to_u64(const uint32_t* in, uint32_t n, uint64_t* out) {
 }
 
 uint32_t round_up4(uint32_t x) { return (x + 3u) & ~3u; }
+
+// deterministic-aggregation scratch of a net: padded synapse entries, ring cells
+uint64_t det_syn_entries(const NetHost& n) {
+    return std::max<uint64_t>(n.syn_capacity ? n.syn_capacity : n.synapses_padded, 4);
+}
+uint64_t det_cells(const NetHost& n) { return (uint64_t)n.ring_slots * n.n_storage; }
 
 uint32_t bit_width(uint64_t x) {
     uint32_t b = 0;
@@ -131,18 +139,8 @@ Engine::~Engine() {
     }
     f(d_ev_part_);
     f(d_ovf_part_);
-    f(det_prefix_);
     f(d_raster_);
     for (auto ev : timer_events_) cudaEventDestroy(ev);
-    for (int i = 0; i < 2; ++i) {
-        f(q_keys_[i]);
-        f(q_vals_[i]);
-        f(e_keys_[i]);
-        f(e_vals_[i]);
-    }
-    f(q_sizes_);
-    f(q_offs_);
-    f(cub_tmp_);
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (h_pinned_) cudaFreeHost(h_pinned_);
     cudaStreamDestroy(stream_);
@@ -238,21 +236,25 @@ uint32_t lif_chunks(const NetHost& description) {
     return (uint32_t)std::min<uint64_t>(c, 0xFFFFFFFFu);
 }
 
-uint32_t Engine::fast_chunk_capacity() {
+uint32_t Engine::fast_chunk_capacity(uint32_t aggregation) {
     DeviceGuard g(device_);
     int optin = 0;
     NAER_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+    const bool det = aggregation == NAER_AGG_DETERMINISTIC;
+    const bool split = det || tuning_.step_kernel == NAER_KERNEL_SPLIT;
+    const void* kern = det ? (const void*)k_det_step<true>
+                           : split ? (const void*)k_step<true> : (const void*)k_run<true>;
     cudaFuncAttributes fa{};
-    NAER_CK(cudaFuncGetAttributes(&fa, k_run<true>));
+    NAER_CK(cudaFuncGetAttributes(&fa, kern));
     optin -= (int)fa.sharedSizeBytes;
-    NAER_CK(cudaFuncSetAttribute(k_run<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    NAER_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     const int bps_hi = tuning_.blocks_per_sm ? (int)std::min<uint32_t>(tuning_.blocks_per_sm, 4) : 4;
     auto fits = [&](int bps, uint32_t own) {
         const uint32_t grid = (uint32_t)bps * (uint32_t)sm_count_;
-        const size_t smem = run_smem_bytes(grid, own, true);
+        const size_t smem = split ? step_smem_bytes(own, true) : run_smem_bytes(grid, own, true);
         if (smem > (size_t)optin) return false;
         int occ = 0;
-        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_run<true>, kLifThreads, smem));
+        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLifThreads, smem));
         return occ >= bps;
     };
     for (int bps = bps_hi; bps >= 1; --bps) {
@@ -463,9 +465,9 @@ void Engine::build(NetHost& n) {
         NAER_CK(cudaGetLastError());
         // synapse count, longest padded row and the final padded size, read
         // back with the build's one synchronisation (below)
-        stats = static_cast<unsigned long long*>(dalloc(3 * 8ull));
-        NAER_CK(cudaMemsetAsync(stats, 0, 3 * 8ull, st));
-        k_row_stats<<<grid_for(Ns, T, maxb), T, 0, st>>>(len, padded2, Ns, stats);
+        stats = static_cast<unsigned long long*>(dalloc(5 * 8ull));
+        NAER_CK(cudaMemsetAsync(stats, 0, 5 * 8ull, st));
+        k_row_stats<<<grid_for(Ns, T, maxb), T, 0, st>>>(len, padded2, n1, Ns, stats);
         NAER_CK(cudaMemcpyAsync(stats + 2, row_ptr2 + Ns, 8, cudaMemcpyDeviceToDevice, st));
         NAER_CK(cudaGetLastError());
         dfree(n.tgt, std::max<uint64_t>(S, 4) * 4ull);
@@ -527,13 +529,15 @@ void Engine::build(NetHost& n) {
         NAER_CK(cudaMemcpyAsync(n.e_plus, ep.data(), n.e_len * 4ull, cudaMemcpyHostToDevice, st));
         NAER_CK(cudaMemcpyAsync(n.e_minus, em.data(), n.e_len * 4ull, cudaMemcpyHostToDevice, st));
     }
-    unsigned long long hstats[3] = {0, 0, 0};
+    unsigned long long hstats[5] = {0, 0, 0, 0, 0};
     NAER_CK(cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, st));
-    dfree(stats, 3 * 8ull);
+    dfree(stats, 5 * 8ull);
     NAER_CK(cudaStreamSynchronize(st));
     n.synapses = hstats[0];
     n.max_row_padded = hstats[1];
     n.synapses_padded = hstats[2];
+    n.max_first_padded = hstats[3];
+    n.max_rest_padded = hstats[4];
 
     NetDev& d = n.dev;
     d = NetDev{};
@@ -588,6 +592,14 @@ void Engine::free_net(NetHost& n) {
     dfree(n.pre, Np * 8ull);
     dfree(n.e_plus, n.e_len * 4ull);
     dfree(n.e_minus, n.e_len * 4ull);
+    if (n.det_w) {
+        dfree(n.det_w, det_syn_entries(n) * 4ull);
+        dfree(n.det_next, det_syn_entries(n) * 4ull);
+        dfree(n.det_head, det_cells(n) * 4ull);
+        n.det_w = nullptr;
+        n.det_next = nullptr;
+        n.det_head = nullptr;
+    }
     n.v = nullptr;
     n.refr = nullptr;
     n.ring = nullptr;
@@ -609,9 +621,6 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     DeviceGuard g(device_);
     NAER_CK(cudaStreamSynchronize(stream_));
     drop_graph();
-    // the fixed-scratch partition was cut for the previous geometry: the
-    // next fixed-scratch call repartitions and re-checks the fit
-    fs_.ready = false;
     nets_ = nets;
     aggregation_ = aggregation;
     inst_raster_cap_ = raster_capacity;
@@ -696,22 +705,33 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     // resident).  Prefer the variant that keeps neuron state in shared
     // memory, with as many blocks per SM as its footprint allows; the
     // deterministic path's LIF uses the same queue regions.
+    const bool det = aggregation == NAER_AGG_DETERMINISTIC;
+    split_kernel_ = !det && tuning_.step_kernel == NAER_KERNEL_SPLIT;
+    const bool list_kernel = det || split_kernel_;  // one contiguous spike list per step
+    const void* kern_smem = det ? (const void*)k_det_step<true>
+                                : split_kernel_ ? (const void*)k_step<true> : (const void*)k_run<true>;
+    const void* kern_glob = det ? (const void*)k_det_step<false>
+                                : split_kernel_ ? (const void*)k_step<false> : (const void*)k_run<false>;
+    auto smem_of = [&](uint32_t grid, uint32_t own, bool state) {
+        return list_kernel ? step_smem_bytes(own, state) : run_smem_bytes(grid, own, state);
+    };
+    det_scratch_ = kScratchNone;  // the next deterministic call points the new tables at its scratch
     int dev_smem_optin = 0;
     NAER_CK(cudaDeviceGetAttribute(&dev_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
     cudaFuncAttributes fa{};
-    NAER_CK(cudaFuncGetAttributes(&fa, k_run<true>));
+    NAER_CK(cudaFuncGetAttributes(&fa, kern_smem));
     dev_smem_optin -= (int)fa.sharedSizeBytes;
-    NAER_CK(cudaFuncSetAttribute(k_run<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_smem_optin));
+    NAER_CK(cudaFuncSetAttribute(kern_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_smem_optin));
     use_smem_state_ = false;
     lif_grid_ = 0;
     const int bps_hi = tuning_.blocks_per_sm ? (int)std::min<uint32_t>(tuning_.blocks_per_sm, 4) : 4;
     for (int bps = bps_hi; bps >= 1 && !use_smem_state_ && tuning_.neuron_state != NAER_STATE_GLOBAL; --bps) {
         const uint32_t grid = (uint32_t)bps * sm_count_;
         const uint32_t own = std::max<uint32_t>(1, (eng_.n_chunks + grid - 1) / grid);
-        const size_t smem = run_smem_bytes(grid, own, true);
+        const size_t smem = smem_of(grid, own, true);
         if (smem > (size_t)dev_smem_optin) continue;
         int occ = 0;
-        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_run<true>, kLifThreads, smem));
+        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern_smem, kLifThreads, smem));
         if (occ >= bps) {
             use_smem_state_ = true;
             lif_grid_ = grid;
@@ -722,11 +742,11 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
         throw Error(NAER_E_INVALID, "neuron state does not fit shared memory at this geometry");
     if (!use_smem_state_) {
         int occ = 0;
-        const size_t smem_bound = run_smem_bytes((uint32_t)sm_count_ * 4, 1, false);
-        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_run<false>, kLifThreads, smem_bound));
+        const size_t smem_bound = smem_of((uint32_t)sm_count_ * 4, 1, false);
+        NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern_glob, kLifThreads, smem_bound));
         if (occ < 1) throw Error(NAER_E_CUDA, "the step kernel cannot be resident on this device");
         lif_grid_ = (uint32_t)std::min(occ, bps_hi) * sm_count_;
-        scatter_smem_ = run_smem_bytes(lif_grid_, 1, false);
+        scatter_smem_ = smem_of(lif_grid_, 1, false);
     }
     scatter_grid_ = lif_grid_;
     const uint32_t chunks_per_block = (eng_.n_chunks + lif_grid_ - 1) / lif_grid_;
@@ -737,7 +757,9 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
         events_base_ += sum_parts(d_ev_part_, ev_part_n_);
         overflow_base_ += sum_parts(d_ovf_part_, ev_part_n_);
     }
-    const uint64_t qentries = (uint64_t)lif_grid_ * region_cap;
+    // per-block regions (k_run, deterministic LIF) or one list of every
+    // neuron at most (k_step)
+    const uint64_t qentries = std::max<uint64_t>((uint64_t)lif_grid_ * region_cap, qcap);
     if (qentries > 0xFFFFFFFFull) throw Error(NAER_E_OVERFLOW, "spike queue larger than 2^32 entries");
     for (int i = 0; i < 2; ++i) {
         regrow(reinterpret_cast<void*&>(d_queue_[i]), queue_bytes_[i], qentries * sizeof(SpikeRec));
@@ -787,6 +809,24 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     const uint32_t psz = eng_.scatter_piece;
     eng_.scatter_split = (uint32_t)std::min<uint64_t>(any_stdp ? 32 : 16, std::max<uint64_t>(1, (max_row + psz - 1) / psz));
     if (tuning_.scatter_split) eng_.scatter_split = std::min<uint32_t>(tuning_.scatter_split, 64);
+    // k_step: the part delivered before the next LIF (delay-1 synapses;
+    // whole rows of plastic sources) and the deferred rest
+    uint64_t max_first = 0, max_rest = 0;
+    for (NetHost* n : nets) {
+        if (n->dev.stdp_on) {
+            max_first = std::max<uint64_t>(max_first, n->max_row_padded);
+        } else {
+            max_first = std::max<uint64_t>(max_first, n->max_first_padded);
+            max_rest = std::max<uint64_t>(max_rest, n->max_rest_padded);
+        }
+    }
+    const uint64_t cap_split = any_stdp ? 32 : 16;
+    eng_.split_first = (uint32_t)std::min<uint64_t>(cap_split, std::max<uint64_t>(1, (max_first + psz - 1) / psz));
+    eng_.split_rest = (uint32_t)std::min<uint64_t>(cap_split, std::max<uint64_t>(1, (max_rest + psz - 1) / psz));
+    if (tuning_.scatter_split) eng_.split_first = eng_.split_rest = std::min<uint32_t>(tuning_.scatter_split, 64);
+    eng_.queue_cap = (uint32_t)qentries;
+    if (qentries * std::max(eng_.split_first, eng_.split_rest) > 0xFFFFFFFFull)
+        throw Error(NAER_E_OVERFLOW, "spike list times warps per spike exceeds 2^32 work items");
     NAER_CK(cudaStreamSynchronize(stream_));  // tables and buffers complete for every stream
 }
 
@@ -798,6 +838,7 @@ void Engine::set_tuning(const Tuning& t) {
     if (v.scatter_piece != 0 && v.scatter_piece != 128 && v.scatter_piece != kScatterPiece)
         throw Error(NAER_E_INVALID, "scatter_piece must be 0, 128 or 256");
     if (v.neuron_state > NAER_STATE_GLOBAL) throw Error(NAER_E_INVALID, "unknown neuron_state");
+    if (v.step_kernel > NAER_KERNEL_TWO_BARRIER) throw Error(NAER_E_INVALID, "unknown step_kernel");
     tuning_ = v;
     if (!nets_.empty()) install(std::vector<NetHost*>(nets_), inst_raster_cap_, inst_record_, aggregation_);
 }
@@ -806,7 +847,7 @@ TuneResult Engine::autotune(uint32_t trial_steps) {
     if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
     TuneResult r;
     r.best = tuning_;
-    if (aggregation_ == NAER_AGG_DETERMINISTIC || trial_steps == 0) return r;
+    if (trial_steps == 0) return r;
     DeviceGuard g(device_);
     cudaEvent_t e0, e1;
     NAER_CK(cudaEventCreate(&e0));
@@ -842,6 +883,8 @@ TuneResult Engine::autotune(uint32_t trial_steps) {
                     if (bps == 0 && L == kDriveSlots && sp == 0) {
                         t.scatter_piece = eng_piece_default == 128 ? kScatterPiece : 128u;
                     }
+                    if (bps == 1 && L == kDriveSlots && sp == 0 && aggregation_ != NAER_AGG_DETERMINISTIC)
+                        t.step_kernel = NAER_KERNEL_TWO_BARRIER;
                     const double us = trial(t);
                     if (us < r.best_us_per_step) {
                         r.best_us_per_step = us;
@@ -910,7 +953,8 @@ void Engine::launch_run(uint32_t steps) { launch_run_ex(steps, false); }
 // of cudaLaunchKernelEx keeps it capturable.
 void Engine::launch_run_ex(uint32_t steps, bool from_ctl) {
     unsigned long long s0 = from_ctl ? kStepFromCtl : host_step_;
-    NAER_CK(cudaMemsetAsync(&d_ctl_->bar_arrive, 0, sizeof(unsigned long long), stream_));
+    static_assert(offsetof(Ctl, qtail) == offsetof(Ctl, bar_arrive) + 8, "Ctl layout");
+    NAER_CK(cudaMemsetAsync(&d_ctl_->bar_arrive, 0, 8 + sizeof(d_ctl_->qtail), stream_));
     const bool timed = profiling_ && !from_ctl;
     if (timed) NAER_CK(cudaEventRecord(timer_event(), stream_));
     cudaLaunchConfig_t cfg{};
@@ -923,10 +967,22 @@ void Engine::launch_run_ex(uint32_t steps, bool from_ctl) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (use_smem_state_)
-        NAER_CK(cudaLaunchKernelEx(&cfg, k_run<true>, eng_, s0, steps));
-    else
-        NAER_CK(cudaLaunchKernelEx(&cfg, k_run<false>, eng_, s0, steps));
+    if (aggregation_ == NAER_AGG_DETERMINISTIC) {
+        if (use_smem_state_)
+            NAER_CK(cudaLaunchKernelEx(&cfg, k_det_step<true>, eng_, s0, steps));
+        else
+            NAER_CK(cudaLaunchKernelEx(&cfg, k_det_step<false>, eng_, s0, steps));
+    } else if (split_kernel_) {
+        if (use_smem_state_)
+            NAER_CK(cudaLaunchKernelEx(&cfg, k_step<true>, eng_, s0, steps));
+        else
+            NAER_CK(cudaLaunchKernelEx(&cfg, k_step<false>, eng_, s0, steps));
+    } else {
+        if (use_smem_state_)
+            NAER_CK(cudaLaunchKernelEx(&cfg, k_run<true>, eng_, s0, steps));
+        else
+            NAER_CK(cudaLaunchKernelEx(&cfg, k_run<false>, eng_, s0, steps));
+    }
     if (timed) {
         NAER_CK(cudaEventRecord(timer_event(), stream_));
         timer_kinds_.push_back(1);
@@ -990,10 +1046,11 @@ void Engine::run(uint64_t nsteps) {
     DeviceGuard g(device_);
     if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
     check_usable();
-    if (aggregation_ == NAER_AGG_DETERMINISTIC) {
-        for (uint64_t i = 0; i < nsteps; ++i) run_deterministic_step();
-        return;
-    }
+    if (aggregation_ == NAER_AGG_DETERMINISTIC) ensure_det_scratch();
+    run_launches(nsteps);
+}
+
+void Engine::run_launches(uint64_t nsteps) {
     // Poisson counts of a chunk of steps are drawn first (full occupancy),
     // then the persistent kernel simulates the chunk
     while (nsteps > 0) {
@@ -1009,10 +1066,11 @@ uint64_t Engine::run_graph(uint64_t nsteps, uint32_t graph_launches) {
     DeviceGuard g(device_);
     if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
     check_usable();
-    if (aggregation_ == NAER_AGG_DETERMINISTIC || graph_launches == 0) {
+    if (graph_launches == 0) {
         run(nsteps);
         return 0;
     }
+    if (aggregation_ == NAER_AGG_DETERMINISTIC) ensure_det_scratch();
     const uint32_t L = tuning_.launch_steps;
     const uint64_t per = (uint64_t)L * graph_launches;
     if (graph_exec_ && graph_launches_ != graph_launches) drop_graph();
@@ -1050,266 +1108,120 @@ uint64_t Engine::run_graph(uint64_t nsteps, uint32_t graph_launches) {
     return done;
 }
 
-void Engine::ensure_det_capacity(uint64_t events) {
-    // Every buffer is checked against the geometry installed now: install()
-    // may have raised the queue capacity or the LIF grid since the buffers
-    // were sized (the served form reinstalls on every change of its set).
-    const uint64_t q = std::max<uint32_t>(queue_cap_, 1);
-    const uint64_t pre = (uint64_t)lif_grid_ + 1;
-    if (events <= e_cap_ && q <= q_cap_alloc_ && pre <= det_prefix_cap_) return;
-    if (events > e_cap_) {
-        uint64_t cap = std::max<uint64_t>(events, 1 << 16);
-        if (cap < e_cap_ * 2 && e_cap_) cap = e_cap_ * 2;
-        for (int i = 0; i < 2; ++i) {
-            if (e_keys_[i]) dfree(e_keys_[i], e_cap_ * 8ull);
-            if (e_vals_[i]) dfree(e_vals_[i], e_cap_ * 4ull);
-            e_keys_[i] = static_cast<unsigned long long*>(dalloc(cap * 8ull));
-            e_vals_[i] = static_cast<float*>(dalloc(cap * 4ull));
+// ---------------------------------------------------------------------------
+// Deterministic aggregation scratch (k_det_step): per net, the weight and the
+// next event of every padded synapse (8 B per synapse) and the list head of
+// every ring cell (4 B per cell, empty between steps).  The plain step keeps
+// it in buffers each network owns, allocated by its first deterministic
+// step; the fixed-scratch step carves it from one fixed device array.
+
+void Engine::point_det_scratch(uint32_t mode) {
+    for (size_t i = 0; i < nets_.size(); ++i) {
+        const NetHost& n = *nets_[i];
+        h_nets_[i].ev_w = n.det_w;
+        h_nets_[i].ev_next = n.det_next;
+        h_nets_[i].cell_head = n.det_head;
+        if (mode == kScratchArena) {
+            h_nets_[i].ev_w = arena_w_[i];
+            h_nets_[i].ev_next = arena_next_[i];
+            h_nets_[i].cell_head = arena_head_[i];
         }
-        e_cap_ = cap;
     }
-    if (q > q_cap_alloc_) {
-        for (int i = 0; i < 2; ++i) {
-            if (q_keys_[i]) dfree(q_keys_[i], q_cap_alloc_ * 8ull);
-            if (q_vals_[i]) dfree(q_vals_[i], q_cap_alloc_ * 4ull);
-            q_keys_[i] = static_cast<unsigned long long*>(dalloc(q * 8ull));
-            q_vals_[i] = static_cast<uint32_t*>(dalloc(q * 4ull));
-        }
-        if (q_sizes_) dfree(q_sizes_, q_cap_alloc_ * 4ull);
-        if (q_offs_) dfree(q_offs_, q_cap_alloc_ * 4ull);
-        q_sizes_ = static_cast<uint32_t*>(dalloc(q * 4ull));
-        q_offs_ = static_cast<uint32_t*>(dalloc(q * 4ull));
-        q_cap_alloc_ = q;
-    }
-    if (pre > det_prefix_cap_) {
-        if (det_prefix_) dfree(det_prefix_, det_prefix_cap_ * sizeof(uint32_t));
-        det_prefix_ = static_cast<uint32_t*>(dalloc(pre * sizeof(uint32_t)));
-        det_prefix_cap_ = pre;
-    }
-    const uint64_t cap = e_cap_;
-    // CUB scratch large enough for every sort/scan of this capacity
-    size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
-    const int qn = (int)std::max<uint32_t>(queue_cap_, 1);
-    NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b1, q_keys_[0], q_keys_[1], q_vals_[0], q_vals_[1],
-                                            qn, 0, 64, stream_));
-    NAER_CK(cub::DeviceScan::ExclusiveSum(nullptr, b2, q_sizes_, q_offs_, qn, stream_));
-    NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b3, e_keys_[0], e_keys_[1], e_vals_[0], e_vals_[1],
-                                            (int)std::min<uint64_t>(cap, 0x7FFFFFFF), 0, 64, stream_));
-    NAER_CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, d_counts_[0], det_prefix_, (int)(lif_grid_ + 1), stream_));
-    const size_t need = std::max({b1, b2, b3, b4});
-    if (need > cub_tmp_bytes_) {
-        if (cub_tmp_) dfree(cub_tmp_, cub_tmp_bytes_);
-        cub_tmp_ = dalloc(need);
-        cub_tmp_bytes_ = need;
-    }
+    NAER_CK(cudaMemcpyAsync(d_nets_, h_nets_.data(), h_nets_.size() * sizeof(NetDev), cudaMemcpyHostToDevice,
+                            stream_));
+    NAER_CK(cudaStreamSynchronize(stream_));  // h_nets_ is pageable host memory
+    det_scratch_ = mode;
 }
 
-void Engine::run_deterministic_step() {
-    cudaStream_t st = stream_;
-    uint64_t own_launches = 2;  // LIF, advance (launch_drive counts itself)
-    ensure_det_capacity(1);  // buffers follow the installed geometry
-    const uint32_t T = 256;
-    launch_drive(host_step_, 1);
-    k_lif<<<lif_grid_, kLifThreads, 0, st>>>(eng_);
-    const uint32_t qb = (uint32_t)(host_step_ & 1ull);
-    size_t b = cub_tmp_bytes_;
-    NAER_CK(cub::DeviceScan::ExclusiveSum(cub_tmp_, b, d_counts_[qb], det_prefix_, (int)(lif_grid_ + 1), st));
-    NAER_CK(cudaMemcpyAsync(h_pinned_, det_prefix_ + lif_grid_, 4, cudaMemcpyDeviceToHost, st));
-    NAER_CK(cudaStreamSynchronize(st));
-    const uint32_t Q = h_pinned_[0];
-    if (Q > 0) {
-        k_det_queue_keys<<<(Q + T - 1) / T, T, 0, st>>>(eng_, det_prefix_, q_keys_[0], q_vals_[0], Q);
-        b = cub_tmp_bytes_;
-        const int qbits = 32 + (int)bit_width(std::max<uint32_t>(eng_.n_nets, 1));
-        NAER_CK(cub::DeviceRadixSort::SortPairs(cub_tmp_, b, q_keys_[0], q_keys_[1], q_vals_[0], q_vals_[1],
-                                                (int)Q, 0, std::min(qbits, 64), st));
-        own_launches += 3;  // queue keys, row sizes, raster
-        k_det_row_sizes<<<(Q + T - 1) / T, T, 0, st>>>(eng_, q_vals_[1], Q, q_sizes_);
-        b = cub_tmp_bytes_;
-        NAER_CK(cub::DeviceScan::ExclusiveSum(cub_tmp_, b, q_sizes_, q_offs_, (int)Q, st));
-        NAER_CK(cudaMemcpyAsync(h_pinned_, q_offs_ + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
-        NAER_CK(cudaMemcpyAsync(h_pinned_ + 1, q_sizes_ + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
-        NAER_CK(cudaStreamSynchronize(st));
-        const uint64_t E = (uint64_t)h_pinned_[0] + h_pinned_[1];
-        if (E > 0x7FFFFFFFull) throw Error(NAER_E_OVERFLOW, "more than 2^31 events in one step");
-        if (Q > q_cap_alloc_) throw Error(NAER_E_OVERFLOW, "spike count exceeds the sorted queue");
-        k_det_raster<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + T - 1) / T, 1024)), T, 0, st>>>(eng_, q_vals_[1], Q);
-        if (E > 0) {
-            own_launches += 2;  // emit, fold
-            ensure_det_capacity(E);
-            k_det_emit<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + 7) / 8, (uint32_t)sm_count_ * 8)),
-                         kScatterThreads, 0, st>>>(eng_, q_vals_[1], Q, q_offs_, e_keys_[0], e_vals_[0]);
-            b = cub_tmp_bytes_;
-            const int ebits = std::max<int>(1, (int)bit_width(total_ring_cells_));
-            NAER_CK(cub::DeviceRadixSort::SortPairs(cub_tmp_, b, e_keys_[0], e_keys_[1], e_vals_[0],
-                                                    e_vals_[1], (int)E, 0, ebits, st));
-            k_det_fold<<<(uint32_t)((E + T - 1) / T), T, 0, st>>>(d_nets_, eng_.n_nets, e_keys_[1],
-                                                                  e_vals_[1], (uint32_t)E);
-        }
-    } else {
-        ++own_launches;
-        k_det_raster<<<1, 32, 0, st>>>(eng_, nullptr, 0);
+void Engine::ensure_det_scratch() {
+    if (det_scratch_ == kScratchOwn) return;
+    for (NetHost* n : nets_) {
+        if (det_syn_entries(*n) >= kNoEvent || det_cells(*n) >= 0xFFFFFFFFull)
+            throw Error(NAER_E_OVERFLOW, "deterministic aggregation needs fewer than 2^32 synapses and ring cells per "
+                                         "network");
+        if (n->det_w) continue;
+        n->det_w = static_cast<float*>(dalloc(det_syn_entries(*n) * 4ull));
+        n->det_next = static_cast<uint32_t*>(dalloc(det_syn_entries(*n) * 4ull));
+        n->det_head = static_cast<uint32_t*>(dalloc(det_cells(*n) * 4ull));
+        NAER_CK(cudaMemsetAsync(n->det_head, 0xFF, det_cells(*n) * 4ull, stream_));
+        n->device_bytes += det_syn_entries(*n) * 8ull + det_cells(*n) * 4ull;
     }
-    k_advance<<<1, 32, 0, st>>>(eng_);
-    NAER_CK(cudaGetLastError());
-    launches_ += own_launches;
-    ++host_step_;
+    point_det_scratch(kScratchOwn);
 }
 
 // ---------------------------------------------------------------------------
-// Deterministic steps with no allocation.  The aggregation's scratch (queue
-// sort, row-size scan, event sort and the CUB temporary storage) is carved
-// from one fixed device array of this library instead of engine-owned
-// buffers that grow with the step's event count.  Its size bounds the
-// networks the call accepts: the worst case of a step (every neuron spiking,
-// so every padded synapse emitting one event) must fit.  One array exists
-// per device and is shared by every engine on that device.
+// Deterministic steps with no allocation (naer_net_step_noalloc).  The
+// scratch above is carved from one fixed device array of this library
+// instead of buffers the network allocates.  Its size bounds the networks
+// the call accepts.  One array exists per device and is shared by every
+// engine on that device: calls whose GPU work overlaps race on it.
 
 constexpr size_t kFixedScratchBytes = 32ull << 20;  // 32 MiB
 static __device__ __align__(256) unsigned char g_fixed_scratch[kFixedScratchBytes];
 
 namespace {
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-}  // namespace
 
-// Looks up this device's copy of the arena and partitions it for the
-// installed networks.  Rejects a network whose worst-case step does not fit
-// before any of its state changes.
-void Engine::fixed_scratch_setup() {
-    if (aggregation_ != NAER_AGG_DETERMINISTIC)
-        throw Error(NAER_E_STATE, "the fixed-scratch step needs a network compiled with deterministic aggregation");
-    uint64_t neurons = 0, events = 0;
-    for (const NetHost* n : nets_) {
-        neurons += n->n_storage;
-        events += n->synapses_padded;
+// Device address of this device's copy of the array, looked up once per
+// device with that device current (a host-side reference to the array is
+// not a device address).
+unsigned char* fixed_scratch_base(int device) {
+    static std::mutex mu;
+    static std::vector<unsigned char*> base;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)base.size() <= device) base.resize(device + 1, nullptr);
+    if (!base[device]) {
+        void* p = nullptr;
+        NAER_CK(cudaGetSymbolAddress(&p, g_fixed_scratch));
+        base[device] = static_cast<unsigned char*>(p);
     }
-    FixedScratch f;
-    f.q_max = std::max<uint64_t>(1, std::min<uint64_t>(queue_cap_, neurons));
-    f.e_max = std::max<uint64_t>(1, events);
-    f.q_bits = std::min(64, 32 + (int)bit_width(std::max<uint32_t>(eng_.n_nets, 1)));
-    f.e_bits = std::max<int>(1, (int)bit_width(total_ring_cells_));
-    if (f.e_max > 0x7FFFFFFFull)
-        throw Error(NAER_E_OVERFLOW, "network exceeds the fixed scratch: more than 2^31 padded synapses");
-    // partition sizes first, addresses after the fit is known
-    const size_t sizes[11] = {
-        (lif_grid_ + 1) * sizeof(uint32_t),
-        f.q_max * 8, f.q_max * 8, f.q_max * 4, f.q_max * 4, f.q_max * 4, f.q_max * 4,
-        f.e_max * 8, f.e_max * 8, f.e_max * 4, f.e_max * 4};
-    size_t offs[11], used = 0;
-    for (int i = 0; i < 11; ++i) {
-        offs[i] = used;
-        used = align256(used + sizes[i]);
-    }
-    // CUB temporary storage of the four operations (double-buffer sorts:
-    // the sorted copies live in the partitions above)
-    size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
-    {
-        cub::DoubleBuffer<unsigned long long> qk(nullptr, nullptr);
-        cub::DoubleBuffer<uint32_t> qv(nullptr, nullptr);
-        cub::DoubleBuffer<unsigned long long> ek(nullptr, nullptr);
-        cub::DoubleBuffer<float> ev(nullptr, nullptr);
-        NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b1, qk, qv, (int)f.q_max, 0, f.q_bits, stream_));
-        NAER_CK(cub::DeviceScan::ExclusiveSum(nullptr, b2, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                              (int)f.q_max, stream_));
-        NAER_CK(cub::DeviceRadixSort::SortPairs(nullptr, b3, ek, ev, (int)f.e_max, 0, f.e_bits, stream_));
-        NAER_CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                              (int)(lif_grid_ + 1), stream_));
-    }
-    f.tmp_bytes = std::max({b1, b2, b3, b4});
-    const size_t need = used + f.tmp_bytes;
-    if (need > kFixedScratchBytes)
-        throw Error(NAER_E_OVERFLOW,
-                    "network too large for the fixed-scratch step: its worst-case step (" + std::to_string(neurons) +
-                        " neurons, " + std::to_string(events) + " padded synapses) needs " +
-                        std::to_string(need) + " bytes of scratch; the fixed arena holds " +
-                        std::to_string(kFixedScratchBytes) + " bytes");
-    void* base = nullptr;
-    NAER_CK(cudaGetSymbolAddress(&base, g_fixed_scratch));
-    unsigned char* a = static_cast<unsigned char*>(base);
-    f.prefix = reinterpret_cast<uint32_t*>(a + offs[0]);
-    f.q_keys[0] = reinterpret_cast<unsigned long long*>(a + offs[1]);
-    f.q_keys[1] = reinterpret_cast<unsigned long long*>(a + offs[2]);
-    f.q_vals[0] = reinterpret_cast<uint32_t*>(a + offs[3]);
-    f.q_vals[1] = reinterpret_cast<uint32_t*>(a + offs[4]);
-    f.q_sizes = reinterpret_cast<uint32_t*>(a + offs[5]);
-    f.q_offs = reinterpret_cast<uint32_t*>(a + offs[6]);
-    f.e_keys[0] = reinterpret_cast<unsigned long long*>(a + offs[7]);
-    f.e_keys[1] = reinterpret_cast<unsigned long long*>(a + offs[8]);
-    f.e_vals[0] = reinterpret_cast<float*>(a + offs[9]);
-    f.e_vals[1] = reinterpret_cast<float*>(a + offs[10]);
-    f.tmp = a + used;
-    // No partition has to start at zero: every word a step reads was
-    // written earlier in the same step.
-    f.ready = true;
-    fs_ = f;
+    return base[device];
 }
+}  // namespace
 
 void Engine::run_fixed_scratch(uint64_t nsteps) {
     DeviceGuard g(device_);
     if (nets_.empty()) throw Error(NAER_E_STATE, "no network installed");
     check_usable();
-    if (!fs_.ready) fixed_scratch_setup();
-    for (uint64_t i = 0; i < nsteps; ++i) run_fixed_scratch_step();
-}
-
-// The deterministic step of run_deterministic_step with the fixed arena's
-// partitions as scratch: same kernels, same order, same results.
-void Engine::run_fixed_scratch_step() {
-    cudaStream_t st = stream_;
-    uint64_t own_launches = 3;  // drive, LIF, advance
-    const FixedScratch& f = fs_;
-    const uint32_t T = 256;
-    const uint32_t dgrid = std::max<uint32_t>(1, std::min<uint32_t>(eng_.n_chunks, (uint32_t)sm_count_ * 16));
-    k_drive<<<dgrid, kLifThreads, 0, st>>>(eng_, (unsigned long long)host_step_, 1u);
-    k_lif<<<lif_grid_, kLifThreads, 0, st>>>(eng_);
-    const uint32_t qb = (uint32_t)(host_step_ & 1ull);
-    size_t b = f.tmp_bytes;
-    NAER_CK(cub::DeviceScan::ExclusiveSum(f.tmp, b, d_counts_[qb], f.prefix, (int)(lif_grid_ + 1), st));
-    NAER_CK(cudaMemcpyAsync(h_pinned_, f.prefix + lif_grid_, 4, cudaMemcpyDeviceToHost, st));
-    NAER_CK(cudaStreamSynchronize(st));
-    const uint32_t Q = h_pinned_[0];
-    // q_max covers every neuron and e_max every padded synapse, so neither
-    // check below can fire while the partition matches the installed
-    // geometry (install() invalidates it); they guard that invariant.  If
-    // one fired, the LIF of this step would already have run: the network's
-    // state would be undefined.
-    if (Q > f.q_max) throw Error(NAER_E_OVERFLOW, "internal: spike count exceeds the fixed scratch partition");
-    if (Q > 0) {
-        k_det_queue_keys<<<(Q + T - 1) / T, T, 0, st>>>(eng_, f.prefix, f.q_keys[0], f.q_vals[0], Q);
-        cub::DoubleBuffer<unsigned long long> qk(f.q_keys[0], f.q_keys[1]);
-        cub::DoubleBuffer<uint32_t> qv(f.q_vals[0], f.q_vals[1]);
-        b = f.tmp_bytes;
-        NAER_CK(cub::DeviceRadixSort::SortPairs(f.tmp, b, qk, qv, (int)Q, 0, f.q_bits, st));
-        const uint32_t* order = qv.Current();
-        own_launches += 3;  // queue keys, row sizes, raster
-        k_det_row_sizes<<<(Q + T - 1) / T, T, 0, st>>>(eng_, order, Q, f.q_sizes);
-        b = f.tmp_bytes;
-        NAER_CK(cub::DeviceScan::ExclusiveSum(f.tmp, b, f.q_sizes, f.q_offs, (int)Q, st));
-        NAER_CK(cudaMemcpyAsync(h_pinned_, f.q_offs + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
-        NAER_CK(cudaMemcpyAsync(h_pinned_ + 1, f.q_sizes + (Q - 1), 4, cudaMemcpyDeviceToHost, st));
-        NAER_CK(cudaStreamSynchronize(st));
-        const uint64_t E = (uint64_t)h_pinned_[0] + h_pinned_[1];
-        if (E > f.e_max) throw Error(NAER_E_OVERFLOW, "internal: event count exceeds the fixed scratch partition");
-        k_det_raster<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + T - 1) / T, 1024)), T, 0, st>>>(eng_, order, Q);
-        if (E > 0) {
-            own_launches += 2;  // emit, fold
-            k_det_emit<<<std::max<uint32_t>(1, std::min<uint32_t>((Q + 7) / 8, (uint32_t)sm_count_ * 8)),
-                         kScatterThreads, 0, st>>>(eng_, order, Q, f.q_offs, f.e_keys[0], f.e_vals[0]);
-            cub::DoubleBuffer<unsigned long long> ek(f.e_keys[0], f.e_keys[1]);
-            cub::DoubleBuffer<float> ev(f.e_vals[0], f.e_vals[1]);
-            b = f.tmp_bytes;
-            NAER_CK(cub::DeviceRadixSort::SortPairs(f.tmp, b, ek, ev, (int)E, 0, f.e_bits, st));
-            k_det_fold<<<(uint32_t)((E + T - 1) / T), T, 0, st>>>(d_nets_, eng_.n_nets, ek.Current(),
-                                                                  ev.Current(), (uint32_t)E);
-        }
-    } else {
-        ++own_launches;
-        k_det_raster<<<1, 32, 0, st>>>(eng_, nullptr, 0);
+    if (aggregation_ != NAER_AGG_DETERMINISTIC)
+        throw Error(NAER_E_STATE, "the fixed-scratch step needs a network compiled with deterministic aggregation");
+    // partition (sizes first: a network that does not fit is refused before
+    // anything changes)
+    size_t used = 0;
+    std::vector<size_t> off_w, off_next, off_head;
+    uint64_t syn = 0, cells = 0;
+    for (const NetHost* n : nets_) {
+        if (det_syn_entries(*n) >= kNoEvent || det_cells(*n) >= 0xFFFFFFFFull)
+            throw Error(NAER_E_OVERFLOW, "network too large for deterministic aggregation");
+        off_w.push_back(used);
+        used = align256(used + det_syn_entries(*n) * 4ull);
+        off_next.push_back(used);
+        used = align256(used + det_syn_entries(*n) * 4ull);
+        off_head.push_back(used);
+        used = align256(used + det_cells(*n) * 4ull);
+        syn += det_syn_entries(*n);
+        cells += det_cells(*n);
     }
-    k_advance<<<1, 32, 0, st>>>(eng_);
-    NAER_CK(cudaGetLastError());
-    launches_ += own_launches;
-    ++host_step_;
+    if (used > kFixedScratchBytes)
+        throw Error(NAER_E_OVERFLOW,
+                    "network too large for the fixed-scratch step: its " + std::to_string(syn) +
+                        " padded synapses and " + std::to_string(cells) + " ring cells need " +
+                        std::to_string(used) + " bytes of scratch (8 per synapse, 4 per ring cell); the fixed "
+                        "arena holds " + std::to_string(kFixedScratchBytes) + " bytes");
+    unsigned char* a = fixed_scratch_base(device_);
+    arena_w_.assign(nets_.size(), nullptr);
+    arena_next_.assign(nets_.size(), nullptr);
+    arena_head_.assign(nets_.size(), nullptr);
+    for (size_t i = 0; i < nets_.size(); ++i) {
+        arena_w_[i] = reinterpret_cast<float*>(a + off_w[i]);
+        arena_next_[i] = reinterpret_cast<uint32_t*>(a + off_next[i]);
+        arena_head_[i] = reinterpret_cast<uint32_t*>(a + off_head[i]);
+        // the array keeps the last call's contents (any network's): every
+        // list head must start empty
+        NAER_CK(cudaMemsetAsync(arena_head_[i], 0xFF, det_cells(*nets_[i]) * 4ull, stream_));
+    }
+    point_det_scratch(kScratchArena);
+    run_launches(nsteps);
 }
 
 void Engine::sync() {

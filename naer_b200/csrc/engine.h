@@ -47,6 +47,7 @@ struct NetHost {
     uint32_t n_ids = 0, n_storage = 0, n_plastic = 0, ring_slots = 0;
     uint32_t n_poisson = 0;
     uint64_t synapses = 0, synapses_padded = 0, max_row_padded = 0;
+    uint64_t max_first_padded = 0, max_rest_padded = 0;  // longest delay-1 part / rest of a row, padded
     uint64_t syn_capacity = 0;  // entries allocated for tgt / w / dly (>= synapses_padded)
     std::vector<int32_t> id_of_storage;   // -1 for padding
     std::vector<uint32_t> storage_of_id;
@@ -67,6 +68,10 @@ struct NetHost {
     float* e_plus = nullptr;
     float* e_minus = nullptr;
     uint32_t e_len = 0;
+    // deterministic-aggregation scratch (allocated by the first deterministic step)
+    float* det_w = nullptr;
+    uint32_t* det_next = nullptr;
+    uint32_t* det_head = nullptr;
     uint64_t device_bytes = 0;
 
     NetDev dev{};
@@ -92,6 +97,7 @@ struct Tuning {
     uint32_t scatter_split = 0;            // warps per spike (0 = enough to cover the longest row)
     uint32_t scatter_piece = 0;            // synapses per warp iteration: 128, 256, 0 = 128 with STDP else 256
     uint32_t neuron_state = 0;             // NAER_STATE_AUTO / _SHARED / _GLOBAL: where the step kernel keeps V
+    uint32_t step_kernel = 0;              // NAER_KERNEL_SPLIT (k_step) / NAER_KERNEL_TWO_BARRIER (k_run)
 };
 
 struct TuneResult {
@@ -129,7 +135,7 @@ public:
     // neuron state in shared memory at the most resident blocks per SM it
     // can have under the current tuning (its fastest geometry); beyond it
     // the step runs with fewer blocks or with state in global memory.
-    uint32_t fast_chunk_capacity();
+    uint32_t fast_chunk_capacity(uint32_t aggregation);
     // Times candidate launch geometries on the installed networks (each
     // trial advances the simulation by trial_steps grid steps) and keeps
     // the fastest.  Deterministic aggregation: nothing to tune.
@@ -184,9 +190,15 @@ public:
 private:
     void launch_run(uint32_t steps);
     void launch_drive(uint64_t s_first, uint32_t nsteps);
-    void run_deterministic_step();
-    void ensure_det_capacity(uint64_t events);
+    void run_launches(uint64_t nsteps);
     void regrow(void*& p, size_t& have, size_t need);
+    // deterministic-aggregation scratch: which one the installed tables point at
+    static constexpr uint32_t kScratchNone = 0, kScratchOwn = 1, kScratchArena = 2;
+    uint32_t det_scratch_ = kScratchNone;
+    std::vector<float*> arena_w_;
+    std::vector<uint32_t*> arena_next_, arena_head_;
+    void ensure_det_scratch();
+    void point_det_scratch(uint32_t mode);
     uint64_t sum_parts(const unsigned long long* d, uint32_t n);
 
     int device_ = 0;
@@ -212,7 +224,6 @@ private:
     size_t queue_bytes_[2] = {0, 0}, qid_bytes_[2] = {0, 0}, counts_bytes_[2] = {0, 0};
     size_t ev_part_bytes_ = 0, ovf_part_bytes_ = 0;
     size_t scatter_smem_ = 0;
-    uint32_t* det_prefix_ = nullptr;
     std::vector<NetDev> h_nets_;
     uint32_t queue_cap_ = 0;
     uint32_t aggregation_ = NAER_AGG_ATOMIC;
@@ -231,44 +242,13 @@ private:
     uint64_t total_ring_cells_ = 0;
 
 
-    // deterministic-mode scratch
-    unsigned long long* q_keys_[2] = {nullptr, nullptr};
-    uint32_t* q_vals_[2] = {nullptr, nullptr};
-    uint32_t* q_sizes_ = nullptr;
-    uint32_t* q_offs_ = nullptr;
-    unsigned long long* e_keys_[2] = {nullptr, nullptr};
-    float* e_vals_[2] = {nullptr, nullptr};
-    uint64_t e_cap_ = 0;
-    uint64_t q_cap_alloc_ = 0;     // entries of q_keys_/q_vals_/q_sizes_/q_offs_
-    uint64_t det_prefix_cap_ = 0;  // entries of det_prefix_
-    void* cub_tmp_ = nullptr;
-    size_t cub_tmp_bytes_ = 0;
     uint32_t* h_pinned_ = nullptr;  // small pinned staging
-
-    // partitions of the fixed scratch arena (set up by the first
-    // run_fixed_scratch call on this engine)
-    struct FixedScratch {
-        bool ready = false;
-        uint64_t q_max = 0, e_max = 0;
-        int q_bits = 64, e_bits = 64;
-        uint32_t* prefix = nullptr;
-        unsigned long long* q_keys[2] = {nullptr, nullptr};
-        uint32_t* q_vals[2] = {nullptr, nullptr};
-        uint32_t* q_sizes = nullptr;
-        uint32_t* q_offs = nullptr;
-        unsigned long long* e_keys[2] = {nullptr, nullptr};
-        float* e_vals[2] = {nullptr, nullptr};
-        void* tmp = nullptr;
-        size_t tmp_bytes = 0;
-    };
-    FixedScratch fs_{};
-    void fixed_scratch_setup();
-    void run_fixed_scratch_step();
 
     bool failed_ = false;  // a launch reported a device error: state undefined
     void check_usable() const;
     bool profiling_ = false;
     bool use_smem_state_ = false;
+    bool split_kernel_ = true;  // k_step (else k_run)
     // CUDA-event timing of launches while profiling (pairs in launch order)
     std::vector<cudaEvent_t> timer_events_;
     std::vector<int> timer_kinds_;  // 0 drive, 1 step kernel

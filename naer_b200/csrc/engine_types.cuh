@@ -18,6 +18,7 @@ namespace naer {
 enum NeuronType : uint32_t { kSTDP = 0, kNOP = 1, kPOISSON = 2 };
 
 constexpr uint32_t kTgtSentinel = 0xFFFFFFFFu;  // padding entry in a CSR row
+constexpr uint32_t kNoEvent = 0xFFFFFFFFu;      // end of a ring cell's event list
 constexpr uint32_t kRowAlign = 4;               // rows start on 16-byte boundaries
 constexpr uint32_t kLifThreads = 256;
 constexpr uint32_t kLifPerThread = 4;
@@ -81,6 +82,12 @@ struct NetDev {
     int2* pre;              // {step of the latest pre spike (-1 = none), pre trace after it (float bits)}
     const float* e_plus;    // [e_len] exp(-k dt / tau_plus) as float
     const float* e_minus;   // [e_len] exp(-k dt / tau_minus) as float
+    // deterministic aggregation: per padded synapse j, the weight it delivered
+    // in the current step and the next event of its ring cell's list; per
+    // ring cell, the list head (kNoEvent when empty between steps)
+    float* ev_w;
+    uint32_t* ev_next;
+    uint32_t* cell_head;
     uint64_t start_step;    // engine step at which this net's step 0 runs
     uint64_t end_step;      // first engine step at which this net no longer runs (~0 = never)
     uint64_t ring_key_base; // first ring cell of this net in the deterministic key space
@@ -138,6 +145,7 @@ struct Ctl {
     unsigned long long prof_steps;
     unsigned long long prof_phase_ns[5];  // LIF, barrier 1, early scatter, late scatter, barrier 2
     unsigned long long bar_arrive;  // grid barrier arrivals of the running launch
+    unsigned int qtail[4];          // k_step: spikes queued in step s, slot s & 3 (zeroed with bar_arrive)
     unsigned int error;
     unsigned int pad_;
     unsigned long long bar_limit_ns;  // bounded wait of one grid barrier (0 = kBarrierLimitNs)
@@ -147,11 +155,14 @@ struct Ctl {
 
 constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // 2 s
 
-constexpr int NAER_STATUS_TIMEOUT = -4;  // NAER_E_TIMEOUT of the C ABI
+constexpr int NAER_STATUS_OVERFLOW = -3;  // NAER_E_OVERFLOW of the C ABI
+constexpr int NAER_STATUS_TIMEOUT = -4;   // NAER_E_TIMEOUT of the C ABI
 
-// Spike queue: LIF block b compacts its spikes into region
-// [b * region_cap, (b + 1) * region_cap) of the step's buffer and writes
-// their number to counts[b]; the scatter prefix-sums the counts.
+// Spike queue.  k_run and the deterministic path: LIF block b compacts its
+// spikes into region [b * region_cap, (b + 1) * region_cap) of the step's
+// buffer and writes their number to counts[b]; the scatter prefix-sums the
+// counts.  k_step: one contiguous list per step, each warp reserving its
+// spikes' places with one atomic on Ctl::qtail.
 struct EngineDev {
     Ctl* ctl;
     const NetDev* nets;
@@ -171,6 +182,12 @@ struct EngineDev {
     uint32_t record;                // append spikes to the raster
     uint32_t scatter_split;         // warps per spike (row pieces of scatter_piece)
     uint32_t scatter_piece;         // synapses per warp iteration: 128 or kScatterPiece
+    // k_step: warps per spike over the part of a row that must arrive
+    // before the next LIF (the delay-1 part; whole rows of plastic sources)
+    // and over the rest (delays >= 2 of static sources)
+    uint32_t split_first;
+    uint32_t split_rest;
+    uint32_t queue_cap;             // entries of queue[i] / qid[i]
 };
 
 }  // namespace naer

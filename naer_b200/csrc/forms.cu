@@ -71,10 +71,7 @@ void Batch::compile() {
 
 void Batch::step(uint64_t nsteps, uint32_t graph_launches) {
     if (!compiled_) throw Error(NAER_E_STATE, "batch is not compiled");
-    if (aggregation_ == NAER_AGG_DETERMINISTIC)
-        eng_->run(nsteps);
-    else
-        eng_->run_graph(nsteps, graph_launches);
+    eng_->run_graph(nsteps, graph_launches);
 }
 
 TuneResult Batch::autotune(uint32_t trial_steps) {
@@ -366,7 +363,7 @@ void Server::loop() {
         // geometry (neuron state in shared memory, most blocks per SM).  A
         // larger set steps more slowly per job, so a backlog that admitted
         // everything would lower the throughput that has to clear it.
-        const uint64_t chunk_cap = eng->fast_chunk_capacity();
+        const uint64_t chunk_cap = eng->fast_chunk_capacity(prm_.aggregation);
         NAER_CK(cudaHostAlloc(reinterpret_cast<void**>(&rec), prm_.raster_capacity * sizeof(uint2),
                               cudaHostAllocDefault));
         NAER_CK(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));

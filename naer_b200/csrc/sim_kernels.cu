@@ -308,24 +308,6 @@ __device__ __forceinline__ void lif_chunk(const EngineDev& eng, uint32_t c, unsi
     }
 }
 
-// Standalone LIF pass (deterministic mode); same queue layout as k_run.
-__global__ void __launch_bounds__(kLifThreads) k_lif(EngineDev eng) {
-    __shared__ uint32_t s_count;
-    const unsigned long long s = eng.ctl->step;
-    const uint32_t qb = (uint32_t)(s & 1ull);
-    const uint32_t region = blockIdx.x * eng.region_cap;
-    SpikeRec* __restrict__ queue = (qb ? eng.queue[1] : eng.queue[0]) + region;
-    uint32_t* __restrict__ qid = (qb ? eng.qid[1] : eng.qid[0]) + region;
-    if (threadIdx.x == 0) {
-        s_count = 0;
-        if (blockIdx.x == 0) eng.ctl->raster_base = eng.ctl->raster_next;
-    }
-    __syncthreads();
-    for (uint32_t c = blockIdx.x; c < eng.n_chunks; c += gridDim.x) lif_chunk(eng, c, s, queue, qid, &s_count);
-    __syncthreads();
-    if (threadIdx.x == 0) (qb ? eng.counts[1] : eng.counts[0])[blockIdx.x] = s_count;
-}
-
 // Exclusive prefix of the LIF blocks' spike counts into shared memory
 // (prefix[0..n]); returns the total.
 __device__ __forceinline__ uint32_t block_prefix_counts(const uint32_t* __restrict__ counts, uint32_t n,
@@ -766,129 +748,820 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
 template __global__ void k_run<true>(EngineDev, unsigned long long, uint32_t);
 template __global__ void k_run<false>(EngineDev, unsigned long long, uint32_t);
 
-size_t run_smem_bytes(uint32_t grid, uint32_t own_max, bool smem_state) {
-    const size_t off_cc = (((grid + 1) * sizeof(uint32_t)) + 15) & ~(size_t)15;
+// ---------------------------------------------------------------------------
+// k_step: the persistent step kernel (atomic mode) with one contiguous spike
+// list per step and the scatter split by deadline.
+//
+// Per grid step s:
+//  1. LIF of the block's chunks.  A warp keeps the spike flags of a batch of
+//     chunks in registers and reserves their places in the step's list with
+//     one atomic on Ctl::qtail[s & 3], then writes the records: no per-block
+//     regions, no prefix sum of block counts, no search for a spike's region.
+//  2. Grid barrier B1 (the list is complete).  While warp 0 waits for it, the
+//     block's other warps deliver what is left of step s-1's deferred part.
+//  3. The first part of every row: the delay-1 synapses of static sources
+//     (the next LIF reads them) and the whole row of plastic sources (their
+//     weight updates must see the post-synaptic state of step s).  Then any
+//     deferred work of step s-1 still left: its delay-2 synapses feed the
+//     LIF of step s+1.
+//  4. Arrive at grid barrier B2.  While warp 0 waits for it, warps 1.. deliver
+//     the rest of step s's rows (delays >= 2 of static sources); what is left
+//     when B2 completes moves to step s+1 (at the latest before its B2
+//     arrival, which precedes the LIF of step s+2).
+// Every delivery is a red.add into the ring as in k_run; only the time at
+// which a synapse is delivered moves, never its ring slot.
+
+// Delivers the synapses [lo, hi) of one spike's row: warp pieces piece,
+// piece + split, ... of psz synapses, 128-bit loads, red.add into the ring
+// (STDP update first for plastic synapses of plastic sources).
+__device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, const SpikeRec& r, uint64_t lo,
+                                             uint64_t hi, uint32_t piece, uint32_t split, uint32_t psz,
+                                             uint32_t lane, unsigned long long& ev, uint32_t& ovf) {
+    const uint32_t D = np->ring_slots;
+    const uint32_t tmod = tl % D;
+    const uint32_t Ns = np->n_storage;
+    float* __restrict__ ring = np->ring;
+    const uint32_t* __restrict__ tgt_a = np->tgt;
+    float* __restrict__ w_a = np->w;
+    const uint8_t* __restrict__ d_a = np->dly;
+    const uint32_t n_plastic = np->n_plastic;
+    const bool plastic_src = np->stdp_on && r.src < n_plastic;
+    StdpView sv;
+    if (plastic_src) sv = stdp_view(*np);
+    const float mult = (!plastic_src && r.aux0 > 1) ? (float)r.aux0 : 1.0f;
+    for (uint64_t base = lo + (uint64_t)piece * psz; base < hi; base += (uint64_t)split * psz) {
+        uint4 tg[kScatterUnroll];
+        float4 ww[kScatterUnroll];
+        uint32_t dd[kScatterUnroll];
+#pragma unroll
+        for (int u = 0; u < (int)kScatterUnroll; ++u) {
+            const uint64_t off = base + (uint64_t)(u * 32 + lane) * 4ull;
+            if (off < hi && (uint32_t)u * 128u < psz) {
+                tg[u] = ld_stream_u4(tgt_a + off);
+                ww[u] = __ldcg(reinterpret_cast<const float4*>(w_a + off));  // STDP may rewrite
+                dd[u] = ld_stream_u32(d_a + off);
+            } else {
+                tg[u] = make_uint4(kTgtSentinel, kTgtSentinel, kTgtSentinel, kTgtSentinel);
+                ww[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                dd[u] = 0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < (int)kScatterUnroll; ++u) {
+            const uint64_t off = base + (uint64_t)(u * 32 + lane) * 4ull;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t tgt = u4_get(tg[u], j);
+                if (tgt == kTgtSentinel) continue;
+                float w = f4_get(ww[u], j);
+                const uint32_t d = (dd[u] >> (8 * j)) & 0xFFu;
+                if (plastic_src && tgt < n_plastic) {
+                    w = stdp_update(sv, w, tgt, (int32_t)tl, r.aux0, r.aux1, ovf);
+                    __stcg(w_a + off + j, w);
+                }
+                if (mult != 1.0f) w = __fmul_rn(w, mult);
+                red_add_f32(ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w);
+                ++ev;
+            }
+        }
+    }
+}
+
+// deliver_span for a static source (no plasticity): the deferred rest.
+__device__ __forceinline__ void deliver_static_span(const NetDev* np, uint32_t tl, int32_t aux0, uint64_t lo,
+                                                    uint64_t hi, uint32_t piece, uint32_t split, uint32_t psz,
+                                                    uint32_t lane, unsigned long long& ev) {
+    const uint32_t D = np->ring_slots;
+    const uint32_t tmod = tl % D;
+    const uint32_t Ns = np->n_storage;
+    float* __restrict__ ring = np->ring;
+    const uint32_t* __restrict__ tgt_a = np->tgt;
+    const float* __restrict__ w_a = np->w;
+    const uint8_t* __restrict__ d_a = np->dly;
+    const float mult = aux0 > 1 ? (float)aux0 : 1.0f;
+    for (uint64_t base = lo + (uint64_t)piece * psz; base < hi; base += (uint64_t)split * psz) {
+        uint4 tg[kScatterUnroll];
+        float4 ww[kScatterUnroll];
+        uint32_t dd[kScatterUnroll];
+#pragma unroll
+        for (int u = 0; u < (int)kScatterUnroll; ++u) {
+            const uint64_t off = base + (uint64_t)(u * 32 + lane) * 4ull;
+            if (off < hi && (uint32_t)u * 128u < psz) {
+                tg[u] = ld_stream_u4(tgt_a + off);
+                ww[u] = __ldcs(reinterpret_cast<const float4*>(w_a + off));
+                dd[u] = ld_stream_u32(d_a + off);
+            } else {
+                tg[u] = make_uint4(kTgtSentinel, kTgtSentinel, kTgtSentinel, kTgtSentinel);
+                ww[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                dd[u] = 0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < (int)kScatterUnroll; ++u) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t tgt = u4_get(tg[u], j);
+                if (tgt == kTgtSentinel) continue;
+                float w = f4_get(ww[u], j);
+                if (mult != 1.0f) w = __fmul_rn(w, mult);
+                red_add_f32(ring + (size_t)ring_slot(tmod, (dd[u] >> (8 * j)) & 0xFFu, D) * Ns + tgt, w);
+                ++ev;
+            }
+        }
+    }
+}
+
+// LIF of one owned chunk with its state in shared memory (the arithmetic of
+// lif_chunk); returns the spike flags of the thread's four neurons (bit k =
+// neuron first + 4 * thread + k).  Post-spike plasticity bookkeeping is left
+// to the record writer.
+__device__ __forceinline__ uint32_t lif_flags_smem(const ChunkCache& cc, uint32_t j, unsigned long long s,
+                                                   float4* sV, uchar4* sR, const float4 I, const uint32_t Dw) {
+    if (!cc.active || s < cc.start || s >= cc.stop) return 0u;
+    const uint32_t i0 = cc.first + threadIdx.x * kLifPerThread;
+    if (i0 >= cc.end) return 0u;
+    uint32_t f = 0;
+    if (cc.p.type == kPOISSON) {
+        if (cc.p.rate_hz > 0.0) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (i0 + k < cc.end && ((Dw >> (8 * k)) & 0xFFu)) f |= 1u << k;
+        }
+        return f;
+    }
+    const uint32_t si = j * kLifThreads + threadIdx.x;
+    const float4 V4 = sV[si];
+    const uchar4 R4 = sR[si];
+    float vv[4] = {V4.x, V4.y, V4.z, V4.w};
+    uint32_t rr[4] = {R4.x, R4.y, R4.z, R4.w};
+    const double prop = cc.p.prop;
+    const float v_th = cc.p.v_th, v_reset = cc.p.v_reset, dw = cc.p.drive_w;
+    const uint32_t tref = cc.p.t_ref_steps, end = cc.end;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (i0 + k >= end) continue;
+        if (rr[k] > 0) {
+            rr[k] -= 1;
+            continue;
+        }
+        float v = __double2float_rn(__dmul_rn((double)vv[k], prop));
+        v = __fadd_rn(v, f4_get(I, k));
+        const uint32_t m = (Dw >> (8 * k)) & 0xFFu;
+        for (uint32_t q = 0; q < m; ++q) v = __fadd_rn(v, dw);
+        if (v > v_th) {
+            v = v_reset;
+            rr[k] = tref;
+            f |= 1u << k;
+        }
+        vv[k] = v;
+    }
+    sV[si] = make_float4(vv[0], vv[1], vv[2], vv[3]);
+    sR[si] = make_uchar4((unsigned char)rr[0], (unsigned char)rr[1], (unsigned char)rr[2], (unsigned char)rr[3]);
+    return f;
+}
+
+// Reserves places for the warp's spikes (cnt per lane) in the step's list:
+// one atomic per warp.  Returns the lane's first place.
+__device__ __forceinline__ uint32_t reserve_places(Ctl* ctl, unsigned long long s, uint32_t cnt, uint32_t lane) {
+    uint32_t x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, x, 31);
+    uint32_t base = 0;
+    if (total) {
+        if (lane == 31) base = atomicAdd(&ctl->qtail[s & 3ull], total);
+        base = __shfl_sync(0xFFFFFFFFu, base, 31);
+    }
+    return base + x - cnt;
+}
+
+// Writes one spike record: POISSON sources carry their multiplicity,
+// plastic neurons run their post-spike bookkeeping here.
+__device__ __forceinline__ void write_spike(const EngineDev& eng, SpikeRec* __restrict__ queue,
+                                            uint32_t* __restrict__ qid, uint32_t pos, uint32_t net, uint32_t i,
+                                            const PopDev& p, bool plastic, uint32_t tl, uint32_t count) {
+    int32_t aux0 = 0;
+    float aux1 = 0.0f;
+    if (p.type == kPOISSON) aux0 = (int32_t)count;
+    else if (plastic) stdp_post_spike(eng.nets + net, i, (int32_t)tl, aux0, aux1);
+    if (pos < eng.queue_cap) {
+        __stcg(reinterpret_cast<int4*>(queue + pos), make_int4((int)net, (int)i, aux0, __float_as_int(aux1)));
+        __stcg(qid + pos, p.id_base + (i - p.storage_base));
+    } else {
+        atomicCAS(&eng.ctl->error, 0u, (unsigned int)(-NAER_STATUS_OVERFLOW));
+    }
+}
+
+// Polls a grid barrier from warp 0, lane 0 (warp 0 does nothing else until
+// it completes) and raises *flag for the block's other warps when it does.
+__device__ __forceinline__ void poll_barrier(Ctl* ctl, unsigned long long target, const BarrierCfg& cfg,
+                                             volatile int* flag, int* ok) {
+    const unsigned long long t0 = globaltimer_ns();
+    const unsigned long long goal = target + cfg.skew;
+    unsigned long long cur;
+    for (;;) {
+        asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(cur) : "l"(&ctl->bar_arrive) : "memory");
+        if (cur >= goal) break;
+        if (globaltimer_ns() - t0 > cfg.limit_ns) {
+            atomicCAS(&ctl->error, 0u, (unsigned int)(-NAER_STATUS_TIMEOUT));
+            *ok = 0;
+            break;
+        }
+        __nanosleep(32);
+    }
+    *flag = 1;
+}
+
+__device__ __forceinline__ void arrive_barrier(Ctl* ctl) {
+    __threadfence();  // the block's stores and reductions (ordered by the preceding __syncthreads)
+    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(&ctl->bar_arrive) : "memory");
+}
+
+// Deferred ("rest") scatter work of one step: the step, its list's buffer
+// and its item count are the same for the whole block (shared memory); each
+// warp walks items it, it + WR, ... (it in a register).
+struct RestWork {
+    unsigned long long step;
+    uint32_t n, qb;
+};
+
+__device__ __forceinline__ void rest_item(const EngineDev& eng, const RestWork& rw, uint32_t it, const NetDev* net0,
+                                          uint32_t lane, unsigned long long& ev) {
+    const uint32_t split = eng.split_rest;
+    const uint32_t e = it / split;
+    const uint32_t piece = it - e * split;
+    const int4 rv = __ldcg(reinterpret_cast<const int4*>(eng.queue[rw.qb] + e));
+    const uint32_t net = (uint32_t)rv.x, src = (uint32_t)rv.y;
+    const NetDev* np = net == 0 ? net0 : eng.nets + net;
+    if (np->stdp_on && src < np->n_plastic) return;  // plastic rows went whole with the first part
+    const ulonglong2 rb = row_bounds(np->row_ptr, src);
+    const uint64_t mid = rb.x + __ldg(np->row_mid + src);
+    deliver_static_span(np, (uint32_t)(rw.step - np->start_step), rv.z, mid, rb.y, piece, split, eng.scatter_piece,
+                        lane, ev);
+}
+
+// Chunk descriptors, membrane potentials and refractory counters of the
+// block's owned chunks into shared memory (start of a persistent launch) and
+// back (end of it).
+__device__ __forceinline__ void load_chunk_state(const EngineDev& eng, uint32_t own, ChunkCache* s_cc, float4* sV,
+                                                 uchar4* sR) {
+    const uint32_t G = gridDim.x;
+    for (uint32_t j = threadIdx.x; j < own; j += blockDim.x) {
+        const ChunkDev ch = eng.chunks[blockIdx.x + j * G];
+        const NetDev* np = eng.nets + ch.net;
+        ChunkCache c;
+        c.p = eng.pops[ch.pop];
+        c.ring = np->ring;
+        c.v = np->v;
+        c.refr = np->refr;
+        c.drive = np->drive;
+        c.start = np->start_step;
+        c.stop = np->end_step;
+        c.first = ch.first;
+        c.end = ch.end;
+        c.net = ch.net;
+        c.Ns = np->n_storage;
+        c.slots = np->ring_slots;
+        c.dt_us = np->dt_us;
+        c.active = np->active;
+        c.plastic = (c.p.type == kSTDP && np->stdp_on) ? 1u : 0u;
+        s_cc[j] = c;
+    }
+    __syncthreads();
+    for (uint32_t j = 0; j < own; ++j) {
+        const uint32_t i0 = s_cc[j].first + threadIdx.x * kLifPerThread;
+        if (i0 < s_cc[j].end) {
+            const uint32_t si = j * kLifThreads + threadIdx.x;
+            sV[si] = *reinterpret_cast<const float4*>(s_cc[j].v + i0);
+            sR[si] = *reinterpret_cast<const uchar4*>(s_cc[j].refr + i0);
+        }
+    }
+}
+
+__device__ __forceinline__ void store_chunk_state(uint32_t own, const ChunkCache* s_cc, const float4* sV,
+                                                  const uchar4* sR) {
+    __syncthreads();
+    for (uint32_t j = 0; j < own; ++j) {
+        const uint32_t i0 = s_cc[j].first + threadIdx.x * kLifPerThread;
+        if (i0 < s_cc[j].end) {
+            const uint32_t si = j * kLifThreads + threadIdx.x;
+            *reinterpret_cast<float4*>(s_cc[j].v + i0) = sV[si];
+            *reinterpret_cast<uchar4*>(s_cc[j].refr + i0) = sR[si];
+        }
+    }
+}
+
+// Per-thread event and history-overflow counts into the block's counters
+// (no same-address global atomics on the hot path).
+__device__ __forceinline__ void finish_counters(const EngineDev& eng, unsigned long long ev, uint32_t ovf,
+                                                uint32_t lane, unsigned long long* s_ev, uint32_t* s_ovf) {
+    ev = warp_sum_u64(ev);
+    const unsigned long long ov = warp_sum_u64((unsigned long long)ovf);
+    if (lane == 0) {
+        if (ev) atomicAdd(s_ev, ev);
+        if (ov) atomicAdd(s_ovf, (uint32_t)ov);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (*s_ev) eng.ev_part[blockIdx.x] += *s_ev;
+        if (*s_ovf) eng.ovf_part[blockIdx.x] += *s_ovf;
+    }
+}
+
+// LIF phase of a persistent step kernel: the block's chunks (state in shared
+// memory with kSmem), spikes appended to the step's list (one reservation
+// per warp and batch of chunks).
+template <bool kSmem>
+__device__ __forceinline__ void lif_phase(const EngineDev& eng, unsigned long long s, uint32_t own,
+                                          const ChunkCache* s_cc, float4* sV, uchar4* sR,
+                                          SpikeRec* __restrict__ queue, uint32_t* __restrict__ qid,
+                                          uint32_t lane) {
+    const uint32_t G = gridDim.x;
+    Ctl* ctl = eng.ctl;
+    if (kSmem) {
+        for (uint32_t j0 = 0; j0 < own; j0 += kLifBatch) {
+            float4 I[kLifBatch];
+            uint32_t Dw[kLifBatch];
+#pragma unroll
+            for (uint32_t b = 0; b < kLifBatch; ++b)
+                if (j0 + b < own) lif_prefetch(s_cc[j0 + b], s, I[b], Dw[b]);
+#pragma unroll
+            for (uint32_t b = 0; b < kLifBatch; ++b)
+                if (j0 + b < own) lif_clear(s_cc[j0 + b], s);
+            uint32_t mask = 0;
+#pragma unroll
+            for (uint32_t b = 0; b < kLifBatch; ++b)
+                if (j0 + b < own) mask |= lif_flags_smem(s_cc[j0 + b], j0 + b, s, sV, sR, I[b], Dw[b]) << (4 * b);
+            if (__any_sync(0xFFFFFFFFu, mask != 0)) {
+                uint32_t pos = reserve_places(ctl, s, __popc(mask), lane);
+#pragma unroll
+                for (uint32_t b = 0; b < kLifBatch; ++b) {
+                    const uint32_t m4 = (mask >> (4 * b)) & 0xFu;
+                    if (!m4) continue;
+                    const ChunkCache& cc = s_cc[j0 + b];
+                    const uint32_t i0 = cc.first + threadIdx.x * kLifPerThread;
+                    const uint32_t tl = (uint32_t)(s - cc.start);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if ((m4 >> q) & 1u)
+                            write_spike(eng, queue, qid, pos++, cc.net, i0 + q, cc.p, cc.plastic != 0, tl,
+                                        (Dw[b] >> (8 * q)) & 0xFFu);
+                }
+            }
+        }
+    } else {
+        for (uint32_t c = blockIdx.x; c < eng.n_chunks; c += G) {
+            const ChunkDev ch = eng.chunks[c];
+            const PopDev p = eng.pops[ch.pop];
+            const NetDev* np = eng.nets + ch.net;
+            const unsigned long long start = np->start_step;
+            if (!np->active || s < start || s >= np->end_step) continue;  // uniform over the block
+            const uint32_t tl = (uint32_t)(s - start);
+            const uint32_t i0 = ch.first + threadIdx.x * kLifPerThread;
+            uint32_t Dw = 0;
+            uint32_t f = 0;
+            if (i0 < ch.end) {
+                const uint8_t* drive_slot = np->drive + (size_t)(s % kDriveSlots) * np->n_storage;
+                if (p.rate_hz > 0.0) Dw = __ldcg(reinterpret_cast<const unsigned int*>(drive_slot + i0));
+                if (p.type == kPOISSON) {
+                    if (p.rate_hz > 0.0) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            if (i0 + q < ch.end && ((Dw >> (8 * q)) & 0xFFu)) f |= 1u << q;
+                    }
+                } else {
+                    const uint32_t Ns = np->n_storage;
+                    float4* ring4 = reinterpret_cast<float4*>(np->ring + (size_t)(tl % np->ring_slots) * Ns) +
+                                    (i0 >> 2);
+                    float4* v4 = reinterpret_cast<float4*>(np->v) + (i0 >> 2);
+                    uchar4* r4 = reinterpret_cast<uchar4*>(np->refr) + (i0 >> 2);
+                    const float4 Iv = __ldcg(ring4);
+                    const float4 V4 = *v4;
+                    const uchar4 R4 = *r4;
+                    __stcg(ring4, make_float4(0.f, 0.f, 0.f, 0.f));
+                    float vv[4] = {V4.x, V4.y, V4.z, V4.w};
+                    uint32_t rr[4] = {R4.x, R4.y, R4.z, R4.w};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (i0 + q >= ch.end) continue;
+                        if (rr[q] > 0) {
+                            rr[q] -= 1;
+                            continue;
+                        }
+                        float v = __double2float_rn(__dmul_rn((double)vv[q], p.prop));
+                        v = __fadd_rn(v, f4_get(Iv, q));
+                        const uint32_t m = (Dw >> (8 * q)) & 0xFFu;
+                        for (uint32_t z = 0; z < m; ++z) v = __fadd_rn(v, p.drive_w);
+                        if (v > p.v_th) {
+                            v = p.v_reset;
+                            rr[q] = p.t_ref_steps;
+                            f |= 1u << q;
+                        }
+                        vv[q] = v;
+                    }
+                    *v4 = make_float4(vv[0], vv[1], vv[2], vv[3]);
+                    *r4 = make_uchar4((unsigned char)rr[0], (unsigned char)rr[1], (unsigned char)rr[2],
+                                      (unsigned char)rr[3]);
+                }
+            }
+            if (__any_sync(0xFFFFFFFFu, f != 0)) {
+                uint32_t pos = reserve_places(ctl, s, __popc(f), lane);
+                const bool plastic = p.type == kSTDP && np->stdp_on;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if ((f >> q) & 1u) write_spike(eng, queue, qid, pos++, ch.net, i0 + q, p, plastic, tl,
+                                                   (Dw >> (8 * q)) & 0xFFu);
+            }
+        }
+    }
+}
+
+template <bool kSmem>
+__global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
+    k_step(EngineDev eng, unsigned long long s0, uint32_t nsteps) {
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    __shared__ unsigned long long s_ev;
+    __shared__ uint32_t s_ovf;
+    __shared__ NetDev s_net0;  // descriptor of the first net (the only one in the plain form)
+    __shared__ BarrierCfg bcfg;
+    __shared__ int s_flag, s_ok;
+    __shared__ RestWork s_rw;                        // deferred work of the previous step
+    __shared__ unsigned long long s_ph[5], s_dropped;  // thread 0 only
+    __shared__ unsigned long long s_bar_target;      // thread 0 only
+    const uint32_t G = gridDim.x;
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t nw_block = kLifThreads / 32;
+    // the whole grid's warps (first part) and the warps 1.. of every block (rest)
+    const uint32_t gw = blockIdx.x * nw_block + wib, W = G * nw_block;
+    // (warp 0 has no deferred items: gr is unused there)
+    const uint32_t gr = blockIdx.x * (nw_block - 1) + (wib - 1), WR = G * (nw_block - 1);
+    Ctl* ctl = eng.ctl;
+    if (threadIdx.x == 0) {
+        s_net0 = eng.nets[0];
+        bcfg = barrier_cfg(ctl);
+        s_ev = 0;
+        s_ovf = 0;
+        s_ok = 1;
+        s_flag = 0;
+        s_rw = RestWork{0, 0, 0};  // nothing deferred at launch start
+        for (int q = 0; q < 5; ++q) s_ph[q] = 0;
+        s_dropped = 0;
+        s_bar_target = 0;
+    }
+    const uint32_t own_max = eng.region_cap / kLifChunk;
+    const size_t off_cc = 16;
+    ChunkCache* s_cc = reinterpret_cast<ChunkCache*>(s_dyn + off_cc);
+    const size_t off_v = off_cc + (((size_t)own_max * sizeof(ChunkCache) + 15) & ~(size_t)15);
+    float4* sV = reinterpret_cast<float4*>(s_dyn + off_v);
+    uchar4* sR = reinterpret_cast<uchar4*>(s_dyn + off_v + (size_t)own_max * kLifThreads * sizeof(float4));
+    const uint32_t own = blockIdx.x < eng.n_chunks ? (eng.n_chunks - blockIdx.x + G - 1) / G : 0u;
+
+    if (s0 == kStepFromCtl) s0 = ctl->step;
+    unsigned long long rbase = ctl->raster_next;
+    unsigned long long ev = 0;
+    uint32_t ovf = 0;
+    const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+    uint32_t rit = 0;  // this warp's next deferred item
+    if (kSmem) load_chunk_state(eng, own, s_cc, sV, sR);
+    __syncthreads();
+    uint32_t k = 0;
+    for (; k < nsteps; ++k) {
+        const unsigned long long s = s0 + k;
+        const uint32_t qb = (uint32_t)(s & 1ull);
+        const unsigned long long ta = timer ? globaltimer_ns() : 0ull;
+        SpikeRec* queue = eng.queue[qb];
+        uint32_t* qid = eng.qid[qb];
+        // ---- 1. LIF
+        lif_phase<kSmem>(eng, s, own, s_cc, sV, sR, queue, qid, lane);
+        __syncthreads();
+        const unsigned long long ta2 = timer ? globaltimer_ns() : 0ull;
+        // ---- 2. B1: the step's list is complete; warps 1.. work off step s-1's rest meanwhile
+        if (threadIdx.x == 0) {
+            s_bar_target += G;
+            arrive_barrier(ctl);
+        }
+        if (wib == 0) {
+            if (lane == 0) poll_barrier(ctl, s_bar_target, bcfg, &s_flag, &s_ok);
+            __syncwarp();
+        } else {
+            while (rit < s_rw.n) {
+                if (*(volatile int*)&s_flag) break;
+                rest_item(eng, s_rw, rit, &s_net0, lane, ev);
+                rit += WR;
+            }
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        const unsigned long long tb = timer ? globaltimer_ns() : 0ull;
+        // ---- 3. first parts of step s, then the rest of step s-1 that is left
+        const uint32_t Q = __ldcg(&ctl->qtail[s & 3ull]);
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->qtail[(s + 2) & 3ull] = 0u;  // reused by step s+2
+        {
+            const uint32_t split = eng.split_first, psz = eng.scatter_piece;
+            const uint64_t n1 = (uint64_t)Q * split;
+            for (uint64_t it = gw; it < n1; it += W) {
+                const uint32_t e = (uint32_t)(it / split);
+                const uint32_t piece = (uint32_t)(it - (uint64_t)e * split);
+                const int4 rv = __ldcg(reinterpret_cast<const int4*>(queue + e));
+                SpikeRec r;
+                r.net = (uint32_t)rv.x;
+                r.src = (uint32_t)rv.y;
+                r.aux0 = rv.z;
+                r.aux1 = __int_as_float(rv.w);
+                if (piece == 0 && lane == 0 && eng.record && rbase + e < eng.raster_cap)
+                    __stcg(eng.raster + rbase + e, make_uint2((uint32_t)s, __ldcg(qid + e)));
+                const NetDev* np = (r.net == 0) ? &s_net0 : eng.nets + r.net;
+                const ulonglong2 rb = row_bounds(np->row_ptr, r.src);
+                const bool plastic_src = np->stdp_on && r.src < np->n_plastic;
+                const uint64_t hi = plastic_src ? rb.y : rb.x + __ldg(np->row_mid + r.src);
+                deliver_span(np, (uint32_t)(s - np->start_step), r, rb.x, hi, piece, split, psz, lane, ev, ovf);
+            }
+        }
+        if (wib != 0) {
+            for (; rit < s_rw.n; rit += WR) rest_item(eng, s_rw, rit, &s_net0, lane, ev);
+        }
+        {
+            const unsigned long long cap = eng.record ? eng.raster_cap : 0ull;
+            const unsigned long long kept = rbase + Q <= cap ? Q : (rbase >= cap ? 0ull : cap - rbase);
+            if (eng.record && threadIdx.x == 0) s_dropped += Q - kept;
+            rbase += kept;
+        }
+        __syncthreads();
+        const unsigned long long tb2 = timer ? globaltimer_ns() : 0ull;
+        // ---- 4. B2: warps 1.. deliver step s's rest while warp 0 waits for it
+        if (threadIdx.x == 0) {
+            s_flag = 0;
+            s_bar_target += G;
+            arrive_barrier(ctl);
+            s_rw.step = s;
+            s_rw.qb = qb;
+            s_rw.n = Q * eng.split_rest;
+        }
+        rit = gr;
+        __syncthreads();
+        if (wib == 0) {
+            if (lane == 0) poll_barrier(ctl, s_bar_target, bcfg, &s_flag, &s_ok);
+            __syncwarp();
+        } else {
+            while (rit < s_rw.n) {
+                if (*(volatile int*)&s_flag) break;
+                rest_item(eng, s_rw, rit, &s_net0, lane, ev);
+                rit += WR;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_flag = 0;
+        if (!s_ok) break;
+        if (timer) {
+            const unsigned long long tc = globaltimer_ns();
+            s_ph[0] += ta2 - ta;
+            s_ph[1] += tb - ta2;
+            s_ph[2] += tb2 - tb;
+            s_ph[4] += tc - tb2;
+        }
+    }
+    // the last step's rest (the next launch's LIF reads it in stream order)
+    if (s_ok && wib != 0)
+        for (; rit < s_rw.n; rit += WR) rest_item(eng, s_rw, rit, &s_net0, lane, ev);
+    if (kSmem) store_chunk_state(own, s_cc, sV, sR);
+    finish_counters(eng, ev, ovf, lane, &s_ev, &s_ovf);
+    if (timer) {
+        ctl->step = s0 + k;
+        ctl->raster_next = rbase;
+        ctl->raster_base = rbase;
+        ctl->raster_dropped += s_dropped;
+        for (int q = 0; q < 5; ++q) ctl->prof_phase_ns[q] += s_ph[q];
+        ctl->prof_lif_ns += s_ph[0] + s_ph[1];
+        ctl->prof_scatter_ns += s_ph[2] + s_ph[4];
+        ctl->prof_steps += k;
+    }
+}
+
+template __global__ void k_step<true>(EngineDev, unsigned long long, uint32_t);
+template __global__ void k_step<false>(EngineDev, unsigned long long, uint32_t);
+
+// ---------------------------------------------------------------------------
+// k_det_step: the persistent step kernel with deterministic aggregation.
+//
+// A source spikes at most once per step, so an event is identified by its
+// synapse index j, and the order of a net's synapse array (rows in
+// ascending source, each row in its canonical order) is the canonical
+// (source, synapse) order.  Per grid step s:
+//  1. LIF, spikes appended to the step's list (as k_step);
+//  2. grid barrier; every event of the step stores the weight it delivers at
+//     ev_w[j] and is linked into its ring cell's list: ev_next[j] =
+//     atomicExch(cell_head[cell], j) (STDP updates first, as in the atomic
+//     path: they do not depend on the order);
+//  3. grid barrier; the event that started a list (ev_next == kNoEvent)
+//     walks it, orders its events by j and adds their left fold to the ring
+//     cell, then empties the head;
+//  4. grid barrier (the next LIF reads the ring).
+// The oracle folds each (step, cell) in the same order, so rings, membrane
+// potentials, weights and rasters are bit-identical; no sort, no host
+// round trip, no allocation while stepping.
+constexpr uint32_t kFoldRegs = 16;  // list length folded from a register copy
+
+__device__ __forceinline__ float fold_cell(const float* __restrict__ ev_w, const uint32_t* __restrict__ ev_next,
+                                           uint32_t head) {
+    uint32_t buf[kFoldRegs];
+    uint32_t n = 0;
+    for (uint32_t h = head; h != kNoEvent; h = __ldcg(ev_next + h)) {
+        if (n < kFoldRegs) buf[n] = h;
+        ++n;
+    }
+    if (n <= kFoldRegs) {
+        for (uint32_t a = 1; a < n; ++a) {  // insertion sort by synapse index
+            const uint32_t x = buf[a];
+            uint32_t b = a;
+            while (b > 0 && buf[b - 1] > x) {
+                buf[b] = buf[b - 1];
+                --b;
+            }
+            buf[b] = x;
+        }
+        float sum = __ldcg(ev_w + buf[0]);
+        for (uint32_t a = 1; a < n; ++a) sum = __fadd_rn(sum, __ldcg(ev_w + buf[a]));
+        return sum;
+    }
+    // long list: take its events in ascending j by repeated minimum search
+    float sum = 0.0f;
+    uint32_t last = 0;
+    for (uint32_t a = 0; a < n; ++a) {
+        uint32_t best = kNoEvent;
+        for (uint32_t h = head; h != kNoEvent; h = __ldcg(ev_next + h))
+            if ((a == 0 || h > last) && h < best) best = h;
+        const float w = __ldcg(ev_w + best);
+        sum = a == 0 ? w : __fadd_rn(sum, w);
+        last = best;
+    }
+    return sum;
+}
+
+// One (spike, piece) item of the deterministic path: pass 0 links events,
+// pass 1 folds the lists whose first event lies in the item.
+__device__ __forceinline__ void det_item(const EngineDev& eng, const SpikeRec* __restrict__ queue, uint32_t e,
+                                         uint32_t piece, uint32_t split, uint32_t psz, unsigned long long s,
+                                         const NetDev* net0, uint32_t lane, int pass, unsigned long long& ev,
+                                         uint32_t& ovf) {
+    const int4 rv = __ldcg(reinterpret_cast<const int4*>(queue + e));
+    SpikeRec r;
+    r.net = (uint32_t)rv.x;
+    r.src = (uint32_t)rv.y;
+    r.aux0 = rv.z;
+    r.aux1 = __int_as_float(rv.w);
+    const NetDev* np = r.net == 0 ? net0 : eng.nets + r.net;
+    const uint32_t tl = (uint32_t)(s - np->start_step);
+    const uint32_t D = np->ring_slots, tmod = tl % D, Ns = np->n_storage;
+    const ulonglong2 rb = row_bounds(np->row_ptr, r.src);
+    const uint32_t* __restrict__ tgt_a = np->tgt;
+    const uint8_t* __restrict__ d_a = np->dly;
+    float* __restrict__ w_a = np->w;
+    float* __restrict__ ev_w = np->ev_w;
+    uint32_t* __restrict__ ev_next = np->ev_next;
+    uint32_t* __restrict__ head = np->cell_head;
+    const bool plastic_src = np->stdp_on && r.src < np->n_plastic;
+    const uint32_t n_plastic = np->n_plastic;
+    StdpView sv;
+    if (pass == 0 && plastic_src) sv = stdp_view(*np);
+    const float mult = (!plastic_src && r.aux0 > 1) ? (float)r.aux0 : 1.0f;
+    for (uint64_t base = rb.x + (uint64_t)piece * psz; base < rb.y; base += (uint64_t)split * psz) {
+        const uint64_t top = rb.y < base + psz ? rb.y : base + psz;
+        for (uint64_t j = base + lane; j < top; j += 32) {
+            const uint32_t tgt = __ldcg(tgt_a + j);
+            if (tgt == kTgtSentinel) continue;
+            const uint32_t cell = ring_slot(tmod, __ldcg(d_a + j), D) * Ns + tgt;
+            if (pass == 0) {
+                float w = __ldcg(w_a + j);
+                if (plastic_src && tgt < n_plastic) {
+                    w = stdp_update(sv, w, tgt, (int32_t)tl, r.aux0, r.aux1, ovf);
+                    __stcg(w_a + j, w);
+                }
+                if (mult != 1.0f) w = __fmul_rn(w, mult);
+                __stcg(ev_w + j, w);
+                __stcg(ev_next + j, atomicExch(head + cell, (uint32_t)j));
+                ++ev;
+            } else if (__ldcg(ev_next + j) == kNoEvent) {
+                float* ring = np->ring + cell;
+                const float sum = fold_cell(ev_w, ev_next, __ldcg(head + cell));
+                __stcg(ring, __fadd_rn(__ldcg(ring), sum));
+                __stcg(head + cell, kNoEvent);
+            }
+        }
+    }
+}
+
+template <bool kSmem>
+__global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
+    k_det_step(EngineDev eng, unsigned long long s0, uint32_t nsteps) {
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    __shared__ unsigned long long s_ev;
+    __shared__ uint32_t s_ovf;
+    __shared__ NetDev s_net0;
+    __shared__ BarrierCfg bcfg;
+    __shared__ unsigned long long s_ph[5], s_dropped, s_bar_target;  // thread 0 only
+    const uint32_t G = gridDim.x;
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t gw = blockIdx.x * (kLifThreads / 32) + wib, W = G * (kLifThreads / 32);
+    Ctl* ctl = eng.ctl;
+    if (threadIdx.x == 0) {
+        s_net0 = eng.nets[0];
+        bcfg = barrier_cfg(ctl);
+        s_ev = 0;
+        s_ovf = 0;
+        for (int q = 0; q < 5; ++q) s_ph[q] = 0;
+        s_dropped = 0;
+        s_bar_target = 0;
+    }
+    const uint32_t own_max = eng.region_cap / kLifChunk;
+    const size_t off_cc = 16;
+    ChunkCache* s_cc = reinterpret_cast<ChunkCache*>(s_dyn + off_cc);
+    const size_t off_v = off_cc + (((size_t)own_max * sizeof(ChunkCache) + 15) & ~(size_t)15);
+    float4* sV = reinterpret_cast<float4*>(s_dyn + off_v);
+    uchar4* sR = reinterpret_cast<uchar4*>(s_dyn + off_v + (size_t)own_max * kLifThreads * sizeof(float4));
+    const uint32_t own = blockIdx.x < eng.n_chunks ? (eng.n_chunks - blockIdx.x + G - 1) / G : 0u;
+    if (s0 == kStepFromCtl) s0 = ctl->step;
+    unsigned long long rbase = ctl->raster_next;
+    unsigned long long ev = 0;
+    uint32_t ovf = 0;
+    const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+    if (kSmem) load_chunk_state(eng, own, s_cc, sV, sR);
+    __syncthreads();
+    const uint32_t split = eng.scatter_split, psz = eng.scatter_piece;
+    uint32_t k = 0;
+    for (; k < nsteps; ++k) {
+        const unsigned long long s = s0 + k;
+        const uint32_t qb = (uint32_t)(s & 1ull);
+        const unsigned long long ta = timer ? globaltimer_ns() : 0ull;
+        SpikeRec* queue = eng.queue[qb];
+        uint32_t* qid = eng.qid[qb];
+        lif_phase<kSmem>(eng, s, own, s_cc, sV, sR, queue, qid, lane);
+        if (threadIdx.x == 0) s_bar_target += G;
+        if (!grid_barrier(ctl, s_bar_target, bcfg)) break;
+        const unsigned long long tb = timer ? globaltimer_ns() : 0ull;
+        const uint32_t Q = __ldcg(&ctl->qtail[s & 3ull]);
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->qtail[(s + 2) & 3ull] = 0u;  // reused by step s+2
+        const uint64_t n = (uint64_t)Q * split;
+        for (uint64_t it = gw; it < n; it += W) {
+            const uint32_t e = (uint32_t)(it / split);
+            const uint32_t piece = (uint32_t)(it - (uint64_t)e * split);
+            if (piece == 0 && lane == 0 && eng.record && rbase + e < eng.raster_cap)
+                __stcg(eng.raster + rbase + e, make_uint2((uint32_t)s, __ldcg(qid + e)));
+            det_item(eng, queue, e, piece, split, psz, s, &s_net0, lane, 0, ev, ovf);
+        }
+        if (threadIdx.x == 0) s_bar_target += G;
+        if (!grid_barrier(ctl, s_bar_target, bcfg)) break;
+        const unsigned long long tb2 = timer ? globaltimer_ns() : 0ull;
+        for (uint64_t it = gw; it < n; it += W) {
+            const uint32_t e = (uint32_t)(it / split);
+            det_item(eng, queue, e, (uint32_t)(it - (uint64_t)e * split), split, psz, s, &s_net0, lane, 1, ev, ovf);
+        }
+        {
+            const unsigned long long cap = eng.record ? eng.raster_cap : 0ull;
+            const unsigned long long kept = rbase + Q <= cap ? Q : (rbase >= cap ? 0ull : cap - rbase);
+            if (eng.record && threadIdx.x == 0) s_dropped += Q - kept;
+            rbase += kept;
+        }
+        if (threadIdx.x == 0) s_bar_target += G;
+        if (!grid_barrier(ctl, s_bar_target, bcfg)) break;
+        if (timer) {
+            const unsigned long long tc = globaltimer_ns();
+            s_ph[0] += tb - ta;
+            s_ph[2] += tb2 - tb;
+            s_ph[4] += tc - tb2;
+        }
+    }
+    if (kSmem) store_chunk_state(own, s_cc, sV, sR);
+    finish_counters(eng, ev, ovf, lane, &s_ev, &s_ovf);
+    if (timer) {
+        ctl->step = s0 + k;
+        ctl->raster_next = rbase;
+        ctl->raster_base = rbase;
+        ctl->raster_dropped += s_dropped;
+        for (int q = 0; q < 5; ++q) ctl->prof_phase_ns[q] += s_ph[q];
+        ctl->prof_lif_ns += s_ph[0];
+        ctl->prof_scatter_ns += s_ph[2] + s_ph[4];
+        ctl->prof_steps += k;
+    }
+}
+
+template __global__ void k_det_step<true>(EngineDev, unsigned long long, uint32_t);
+template __global__ void k_det_step<false>(EngineDev, unsigned long long, uint32_t);
+
+size_t step_smem_bytes(uint32_t own_max, bool smem_state) {
+    const size_t off_cc = 16;
     if (!smem_state) return off_cc;
     const size_t off_v = off_cc + (((size_t)own_max * sizeof(ChunkCache) + 15) & ~(size_t)15);
     return off_v + (size_t)own_max * kLifThreads * (sizeof(float4) + sizeof(uchar4));
 }
 
-// ---------------------------------------------------------------------------
-// Deterministic aggregation.  Per step: sort the queue by (net, source);
-// emit one (ring cell, weight) event per synapse in ascending (source,
-// synapse) order; stable-sort the events by cell; fold each cell's run from
-// left to right and add the sum to the ring.  The oracle performs the same
-// per-(step, cell) fold, so ring contents and rasters are bit-identical.
-// `prefix` is the exclusive scan of the LIF blocks' counts (lif_grid + 1).
-
-__global__ void k_det_queue_keys(EngineDev eng, const uint32_t* prefix, unsigned long long* keys,
-                                 uint32_t* vals, uint32_t count) {
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= count) return;
-    const uint32_t qb = (uint32_t)(eng.ctl->step & 1ull);
-    const uint32_t reg = locate(prefix, eng.lif_grid, e);
-    const uint32_t qpos = reg * eng.region_cap + (e - prefix[reg]);
-    const SpikeRec r = (qb ? eng.queue[1] : eng.queue[0])[qpos];
-    keys[e] = ((unsigned long long)r.net << 32) | r.src;
-    vals[e] = qpos;
-}
-
-__global__ void k_det_row_sizes(EngineDev eng, const uint32_t* order, uint32_t count, uint32_t* sizes) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    const uint32_t qb = (uint32_t)(eng.ctl->step & 1ull);
-    const SpikeRec r = (qb ? eng.queue[1] : eng.queue[0])[order[k]];
-    const NetDev& n = eng.nets[r.net];
-    sizes[k] = (uint32_t)(n.row_ptr[r.src + 1] - n.row_ptr[r.src]);
-}
-
-// Raster records of the sorted queue; advances the raster position.
-__global__ void k_det_raster(EngineDev eng, const uint32_t* order, uint32_t count) {
-    const unsigned long long s = eng.ctl->step;
-    const uint32_t qb = (uint32_t)(s & 1ull);
-    const unsigned long long rbase = eng.ctl->raster_base;
-    const uint32_t* __restrict__ qid = qb ? eng.qid[1] : eng.qid[0];
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
-        if (eng.record && rbase + k < eng.raster_cap) eng.raster[rbase + k] = make_uint2((uint32_t)s, qid[order[k]]);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const unsigned long long cap = eng.record ? eng.raster_cap : 0ull;
-        const unsigned long long kept = rbase + count <= cap ? count : (rbase >= cap ? 0ull : cap - rbase);
-        eng.ctl->raster_next = rbase + kept;
-        if (eng.record && kept < count) eng.ctl->raster_dropped += count - kept;
-    }
-}
-
-__global__ void __launch_bounds__(kScatterThreads) k_det_emit(EngineDev eng, const uint32_t* order,
-                                                              uint32_t count, const uint32_t* offsets,
-                                                              unsigned long long* keys, float* vals) {
-    const unsigned long long s = eng.ctl->step;
-    const uint32_t qb = (uint32_t)(s & 1ull);
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    unsigned long long ev = 0;
-    uint32_t ovf = 0;
-    for (uint32_t k = warp; k < count; k += nwarps) {
-        const SpikeRec r = (qb ? eng.queue[1] : eng.queue[0])[order[k]];
-        const NetDev& n = eng.nets[r.net];
-        const uint32_t tl = (uint32_t)(s - n.start_step);
-        const uint32_t tmod = tl % n.ring_slots;
-        const uint64_t beg = n.row_ptr[r.src];
-        const uint64_t end = n.row_ptr[r.src + 1];
-        const bool plastic_src = n.stdp_on && r.src < n.n_plastic;
-        StdpView sv;
-        if (plastic_src) sv = stdp_view(n);
-        const float mult = (!plastic_src && r.aux0 > 1) ? (float)r.aux0 : 1.0f;
-        const uint32_t out0 = offsets[k];
-        for (uint64_t j = beg + lane; j < end; j += 32) {
-            const uint32_t tgt = n.tgt[j];
-            unsigned long long key = ~0ull;
-            float w = 0.0f;
-            if (tgt != kTgtSentinel) {
-                w = n.w[j];
-                if (plastic_src && tgt < n.n_plastic) {
-                    w = stdp_update(sv, w, tgt, (int32_t)tl, r.aux0, r.aux1, ovf);
-                    n.w[j] = w;
-                }
-                if (mult != 1.0f) w = __fmul_rn(w, mult);
-                key = n.ring_key_base +
-                      (unsigned long long)ring_slot(tmod, n.dly[j], n.ring_slots) * n.n_storage + tgt;
-                ++ev;
-            }
-            keys[out0 + (uint32_t)(j - beg)] = key;
-            vals[out0 + (uint32_t)(j - beg)] = w;
-        }
-    }
-    ev = warp_sum_u64(ev);
-    const unsigned long long ov = warp_sum_u64((unsigned long long)ovf);
-    if (lane == 0) {
-        if (ev) atomicAdd(&eng.ctl->events, ev);
-        if (ov) atomicAdd(&eng.ctl->stdp_hist_overflow, ov);
-    }
-}
-
-__global__ void k_det_fold(const NetDev* nets, uint32_t n_nets, const unsigned long long* keys,
-                           const float* vals, uint32_t count) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
-    const unsigned long long key = keys[i];
-    if (key == ~0ull) return;
-    if (i > 0 && keys[i - 1] == key) return;
-    float sum = vals[i];
-    for (uint32_t j = i + 1; j < count && keys[j] == key; ++j) sum = __fadd_rn(sum, vals[j]);
-    // net owning this key: last net whose ring_key_base <= key
-    uint32_t lo = 0, hi = n_nets;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (nets[mid].ring_key_base <= key) lo = mid; else hi = mid;
-    }
-    float* cell = nets[lo].ring + (key - nets[lo].ring_key_base);
-    *cell = __fadd_rn(*cell, sum);
-}
-
-// Advances the engine step after the deterministic aggregation.
-__global__ void k_advance(EngineDev eng) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) eng.ctl->step = eng.ctl->step + 1;
+size_t run_smem_bytes(uint32_t grid, uint32_t own_max, bool smem_state) {
+    const size_t off_cc = (((grid + 1) * sizeof(uint32_t)) + 15) & ~(size_t)15;
+    if (!smem_state) return off_cc;
+    const size_t off_v = off_cc + (((size_t)own_max * sizeof(ChunkCache) + 15) & ~(size_t)15);
+    return off_v + (size_t)own_max * kLifThreads * (sizeof(float4) + sizeof(uchar4));
 }
 
 }  // namespace naer

@@ -175,21 +175,21 @@ __device__ __forceinline__ uint32_t ring_slot(uint32_t t_mod, uint32_t d, uint32
 }
 
 // Kernels ---------------------------------------------------------------------
-__global__ void k_lif(EngineDev eng);
+// Persistent step kernels (cooperative launches of up to kDriveSlots grid
+// steps): k_step (atomic, one spike list per step, split scatter), k_run
+// (atomic, per-block spike regions, two barriers per step), k_det_step
+// (deterministic aggregation).  kSmem: neuron state in shared memory.
 template <bool kSmem>
 __global__ void k_run(EngineDev eng, unsigned long long s0, uint32_t nsteps);
+template <bool kSmem>
+__global__ void k_step(EngineDev eng, unsigned long long s0, uint32_t nsteps);
+template <bool kSmem>
+__global__ void k_det_step(EngineDev eng, unsigned long long s0, uint32_t nsteps);
 // dynamic shared memory of k_run for a grid and a number of owned chunks per block
 size_t run_smem_bytes(uint32_t grid, uint32_t own_max, bool smem_state);
-__global__ void k_advance(EngineDev eng);
+// dynamic shared memory of k_step / k_det_step for a number of owned chunks per block
+size_t step_smem_bytes(uint32_t own_max, bool smem_state);
+// Poisson counts of up to kDriveSlots steps ahead
 __global__ void k_drive(EngineDev eng, unsigned long long s_first, uint32_t nsteps);
-// deterministic aggregation
-__global__ void k_det_queue_keys(EngineDev eng, const uint32_t* prefix, unsigned long long* keys,
-                                 uint32_t* vals, uint32_t count);
-__global__ void k_det_row_sizes(EngineDev eng, const uint32_t* order, uint32_t count, uint32_t* sizes);
-__global__ void k_det_raster(EngineDev eng, const uint32_t* order, uint32_t count);
-__global__ void k_det_emit(EngineDev eng, const uint32_t* order, uint32_t count, const uint32_t* offsets,
-                           unsigned long long* keys, float* vals);
-__global__ void k_det_fold(const NetDev* nets, uint32_t n_nets, const unsigned long long* keys,
-                           const float* vals, uint32_t count);
 
 }  // namespace naer

@@ -706,10 +706,15 @@ int oracle_max_threads() {
 // (step, neuron) pairs where the double trajectory's threshold test
 // disagrees with the raster (V > V_th without a recorded spike, or a
 // recorded spike while refractory), a diagnostic only.
-int oracle_reintegrate_fp64(void* h, uint64_t nsteps, const uint32_t* sp_step, const uint32_t* sp_id, uint64_t nsp,
-                            double* v_out, double* w_out, uint64_t* mismatch) {
+// uncapped != 0: lazy LTP sees every post spike since the source's last
+// spike (the pair rule without the post-history limit the device and the
+// fp32 oracle share); *lost counts, with the limit, the pairs it drops.
+int oracle_reintegrate_fp64_ex(void* h, uint64_t nsteps, const uint32_t* sp_step, const uint32_t* sp_id, uint64_t nsp,
+                               double* v_out, double* w_out, uint64_t* mismatch, int uncapped, uint64_t* lost) {
     const Net& net = *static_cast<Net*>(h);
     const OrParams& P = net.prm;
+    std::vector<std::vector<int32_t>> posts;  // every post spike, oldest first (uncapped)
+    uint64_t dropped = 0;
     const uint32_t n = net.n, D = net.D;
     std::vector<double> v(n, 0.0), ring((size_t)D * n, 0.0), w(net.w.begin(), net.w.end());
     std::vector<uint32_t> refr(n, 0);
@@ -774,6 +779,8 @@ int oracle_reintegrate_fp64(void* h, uint64_t nsteps, const uint32_t* sp_step, c
                     int32_t* hh = &hist[(size_t)i * P.stdp_history];
                     for (int q = (int)P.stdp_history - 1; q > 0; --q) hh[q] = hh[q - 1];
                     hh[0] = ts;
+                    if (posts.empty()) posts.resize(n);
+                    posts[i].push_back(ts);
                 }
             } else if (x > (double)pop.v_th) {
                 ++mis;
@@ -806,11 +813,16 @@ int oracle_reintegrate_fp64(void* h, uint64_t nsteps, const uint32_t* sp_step, c
                 double wv = w[j];
                 if (src_plastic && net.kind[tg] == 0) {
                     if (pre_last[a] >= 0) {
-                        const int32_t* hh = &hist[(size_t)tg * P.stdp_history];
-                        uint32_t c = 0;
-                        while (c < P.stdp_history && hh[c] > pre_last[a]) ++c;
-                        for (int q = (int)c - 1; q >= 0; --q) {
-                            const double xx = pre_x[a] * std::exp(-(double)(hh[q] - pre_last[a]) * P.dt_us / tau_p);
+                        // post spikes in (pre_last, t], oldest first
+                        static const std::vector<int32_t> none;
+                        const std::vector<int32_t>& all = posts.empty() ? none : posts[tg];
+                        size_t first = all.size();
+                        while (first > 0 && all[first - 1] > pre_last[a]) --first;
+                        const size_t avail = all.size() - first;
+                        const size_t keep = std::min<size_t>(avail, P.stdp_history);
+                        dropped += avail - keep;
+                        for (size_t q = uncapped ? first : all.size() - keep; q < all.size(); ++q) {
+                            const double xx = pre_x[a] * std::exp(-(double)(all[q] - pre_last[a]) * P.dt_us / tau_p);
                             wv = std::min(wv + ap * xx, wmax);
                         }
                     }
@@ -831,7 +843,13 @@ int oracle_reintegrate_fp64(void* h, uint64_t nsteps, const uint32_t* sp_step, c
     if (v_out) std::copy(v.begin(), v.end(), v_out);
     if (w_out) std::copy(w.begin(), w.end(), w_out);
     if (mismatch) *mismatch = mis;
+    if (lost) *lost = dropped;
     return 0;
+}
+
+int oracle_reintegrate_fp64(void* h, uint64_t nsteps, const uint32_t* sp_step, const uint32_t* sp_id, uint64_t nsp,
+                            double* v_out, double* w_out, uint64_t* mismatch) {
+    return oracle_reintegrate_fp64_ex(h, nsteps, sp_step, sp_id, nsp, v_out, w_out, mismatch, 0, nullptr);
 }
 
 // ---------------------------------------------------------------------------

@@ -82,6 +82,8 @@ def load() -> C.CDLL:
             "oracle_max_threads": (C.c_int, []),
             "oracle_reintegrate_fp64": (C.c_int, [_vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp, _vp,
                                                   C.POINTER(C.c_uint64)]),
+            "oracle_reintegrate_fp64_ex": (C.c_int, [_vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp, _vp,
+                                                     C.POINTER(C.c_uint64), C.c_int, C.POINTER(C.c_uint64)]),
             "oracle_net_run_events": (C.c_int, [_vp, C.c_uint64, C.c_uint32]),
             "oracle_net_event_spike_count": (C.c_uint64, [_vp]),
             "oracle_net_event_copy": (None, [_vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
@@ -231,6 +233,21 @@ class OracleNet:
         self._lib.oracle_reintegrate_fp64(self._h, int(nsteps), _ptr(st), _ptr(ii), len(st), _ptr(v), _ptr(w),
                                           C.byref(mis))
         return v, w, mis.value
+
+    def reintegrate_fp64_uncapped(self, steps: np.ndarray, ids: np.ndarray, nsteps: int):
+        """reintegrate_fp64 with lazy LTP over every post spike since the
+        source's last spike (no post-history limit): the pair rule itself.
+        Returns (V, weights, threshold mismatches, pairs the history limit
+        drops on these spike times)."""
+        st = np.ascontiguousarray(steps, dtype=np.uint32)
+        ii = np.ascontiguousarray(ids, dtype=np.uint32)
+        v = np.empty(self.n, dtype=np.float64)
+        w = np.empty(self.S, dtype=np.float64)
+        mis = C.c_uint64()
+        lost = C.c_uint64()
+        self._lib.oracle_reintegrate_fp64_ex(self._h, int(nsteps), _ptr(st), _ptr(ii), len(st), _ptr(v), _ptr(w),
+                                             C.byref(mis), 1, C.byref(lost))
+        return v, w, mis.value, lost.value
 
 
 def max_threads() -> int:

@@ -125,7 +125,8 @@ def test_roofline_workload_statistics(O):
 def test_plastic_workload_fp64(O):
     """100k LIF, fixed in-degree 1,000 (1e8 synapses), delays 1-20, pair
     STDP on E->E, 1,000 steps: membrane potentials and weights within 1e-5
-    of the FP64 re-integration of the same spike inputs."""
+    of the FP64 re-integration of the same spike inputs, with lazy LTP over
+    every post spike (no history limit)."""
     s = S.plastic_indegree(n=100_000, k=1000)
     steps = 1000
     with S.build(s) as net:
@@ -136,8 +137,11 @@ def test_plastic_workload_fp64(O):
         _, _, w, _ = net.read_csr()
     assert len(ids) > 10_000
     o = O.OracleNet(s)
-    v64, w64, _ = o.reintegrate_fp64(st, ids, steps)
+    # against the pair rule itself: every post spike since the source's last
+    # spike, no history limit (the limit drops no pair on this run)
+    v64, w64, _, lost = o.reintegrate_fp64_uncapped(st, ids, steps)
     o.close()
+    assert lost == 0
     for x32, x64, floor in [(v, v64, 1.0), (w, w64, 1e-3 * s.w_max)]:
         x64 = np.asarray(x64, dtype=np.float64)
         err = np.abs(np.asarray(x32, dtype=np.float64) - x64) / np.maximum(np.abs(x64), floor)

@@ -271,6 +271,30 @@ def test_oracle_fp32_within_fp64_reintegration(oracle_mod, make, steps):
     assert mismatch == 0
 
 
+def test_fp64_uncapped_history(oracle_mod):
+    O = oracle_mod
+    """The uncapped re-integration (every post spike since the source's last
+    spike) equals the capped one when the cap drops nothing, and departs
+    from it when a one-entry history drops pairs."""
+    s = S.plastic_indegree(n=1500, k=150, drive_weight=21.0, drive_rate_hz=20.0).with_(stdp_history=16)
+    steps = 1200
+    o = O.OracleNet(s)
+    o.run(steps)
+    st, ids = o.spikes()
+    v64, w64, _ = O.OracleNet(s).reintegrate_fp64(st, ids, steps)
+    u64, uw64, _, lost = O.OracleNet(s).reintegrate_fp64_uncapped(st, ids, steps)
+    assert lost == 0
+    assert np.array_equal(v64, u64) and np.array_equal(w64, uw64)
+    s1 = s.with_(stdp_history=1)
+    o1 = O.OracleNet(s1)
+    o1.run(steps)
+    st1, ids1 = o1.spikes()
+    _, cw, _ = O.OracleNet(s1).reintegrate_fp64(st1, ids1, steps)
+    _, uw, _, lost1 = O.OracleNet(s1).reintegrate_fp64_uncapped(st1, ids1, steps)
+    assert lost1 > 0
+    assert not np.array_equal(cw, uw) and (uw >= cw - 1e-12).all()  # dropped pairs are potentiation only
+
+
 # Reference-compatible event mode (oracle only): the `.cl` kernels' time model.
 
 def _lif_event_model(times, w, tau_ms, v_th, v_reset, t_ref_ms):

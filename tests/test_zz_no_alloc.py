@@ -58,10 +58,10 @@ def test_noalloc_matches_step_on_two_calls(lib, name, make, plastic):
 
 
 def test_noalloc_rejects_oversize_before_stepping(lib):
-    """1.6 M padded synapses need more than the 32 MiB arena: refused with
-    NAER_E_OVERFLOW and the network's state untouched; naer_net_step still
-    runs it."""
-    s = S.scatter_outdegree(n=4000, k=400, drive_weight=24.0).with_(deterministic=True)
+    """4.8 M padded synapses (8 B of scratch each) need more than the 32 MiB
+    arena: refused with NAER_E_OVERFLOW and the network's state untouched;
+    naer_net_step still runs it."""
+    s = S.scatter_outdegree(n=12000, k=400, drive_weight=24.0).with_(deterministic=True)
     with S.build(s) as net:
         assert step_noalloc(net, 5) == capi.NAER_E_OVERFLOW
         assert "fixed arena holds 33554432 bytes" in capi.last_error()
