@@ -199,9 +199,11 @@ def run_reference(args):
     threads = O.max_threads()
     o = O.OracleNet(spec, threads=threads, deterministic=False)
     o.run(args.cpu_warmup)
-    per_step = max(10, args.cpu_steps // max(1, args.steps))
+    # one bench step is the same work as on the GPU arm: args.chunk grid
+    # steps (100 ms simulated), so ms_per_step compares like with like
+    per_step = args.chunk
     for _ in range(args.warmup):
-        o.run(max(1, per_step // 4))
+        o.run(max(1, per_step // 10))
     e0 = o.events
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -215,8 +217,9 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": workload_config(args, int(o.S)),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"each step {per_step} grid steps of the same network on the host cores "
-                                   f"(the reference's OpenCL kernels cannot run here: no OpenCL runtime)"},
+                         "sample": f"each step {per_step} grid steps ({per_step * 0.1:.0f} ms simulated) of the same "
+                                   f"network on the host cores, as one step of the GPU arm (the reference's OpenCL "
+                                   f"kernels cannot run here: no OpenCL runtime)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -130,6 +130,20 @@ public:
         return n;
     }
 
+    // Recorded spikes (no counterpart in the reference, which never reads
+    // spikes back): grid steps and reference addresses, grouped by step,
+    // ascending address within a step.  Blocks.
+    void readSpikes(std::vector<uint32_t>& steps, std::vector<uint32_t>& addresses) {
+        naer_stats st{};
+        check(naer_net_get_stats(m_net, &st));
+        steps.resize(st.spikes);
+        addresses.resize(st.spikes);
+        uint64_t n = 0;
+        if (st.spikes) check(naer_net_read_spikes(m_net, 0, st.spikes, steps.data(), addresses.data(), &n));
+        steps.resize(n);
+        addresses.resize(n);
+    }
+
     // Per-kernel device time (s) while profiling is enabled (Network.h:50-55).
     void setProfiling(bool on) { check(naer_net_set_profiling(m_net, on ? 1 : 0)); }
     void readProfile() {

@@ -72,6 +72,7 @@ extern "C" {
 #define NAER_CONN_REF_BERNOULLI 0u
 #define NAER_CONN_FIXED_INDEGREE 1u
 #define NAER_CONN_FIXED_OUTDEGREE 2u
+#define NAER_CONN_EXPLICIT 3u  /* synapses given by naer_net_add_connection_csr */
 
 /* ---- parameter blocks ------------------------------------------------- */
 typedef struct naer_net_params {
@@ -162,6 +163,19 @@ NAER_API int naer_net_add_population(naer_net* net, uint32_t neuron_type, uint32
 NAER_API int naer_net_add_connection(naer_net* net, uint32_t src_pop, uint32_t dst_pop,
                                      const naer_conn_spec* spec);
 
+/* Connectivity given explicitly (no counterpart in the reference, whose
+ * only generator is include/naer/kernels/network.cl:14-107): the synapses
+ * from population src_pop to population dst_pop as a CSR over the source
+ * population.  row_ptr has src_size + 1 entries (row_ptr[0] = 0, rows in
+ * source order); per synapse: the target's index within the destination
+ * population, its weight and its delay in grid steps (1..254).  The arrays
+ * are copied; each row keeps the given synapse order (then, like every
+ * row, a stable split puts its delay-1 synapses first).  Explicit and
+ * rule-generated connections can be mixed; rows concatenate in the order
+ * the connections were added. */
+NAER_API int naer_net_add_connection_csr(naer_net* net, uint32_t src_pop, uint32_t dst_pop, const uint64_t* row_ptr,
+                                         const uint32_t* targets, const float* weights, const uint8_t* delays);
+
 /* Network::compile (Network.cpp:267-308): address layout, device buffers,
  * connectivity generated on the device. */
 NAER_API int naer_net_compile(naer_net* net);
@@ -251,6 +265,24 @@ NAER_API int naer_net_get_phases(naer_net* net, double* phase_ms5);
 NAER_API int naer_net_get_launch_times(naer_net* net, double* drive_ms, double* step_kernel_ms,
                                        uint64_t* step_kernel_launches);
 
+/* Checkpoint and restore (no counterpart in the reference, whose state
+ * lives only in its OpenCL buffers, src/Network.cpp:379-569).  A checkpoint
+ * is the network's whole simulation state between steps: the step counter,
+ * the event counter, membrane potentials, refractory counters, the delay
+ * ring (inputs already on their way), and with plasticity the weights and
+ * the pre/post traces and post-spike history.  Connectivity is not stored:
+ * it is regenerated bit for bit from the same description at compile, and
+ * the Poisson input follows from the step counter.
+ * naer_net_checkpoint blocks until the queued steps end and writes
+ * checkpoint_size bytes into buf.  naer_net_restore loads a checkpoint into
+ * a compiled network built from the same description (NAER_E_INVALID when
+ * its layout differs); stepping continues from the saved step, and a
+ * deterministic network then produces the raster and state of the
+ * uninterrupted run bit for bit.  The raster restarts empty. */
+NAER_API int naer_net_checkpoint_size(naer_net* net, uint64_t* bytes);
+NAER_API int naer_net_checkpoint(naer_net* net, void* buf, uint64_t capacity);
+NAER_API int naer_net_restore(naer_net* net, const void* buf, uint64_t size);
+
 /* Bounded device waits (no counterpart in the reference, whose OpenCL
  * queue has none).  Every grid barrier of the step kernel gives up after
  * limit_us microseconds (default 2 s), records NAER_E_TIMEOUT on the device
@@ -265,6 +297,13 @@ NAER_API int naer_net_set_wait_limit(naer_net* net, uint64_t limit_us);
  * after the limit above; the kernel then returns normally with the error
  * recorded.  Nothing else changes on the device.  0 = normal operation. */
 NAER_API int naer_test_set_barrier_skew(naer_net* net, uint64_t skew);
+
+/* Fault injection for tests (no counterpart in the reference): the device
+ * allocation `after` allocations from now (0 = the next one, in any handle
+ * of this process) fails as if the device were out of memory, once; -1
+ * turns it off.  The call that hits it returns NAER_E_OOM and releases
+ * whatever it had allocated. */
+NAER_API int naer_test_fail_allocation(int64_t after);
 
 /* ---- device probe ------------------------------------------------------
  * No counterpart in the reference.  Measures, on `device`, the ceilings the
@@ -395,10 +434,11 @@ typedef struct naer_server_params {
 #define NAER_JOB_RUNNING 1u
 #define NAER_JOB_DONE 2u
 #define NAER_JOB_FAILED 3u
+#define NAER_JOB_CANCELLED 4u
 
 typedef struct naer_job_info {
     uint32_t state;            /* NAER_JOB_* */
-    uint32_t pad_;
+    uint32_t preemptions;      /* times the job was pre-empted and resumed */
     uint64_t duration;         /* grid steps asked for */
     uint64_t steps_done;
     uint64_t spikes;           /* raster records of the job (when done) */
@@ -436,6 +476,17 @@ NAER_API int naer_server_read_spikes(naer_server* server, uint64_t job, uint64_t
                                      uint64_t* count);
 /* Forgets a finished job and its raster. */
 NAER_API int naer_server_release(naer_server* server, uint64_t job);
+/* Pre-emption: takes a running job off the device at the next chunk
+ * boundary (NAER_E_STATE if it is not running).  Its whole simulation state
+ * (as naer_net_checkpoint) moves to host memory, its device memory is freed
+ * and it queues again; when re-admitted it is rebuilt, restored and
+ * continues from the step it reached, so a deterministic job's raster
+ * equals its uninterrupted run. */
+NAER_API int naer_server_preempt(naer_server* server, uint64_t job);
+/* Cancels a job that has not ended: a queued or built job at once, a
+ * running job at the next chunk boundary.  It ends in NAER_JOB_CANCELLED
+ * and its raster is discarded.  NAER_E_STATE if it already ended. */
+NAER_API int naer_server_cancel(naer_server* server, uint64_t job);
 NAER_API int naer_server_get_stats(naer_server* server, naer_server_stats* st);
 
 #ifdef __cplusplus

@@ -34,7 +34,7 @@ STATUS_NAMES = {
 NEURON_STDP, NEURON_NOP, NEURON_POISSON = 0, 1, 2
 MODE_GRID, MODE_EVENT = 0, 1
 AGG_ATOMIC, AGG_DETERMINISTIC = 0, 1
-CONN_REF_BERNOULLI, CONN_FIXED_INDEGREE, CONN_FIXED_OUTDEGREE = 0, 1, 2
+CONN_REF_BERNOULLI, CONN_FIXED_INDEGREE, CONN_FIXED_OUTDEGREE, CONN_EXPLICIT = 0, 1, 2, 3
 
 
 class NetParams(C.Structure):
@@ -148,13 +148,13 @@ class DeviceProbe(C.Structure):
     ]
 
 
-JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
 
 
 class JobInfo(C.Structure):
     _fields_ = [
         ("state", C.c_uint32),
-        ("pad_", C.c_uint32),
+        ("preemptions", C.c_uint32),
         ("duration", C.c_uint64),
         ("steps_done", C.c_uint64),
         ("spikes", C.c_uint64),
@@ -193,6 +193,7 @@ PROTOTYPES = {
     "naer_net_destroy": [_vp],
     "naer_net_add_population": [_vp, C.c_uint32, C.c_uint32, _P(PopParams), _P(C.c_uint32), _P(C.c_uint32)],
     "naer_net_add_connection": [_vp, C.c_uint32, C.c_uint32, _P(ConnSpecC)],
+    "naer_net_add_connection_csr": [_vp, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp],
     "naer_net_compile": [_vp],
     "naer_net_population_base": [_vp, C.c_uint32, _P(C.c_uint32)],
     "naer_net_step": [_vp, C.c_uint64],
@@ -215,6 +216,7 @@ PROTOTYPES = {
     "naer_net_get_launch_times": [_vp, _P(C.c_double), _P(C.c_double), _P(C.c_uint64)],
     "naer_net_set_wait_limit": [_vp, C.c_uint64],
     "naer_test_set_barrier_skew": [_vp, C.c_uint64],
+    "naer_test_fail_allocation": [C.c_int64],
     "naer_probe_device": [C.c_int, C.c_uint64, C.c_uint64, _P(DeviceProbe)],
     "naer_net_autotune": [_vp, C.c_uint32, _P(Tuning)],
     "naer_net_set_tuning": [_vp, _P(Tuning)],
@@ -243,6 +245,11 @@ PROTOTYPES = {
     "naer_server_drain": [_vp, C.c_double, _P(C.c_int)],
     "naer_server_read_spikes": [_vp, C.c_uint64, C.c_uint64, C.c_uint64, _vp, _vp, _P(C.c_uint64)],
     "naer_server_release": [_vp, C.c_uint64],
+    "naer_server_preempt": [_vp, C.c_uint64],
+    "naer_server_cancel": [_vp, C.c_uint64],
+    "naer_net_checkpoint_size": [_vp, _P(C.c_uint64)],
+    "naer_net_checkpoint": [_vp, _vp, C.c_uint64],
+    "naer_net_restore": [_vp, _vp, C.c_uint64],
     "naer_server_get_stats": [_vp, _P(ServerStats)],
 }
 

@@ -176,6 +176,22 @@ __global__ void k_row_pad(const uint64_t* len, uint32_t n, uint64_t* padded) {
         padded[i] = i < n ? (len[i] + (kRowAlign - 1)) / kRowAlign * kRowAlign : 0ull;
 }
 
+// Explicit connectivity: one warp per source row copies its synapses, in
+// the given order, to the row's cursor (targets shifted to storage indices).
+__global__ void k_explicit_fill(ConnBuild cb, const uint64_t* rp, const uint32_t* tg, const float* wv,
+                                const uint8_t* dv, const uint64_t* cursor, uint32_t* tgt, float* w, uint8_t* dly) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < cb.src_size; s += nw) {
+        const uint64_t b = rp[s], e = rp[s + 1], o = cursor[cb.src_storage + s];
+        for (uint64_t j = b + lane; j < e; j += 32) {
+            tgt[o + (j - b)] = cb.dst_storage + tg[j];
+            w[o + (j - b)] = wv[j];
+            dly[o + (j - b)] = dv[j];
+        }
+    }
+}
+
 __global__ void k_cursor_advance(const uint32_t* cnt, uint32_t src_size, uint32_t src_storage,
                                  uint64_t* cursor) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < src_size; s += gridDim.x * blockDim.x)

@@ -72,6 +72,8 @@ __global__ void k_indeg_count(ConnBuild cb, uint32_t* cnt);
 __global__ void k_row_stats(const uint64_t* len, const uint64_t* padded, const uint32_t* n1, uint32_t n,
                             unsigned long long* out);
 __global__ void k_indeg_keys(ConnBuild cb, uint32_t* keys, uint32_t* vals);
+__global__ void k_explicit_fill(ConnBuild cb, const uint64_t* rp, const uint32_t* tg, const float* wv,
+                                const uint8_t* dv, const uint64_t* cursor, uint32_t* tgt, float* w, uint8_t* dly);
 __global__ void k_indeg_finalize(ConnBuild cb, const uint32_t* keys, const uint32_t* vals, uint64_t total,
                                  const uint64_t* conn_off, const uint64_t* cursor, uint32_t* tgt,
                                  float* w, uint8_t* dly);

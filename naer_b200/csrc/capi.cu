@@ -1,4 +1,5 @@
 // extern "C" boundary: every entry point of include/naer/naer_capi.h.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -171,11 +172,50 @@ int naer_net_add_connection(naer_net* net, uint32_t src_pop, uint32_t dst_pop,
         need(!net->net.compiled, NAER_E_STATE, "network already compiled");
         need(src_pop < net->net.pops.size() && dst_pop < net->net.pops.size(), NAER_E_INVALID,
              "unknown population");
+        need(spec->rule != NAER_CONN_EXPLICIT, NAER_E_INVALID,
+             "explicit connectivity is added with naer_net_add_connection_csr");
         naer::ConnSpec c;
         c.src = src_pop;
         c.dst = dst_pop;
         c.spec = *spec;
         net->net.conns.push_back(c);
+    });
+}
+
+int naer_net_add_connection_csr(naer_net* net, uint32_t src_pop, uint32_t dst_pop, const uint64_t* row_ptr,
+                                const uint32_t* targets, const float* weights, const uint8_t* delays) {
+    return guarded([&] {
+        need(net != nullptr && row_ptr != nullptr, NAER_E_INVALID, "null argument");
+        need(!net->net.compiled, NAER_E_STATE, "network already compiled");
+        need(src_pop < net->net.pops.size() && dst_pop < net->net.pops.size(), NAER_E_INVALID,
+             "unknown population");
+        const uint32_t ns = net->net.pops[src_pop].size, nd = net->net.pops[dst_pop].size;
+        need(row_ptr[0] == 0, NAER_E_INVALID, "row_ptr[0] must be 0");
+        for (uint32_t r = 0; r < ns; ++r)
+            need(row_ptr[r + 1] >= row_ptr[r], NAER_E_INVALID, "row_ptr must not decrease");
+        const uint64_t nnz = row_ptr[ns];
+        need(nnz == 0 || (targets && weights && delays), NAER_E_INVALID, "null synapse arrays");
+        need(nnz < (1ull << 40), NAER_E_INVALID, "too many synapses");
+        auto x = std::make_shared<naer::ExplicitCsr>();
+        x->row_ptr.assign(row_ptr, row_ptr + ns + 1);
+        x->tgt.assign(targets, targets + nnz);
+        x->w.assign(weights, weights + nnz);
+        x->dly.assign(delays, delays + nnz);
+        uint32_t dmin = 254, dmax = 1;
+        for (uint64_t j = 0; j < nnz; ++j) {
+            need(x->tgt[j] < nd, NAER_E_INVALID, "target index outside the destination population");
+            need(x->dly[j] >= 1 && x->dly[j] <= 254, NAER_E_INVALID, "delays must be in 1..254 steps");
+            dmin = std::min<uint32_t>(dmin, x->dly[j]);
+            dmax = std::max<uint32_t>(dmax, x->dly[j]);
+        }
+        naer::ConnSpec c;
+        c.src = src_pop;
+        c.dst = dst_pop;
+        c.spec.rule = NAER_CONN_EXPLICIT;
+        c.spec.delay_min = nnz ? dmin : 1;
+        c.spec.delay_max = nnz ? dmax : 1;
+        c.csr = std::move(x);
+        net->net.conns.push_back(std::move(c));
     });
 }
 
@@ -187,7 +227,12 @@ int naer_net_compile(naer_net* net) {
              "description-only network (device -1): add it to a batch or submit it to a server");
         net->eng->build(net->net);
         const auto& P = net->net.params;
-        net->eng->install({&net->net}, P.raster_capacity, P.record_spikes != 0, P.aggregation);
+        try {
+            net->eng->install({&net->net}, P.raster_capacity, P.record_spikes != 0, P.aggregation);
+        } catch (...) {
+            net->eng->free_net(net->net);  // compile either completes or leaves nothing built
+            throw;
+        }
     });
 }
 
@@ -231,6 +276,80 @@ int naer_net_finish(naer_net* net) {
     });
 }
 
+namespace {
+// Header of a checkpoint: the layout it was taken from (checked on restore)
+// and the counters it restores.
+struct CheckpointHeader {
+    char magic[8];
+    uint32_t version, stdp_on;
+    uint64_t step, events, payload;
+    uint64_t synapses, synapses_padded;
+    uint32_t n_ids, n_storage, ring_slots, n_plastic, post_stride, dt_us;
+};
+constexpr char kCheckpointMagic[8] = {'N', 'A', 'E', 'R', 'C', 'K', 'P', 'T'};
+
+CheckpointHeader checkpoint_header(naer::Engine& eng, const naer::NetHost& n) {
+    CheckpointHeader h{};
+    std::memcpy(h.magic, kCheckpointMagic, 8);
+    h.version = 1;
+    h.stdp_on = n.dev.stdp_on;
+    h.step = eng.host_step();
+    h.events = eng.events_total();
+    h.payload = naer::state_bytes(n);
+    h.synapses = n.synapses;
+    h.synapses_padded = n.synapses_padded;
+    h.n_ids = n.n_ids;
+    h.n_storage = n.n_storage;
+    h.ring_slots = n.ring_slots;
+    h.n_plastic = n.dev.stdp_on ? n.n_plastic : 0;
+    h.post_stride = n.post_stride;
+    h.dt_us = n.params.dt_us;
+    return h;
+}
+}  // namespace
+
+int naer_net_checkpoint_size(naer_net* net, uint64_t* bytes) {
+    return guarded([&] {
+        need_compiled(net);
+        need(bytes != nullptr, NAER_E_INVALID, "null argument");
+        *bytes = sizeof(CheckpointHeader) + naer::state_bytes(net->net);
+    });
+}
+
+int naer_net_checkpoint(naer_net* net, void* buf, uint64_t capacity) {
+    return guarded([&] {
+        need_compiled(net);
+        need(buf != nullptr, NAER_E_INVALID, "null buffer");
+        need(capacity >= sizeof(CheckpointHeader) + naer::state_bytes(net->net), NAER_E_OVERFLOW,
+             "buffer smaller than naer_net_checkpoint_size");
+        net->eng->sync();
+        throw_device_status(*net->eng);
+        const CheckpointHeader h = checkpoint_header(*net->eng, net->net);
+        std::memcpy(buf, &h, sizeof(h));
+        net->eng->save_state(net->net, static_cast<uint8_t*>(buf) + sizeof(h));
+    });
+}
+
+int naer_net_restore(naer_net* net, const void* buf, uint64_t size) {
+    return guarded([&] {
+        need_compiled(net);
+        need(buf != nullptr && size >= sizeof(CheckpointHeader), NAER_E_INVALID, "not a checkpoint");
+        CheckpointHeader h;
+        std::memcpy(&h, buf, sizeof(h));
+        need(std::memcmp(h.magic, kCheckpointMagic, 8) == 0 && h.version == 1, NAER_E_INVALID, "not a checkpoint");
+        net->eng->sync();
+        const CheckpointHeader mine = checkpoint_header(*net->eng, net->net);
+        need(h.stdp_on == mine.stdp_on && h.payload == mine.payload && h.synapses == mine.synapses &&
+                 h.synapses_padded == mine.synapses_padded && h.n_ids == mine.n_ids &&
+                 h.n_storage == mine.n_storage && h.ring_slots == mine.ring_slots &&
+                 h.n_plastic == mine.n_plastic && h.post_stride == mine.post_stride && h.dt_us == mine.dt_us,
+             NAER_E_INVALID, "checkpoint was taken from a network of another layout");
+        need(size >= sizeof(h) + h.payload, NAER_E_INVALID, "checkpoint truncated");
+        net->eng->load_state(net->net, static_cast<const uint8_t*>(buf) + sizeof(h));
+        net->eng->set_step(h.step, h.events);
+    });
+}
+
 int naer_net_set_wait_limit(naer_net* net, uint64_t limit_us) {
     return guarded([&] {
         need_compiled(net);
@@ -243,6 +362,13 @@ int naer_test_set_barrier_skew(naer_net* net, uint64_t skew) {
     return guarded([&] {
         need_compiled(net);
         net->eng->set_barrier_skew(skew);
+    });
+}
+
+int naer_test_fail_allocation(int64_t after) {
+    return guarded([&] {
+        need(after >= -1, NAER_E_INVALID, "after must be >= -1");
+        naer::set_allocation_failure(after);
     });
 }
 
@@ -694,6 +820,7 @@ int naer_server_job_info(naer_server* server, uint64_t job, naer_job_info* info)
         const naer::JobInfo j = server->s->info(job);
         std::memset(info, 0, sizeof(*info));
         info->state = j.state;
+        info->preemptions = j.preemptions;
         info->duration = j.duration;
         info->steps_done = j.steps_done;
         info->spikes = j.spikes;
@@ -742,6 +869,20 @@ int naer_server_release(naer_server* server, uint64_t job) {
     return guarded([&] {
         need(server != nullptr, NAER_E_INVALID, "null server handle");
         server->s->release(job);
+    });
+}
+
+int naer_server_preempt(naer_server* server, uint64_t job) {
+    return guarded([&] {
+        need(server != nullptr, NAER_E_INVALID, "null server handle");
+        server->s->preempt(job);
+    });
+}
+
+int naer_server_cancel(naer_server* server, uint64_t job) {
+    return guarded([&] {
+        need(server != nullptr, NAER_E_INVALID, "null server handle");
+        server->s->cancel(job);
     });
 }
 

@@ -1,6 +1,7 @@
 // Host engine implementation.
 #include <cub/cub.cuh>
 
+#include <atomic>
 #include <mutex>
 
 #include <algorithm>
@@ -156,10 +157,23 @@ Engine::~Engine() {
 // (every engine entry point that hands memory elsewhere synchronises);
 // dfree is ordered after the work already queued on this stream (callers
 // free memory only when no other stream still uses it).
+namespace {
+// Fault injection for tests (naer_test_fail_allocation): the allocation
+// this many allocations from now fails as an out-of-memory would; -1 = off.
+std::atomic<int64_t> g_alloc_fail_after{-1};
+}  // namespace
+
+void set_allocation_failure(int64_t after) { g_alloc_fail_after.store(after); }
+
 void* Engine::dalloc(size_t bytes) {
+    int64_t left = g_alloc_fail_after.load();
+    while (left >= 0 && !g_alloc_fail_after.compare_exchange_weak(left, left - 1)) {
+    }
+    if (left == 0) throw Error(NAER_E_OOM, "injected allocation failure (test hook)");
     void* p = nullptr;
     NAER_CK(cudaMallocAsync(&p, bytes ? bytes : 16, stream_));
     bytes_ += bytes;
+    if (alloc_log_) alloc_log_->push_back({p, bytes});
     return p;
 }
 
@@ -167,6 +181,9 @@ void Engine::dfree(void* p, size_t bytes) {
     if (!p) return;
     NAER_CK(cudaFreeAsync(p, stream_));
     bytes_ -= std::min<uint64_t>(bytes_, bytes);
+    if (alloc_log_)
+        for (auto& e : *alloc_log_)
+            if (e.first == p) e.first = nullptr;
 }
 
 // ---------------------------------------------------------------------------
@@ -208,7 +225,8 @@ static void layout(NetHost& n) {
             throw Error(NAER_E_INVALID, "connection refers to an unknown population");
         if (n.pops[c.dst].type == kPOISSON)
             throw Error(NAER_E_INVALID, "POISSON populations cannot receive connections");
-        if (sp.rule > NAER_CONN_FIXED_OUTDEGREE) throw Error(NAER_E_INVALID, "unknown connection rule");
+        if (sp.rule > NAER_CONN_EXPLICIT || (sp.rule == NAER_CONN_EXPLICIT) != (c.csr != nullptr))
+            throw Error(NAER_E_INVALID, "unknown connection rule");
         if (sp.delay_min < 1 || sp.delay_max < sp.delay_min || sp.delay_max > 254)
             throw Error(NAER_E_INVALID, "delays must satisfy 1 <= delay_min <= delay_max <= 254");
         if (sp.rule == NAER_CONN_REF_BERNOULLI && !(sp.probability >= 0.0 && sp.probability <= 1.0))
@@ -288,6 +306,8 @@ uint64_t estimate_device_bytes(const NetHost& description) {
             syn += m + 6.0 * std::sqrt(std::max(m, 1.0));
         } else if (sp.rule == NAER_CONN_FIXED_OUTDEGREE) {
             syn += (double)sp.degree * src;
+        } else if (sp.rule == NAER_CONN_EXPLICIT) {
+            syn += (double)c.csr->tgt.size();
         } else {
             syn += (double)sp.degree * dst;
         }
@@ -328,6 +348,36 @@ static ConnBuild make_cb(const NetHost& n, const ConnSpec& c) {
 
 void Engine::build(NetHost& n) {
     DeviceGuard g(device_);
+    // every allocation of the build is logged, so that a build that fails
+    // part way (an allocation, a launch) leaves no device memory behind
+    std::vector<std::pair<void*, size_t>> log;
+    alloc_log_ = &log;
+    try {
+        build_arrays(n);
+    } catch (...) {
+        alloc_log_ = nullptr;
+        cudaStreamSynchronize(stream_);
+        for (auto& e : log)
+            if (e.first) dfree(e.first, e.second);
+        n.v = nullptr;
+        n.refr = nullptr;
+        n.ring = nullptr;
+        n.drive = nullptr;
+        n.row_ptr = nullptr;
+        n.row_mid = nullptr;
+        n.tgt = nullptr;
+        n.w = nullptr;
+        n.dly = nullptr;
+        n.post = nullptr;
+        n.pre = nullptr;
+        n.e_plus = n.e_minus = nullptr;
+        n.compiled = false;
+        throw;
+    }
+    alloc_log_ = nullptr;
+}
+
+void Engine::build_arrays(NetHost& n) {
     layout(n);
     const uint32_t Ns = n.n_storage;
     const uint32_t T = 256;
@@ -348,6 +398,12 @@ void Engine::build(NetHost& n) {
         if (cb.src_size == 0 || cb.dst_size == 0) continue;
         if (cb.rule == NAER_CONN_REF_BERNOULLI) {
             k_bern_count<<<grid_for((uint64_t)cb.src_size * 32, T, maxb), T, 0, st>>>(cb, cnt[ci]);
+        } else if (cb.rule == NAER_CONN_EXPLICIT) {
+            const ExplicitCsr& x = *n.conns[ci].csr;
+            std::vector<uint32_t> lens(cb.src_size);
+            for (uint32_t r = 0; r < cb.src_size; ++r) lens[r] = (uint32_t)(x.row_ptr[r + 1] - x.row_ptr[r]);
+            NAER_CK(cudaMemcpyAsync(cnt[ci], lens.data(), cb.src_size * 4ull, cudaMemcpyHostToDevice, st));
+            NAER_CK(cudaStreamSynchronize(st));  // lens is pageable and local
         } else if (cb.rule == NAER_CONN_FIXED_OUTDEGREE) {
             k_fill_u32<<<grid_for(cb.src_size, T, maxb), T, 0, st>>>(cnt[ci], cb.src_size, cb.K);
         } else {
@@ -367,6 +423,7 @@ void Engine::build(NetHost& n) {
     for (const auto& c : n.conns) {
         const auto& sp = c.spec;
         if (sp.rule == NAER_CONN_REF_BERNOULLI) exact = false;
+        else if (sp.rule == NAER_CONN_EXPLICIT) syn_exact += c.csr->tgt.size();
         else if (sp.rule == NAER_CONN_FIXED_OUTDEGREE) syn_exact += (uint64_t)sp.degree * n.pops[c.src].size;
         else syn_exact += (uint64_t)sp.degree * n.pops[c.dst].size;
     }
@@ -396,6 +453,26 @@ void Engine::build(NetHost& n) {
         if (cb.rule == NAER_CONN_REF_BERNOULLI) {
             k_bern_fill<<<grid_for((uint64_t)cb.src_size * 32, T, maxb), T, 0, st>>>(cb, cursor, n.tgt,
                                                                                      n.w, n.dly);
+        } else if (cb.rule == NAER_CONN_EXPLICIT) {
+            const ExplicitCsr& x = *n.conns[ci].csr;
+            const uint64_t nnz = x.tgt.size();
+            auto* rp = static_cast<uint64_t*>(dalloc((cb.src_size + 1) * 8ull));
+            auto* tg = static_cast<uint32_t*>(dalloc(std::max<uint64_t>(nnz, 1) * 4ull));
+            auto* wv = static_cast<float*>(dalloc(std::max<uint64_t>(nnz, 1) * 4ull));
+            auto* dv = static_cast<uint8_t*>(dalloc(std::max<uint64_t>(nnz, 1)));
+            NAER_CK(cudaMemcpyAsync(rp, x.row_ptr.data(), (cb.src_size + 1) * 8ull, cudaMemcpyHostToDevice, st));
+            if (nnz) {
+                NAER_CK(cudaMemcpyAsync(tg, x.tgt.data(), nnz * 4ull, cudaMemcpyHostToDevice, st));
+                NAER_CK(cudaMemcpyAsync(wv, x.w.data(), nnz * 4ull, cudaMemcpyHostToDevice, st));
+                NAER_CK(cudaMemcpyAsync(dv, x.dly.data(), nnz, cudaMemcpyHostToDevice, st));
+            }
+            k_explicit_fill<<<grid_for((uint64_t)cb.src_size * 32, T, maxb), T, 0, st>>>(cb, rp, tg, wv, dv, cursor,
+                                                                                         n.tgt, n.w, n.dly);
+            NAER_CK(cudaGetLastError());
+            dfree(rp, (cb.src_size + 1) * 8ull);
+            dfree(tg, std::max<uint64_t>(nnz, 1) * 4ull);
+            dfree(wv, std::max<uint64_t>(nnz, 1) * 4ull);
+            dfree(dv, std::max<uint64_t>(nnz, 1));
         } else if (cb.rule == NAER_CONN_FIXED_OUTDEGREE) {
             const uint64_t items = (uint64_t)cb.src_size * ((cb.K + 3) / 4);
             if (items)
@@ -682,20 +759,16 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     auto upload = [&](void*& dst, size_t& cap_bytes, const void* src, size_t bytes) {
         if (bytes > cap_bytes) {
             if (dst) dfree(dst, cap_bytes);
+            dst = nullptr;
+            cap_bytes = 0;
             dst = dalloc(bytes);
             cap_bytes = bytes;
         }
         if (bytes) NAER_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
     };
-    void* p = d_nets_;
-    upload(p, nets_bytes_, h_nets_.data(), h_nets_.size() * sizeof(NetDev));
-    d_nets_ = static_cast<NetDev*>(p);
-    p = d_pops_;
-    upload(p, pops_bytes_, pops.data(), pops.size() * sizeof(PopDev));
-    d_pops_ = static_cast<PopDev*>(p);
-    p = d_chunks_;
-    upload(p, chunks_bytes_, chunks.data(), chunks.size() * sizeof(ChunkDev));
-    d_chunks_ = static_cast<ChunkDev*>(p);
+    upload(reinterpret_cast<void*&>(d_nets_), nets_bytes_, h_nets_.data(), h_nets_.size() * sizeof(NetDev));
+    upload(reinterpret_cast<void*&>(d_pops_), pops_bytes_, pops.data(), pops.size() * sizeof(PopDev));
+    upload(reinterpret_cast<void*&>(d_chunks_), chunks_bytes_, chunks.data(), chunks.size() * sizeof(ChunkDev));
 
     eng_ = EngineDev{};
     eng_.n_chunks = (uint32_t)chunks.size();
@@ -776,6 +849,8 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     const size_t rbytes = std::max<uint64_t>(raster_capacity, 1) * sizeof(uint2);
     if (rbytes != raster_bytes_) {
         if (d_raster_) dfree(d_raster_, raster_bytes_);
+        d_raster_ = nullptr;
+        raster_bytes_ = 0;
         d_raster_ = static_cast<uint2*>(dalloc(rbytes));
         raster_bytes_ = rbytes;
     }
@@ -917,6 +992,8 @@ void Engine::regrow(void*& p, size_t& have, size_t need) {
     need = std::max<size_t>(need, 16);
     if (need <= have && p) return;
     if (p) dfree(p, have);
+    p = nullptr;  // nothing dangles if the allocation below fails
+    have = 0;
     p = dalloc(need);
     have = need;
 }
@@ -1294,6 +1371,82 @@ uint64_t Engine::read_raster(uint64_t first, uint64_t cap, uint32_t* steps, uint
         ids[i] = rec[i].y;
     }
     return n;
+}
+
+// ---------------------------------------------------------------------------
+// Simulation state of one network between steps: membrane potentials,
+// refractory counters, the delay ring (slots in the network's own step
+// time), and with plasticity the weights, post rows and pre traces.  The
+// connectivity itself is regenerated bit for bit from the description and
+// the Poisson drive from the step counter (counter-based Philox), so
+// neither is stored.  Layout: V f32[Ns] | refr u8[Ns] (padded to 4) |
+// ring f32[D * Ns] | with plasticity: w f32[S] | post i32[Np * stride] |
+// pre int2[Np].
+
+uint64_t state_bytes(const NetHost& n) {
+    const uint64_t Ns = n.n_storage;
+    uint64_t b = Ns * 4ull + ((Ns + 3ull) & ~3ull) + (uint64_t)n.ring_slots * Ns * 4ull;
+    if (n.dev.stdp_on) {
+        b += n.synapses_padded * 4ull;
+        b += (uint64_t)n.n_plastic * n.post_stride * 4ull + (uint64_t)n.n_plastic * 8ull;
+    }
+    return b;
+}
+
+void Engine::save_state(const NetHost& n, uint8_t* dst) {
+    DeviceGuard g(device_);
+    const uint64_t Ns = n.n_storage;
+    uint8_t* p = dst;
+    auto copy = [&](const void* src, uint64_t bytes, uint64_t advance) {
+        if (bytes) NAER_CK(cudaMemcpyAsync(p, src, bytes, cudaMemcpyDeviceToHost, stream_));
+        p += advance;
+    };
+    copy(n.v, Ns * 4ull, Ns * 4ull);
+    copy(n.refr, Ns, (Ns + 3ull) & ~3ull);
+    copy(n.ring, (uint64_t)n.ring_slots * Ns * 4ull, (uint64_t)n.ring_slots * Ns * 4ull);
+    if (n.dev.stdp_on) {
+        copy(n.w, n.synapses_padded * 4ull, n.synapses_padded * 4ull);
+        copy(n.post, (uint64_t)n.n_plastic * n.post_stride * 4ull, (uint64_t)n.n_plastic * n.post_stride * 4ull);
+        copy(n.pre, (uint64_t)n.n_plastic * 8ull, (uint64_t)n.n_plastic * 8ull);
+    }
+    NAER_CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::load_state(NetHost& n, const uint8_t* src) {
+    DeviceGuard g(device_);
+    const uint64_t Ns = n.n_storage;
+    const uint8_t* p = src;
+    auto copy = [&](void* dst, uint64_t bytes, uint64_t advance) {
+        if (bytes) NAER_CK(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, stream_));
+        p += advance;
+    };
+    copy(n.v, Ns * 4ull, Ns * 4ull);
+    copy(n.refr, Ns, (Ns + 3ull) & ~3ull);
+    copy(n.ring, (uint64_t)n.ring_slots * Ns * 4ull, (uint64_t)n.ring_slots * Ns * 4ull);
+    if (n.dev.stdp_on) {
+        copy(n.w, n.synapses_padded * 4ull, n.synapses_padded * 4ull);
+        copy(n.post, (uint64_t)n.n_plastic * n.post_stride * 4ull, (uint64_t)n.n_plastic * n.post_stride * 4ull);
+        copy(n.pre, (uint64_t)n.n_plastic * 8ull, (uint64_t)n.n_plastic * 8ull);
+    }
+    NAER_CK(cudaStreamSynchronize(stream_));  // the source is host memory the caller may reuse
+}
+
+void Engine::set_step(uint64_t step, uint64_t events) {
+    DeviceGuard g(device_);
+    drop_graph();
+    host_step_ = step;
+    // the step counter, an empty raster, the event counters restarted from
+    // the saved total
+    NAER_CK(cudaStreamSynchronize(stream_));
+    Ctl c = read_ctl();
+    c.step = step;
+    c.raster_base = c.raster_next = c.raster_dropped = 0;
+    c.events = 0;
+    std::memcpy(h_pinned_, &c, sizeof(Ctl));
+    NAER_CK(cudaMemcpyAsync(d_ctl_, h_pinned_, sizeof(Ctl), cudaMemcpyHostToDevice, stream_));
+    NAER_CK(cudaMemsetAsync(d_ev_part_, 0, ev_part_n_ * sizeof(unsigned long long), stream_));
+    NAER_CK(cudaStreamSynchronize(stream_));
+    events_base_ = events;
 }
 
 uint64_t Engine::read_raster_raw(uint64_t first, uint64_t cap, uint32_t* records) {

@@ -30,9 +30,19 @@ struct PopSpec {
     uint32_t storage_base = 0;
 };
 
+// Synapses given explicitly (naer_net_add_connection_csr): a CSR over the
+// source population, targets as indices within the destination population.
+struct ExplicitCsr {
+    std::vector<uint64_t> row_ptr;  // [src_size + 1]
+    std::vector<uint32_t> tgt;
+    std::vector<float> w;
+    std::vector<uint8_t> dly;
+};
+
 struct ConnSpec {
     uint32_t src = 0, dst = 0;
     naer_conn_spec spec{};
+    std::shared_ptr<const ExplicitCsr> csr;  // rule NAER_CONN_EXPLICIT
 };
 
 // One network: description, layout and device arrays.
@@ -85,6 +95,13 @@ uint64_t estimate_device_bytes(const NetHost& description);
 // LIF work items (chunks of up to 1,024 neurons of one population) a
 // network adds to an engine, from its description alone.
 uint32_t lif_chunks(const NetHost& description);
+
+// Test hook: the device allocation `after` allocations from now fails with
+// NAER_E_OOM (once); -1 turns it off.
+void set_allocation_failure(int64_t after);
+
+// Bytes of one network's saved simulation state (Engine::save_state).
+uint64_t state_bytes(const NetHost& n);
 
 // Device probe (probe.cu), see naer_probe_device.
 void probe_device(int device, uint64_t ring_cells, uint64_t small_cells, naer_device_probe* out);
@@ -179,6 +196,15 @@ public:
     void* dalloc(size_t bytes);
     void dfree(void* p, size_t bytes);
 
+    // Simulation state of one network between steps (state_bytes() bytes:
+    // neuron state, ring, plasticity state), to host memory and back.  The
+    // network must be built; nothing may be queued that uses it.
+    void save_state(const NetHost& n, uint8_t* dst);
+    void load_state(NetHost& n, const uint8_t* src);
+    // Sets the engine step (a restored network continues from it), empties
+    // the raster and restarts the event counter at `events`.
+    void set_step(uint64_t step, uint64_t events);
+
     // Bounded waits of the step kernel's grid barriers (0 = default) and the
     // test hook that makes every barrier unsatisfiable (see naer_capi.h).
     void set_barrier_limit(uint64_t limit_ns);
@@ -188,6 +214,8 @@ public:
     int device_status();
 
 private:
+    void build_arrays(NetHost& n);
+    std::vector<std::pair<void*, size_t>>* alloc_log_ = nullptr;  // allocations of a build in progress
     void launch_run(uint32_t steps);
     void launch_drive(uint64_t s_first, uint32_t nsteps);
     void run_launches(uint64_t nsteps);

@@ -196,6 +196,46 @@ void Server::release(uint64_t job) {
     if (it->second->freed) jobs_.erase(it); else it->second->released = true;  // the builder erases it
 }
 
+void Server::preempt(uint64_t job) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = jobs_.find(job);
+    if (it == jobs_.end() || it->second->released) throw Error(NAER_E_INVALID, "unknown job");
+    if (it->second->info.state != kJobRunning) throw Error(NAER_E_STATE, "job is not running");
+    it->second->preempt_req = true;
+}
+
+void Server::cancel(uint64_t job) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = jobs_.find(job);
+    if (it == jobs_.end() || it->second->released) throw Error(NAER_E_INVALID, "unknown job");
+    Job* j = it->second.get();
+    if (j->info.state >= kJobDone) throw Error(NAER_E_STATE, "job has already ended");
+    auto end_now = [&] {
+        j->info.state = kJobCancelled;
+        j->info.error = "cancelled";
+        j->steps.clear();
+        j->ids.clear();
+        j->saved.clear();
+        cv_done_.notify_all();
+    };
+    auto p = std::find(pending_.begin(), pending_.end(), job);
+    if (p != pending_.end()) {  // not built: nothing on the device
+        pending_.erase(p);
+        if (j->preempt_req || !j->saved.empty()) j->preempt_req = false;
+        end_now();
+        return;
+    }
+    auto r = std::find(ready_.begin(), ready_.end(), j);
+    if (r != ready_.end()) {  // built, never stepped: the builder frees it
+        ready_.erase(r);
+        to_free_.push_back(j);
+        end_now();
+        cv_build_.notify_all();
+        return;
+    }
+    j->cancel_req = true;  // running: the stepper retires it at the next boundary
+}
+
 ServerStats Server::stats() {
     std::lock_guard<std::mutex> lk(mu_);
     ServerStats s = st_;
@@ -275,6 +315,10 @@ void Server::build_loop() {
             const double t = now_s();
             try {
                 eng->build(*j->net);
+                if (!j->saved.empty()) {  // a pre-empted job: its state from before
+                    eng->load_state(*j->net, j->saved.data());
+                    std::vector<uint8_t>().swap(j->saved);
+                }
                 eng->sync();  // complete before another stream uses it
             } catch (const Error& e) {
                 if (e.code == NAER_E_CUDA) throw;
@@ -409,16 +453,28 @@ void Server::loop() {
                 ms_per_step = ms_per_step > 0.0 ? 0.5 * (ms_per_step + m) : m;
             }
             const uint64_t hs = eng->host_step();
-            // jobs whose last step has run
-            std::vector<Job*> keep, finished;
-            for (Job* j : running) {
-                if (hs >= j->net->dev.end_step) finished.push_back(j); else keep.push_back(j);
+            // jobs whose last step has run; jobs to pre-empt or cancel (the
+            // chunk in flight has been waited for, so their state is whole)
+            std::vector<Job*> keep, finished, preempted, cancelled;
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                for (Job* j : running) {
+                    if (hs >= j->net->dev.end_step) finished.push_back(j);
+                    else if (j->cancel_req) cancelled.push_back(j);
+                    else if (j->preempt_req) preempted.push_back(j);
+                    else keep.push_back(j);
+                }
             }
-            if (!finished.empty()) changed = true;
+            for (Job* j : preempted) {
+                j->resume_steps = hs - j->net->dev.start_step;
+                j->saved.resize(state_bytes(*j->net));
+                eng->save_state(*j->net, j->saved.data());
+            }
+            if (!finished.empty() || !preempted.empty() || !cancelled.empty()) changed = true;
             running.swap(keep);
             for (Job* j : admit) {
-                j->net->dev.start_step = hs;
-                j->net->dev.end_step = hs + j->info.duration;
+                j->net->dev.start_step = hs - j->resume_steps;  // a resumed job keeps its own step count
+                j->net->dev.end_step = j->net->dev.start_step + j->info.duration;
                 running.push_back(j);
                 changed = true;
             }
@@ -490,6 +546,26 @@ void Server::loop() {
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 const double tn2 = now_s();
+                for (Job* j : preempted) {  // device memory freed by the builder, then rebuilt from the queue
+                    j->preempt_req = false;
+                    j->info.state = kJobQueued;
+                    j->info.steps_done = j->resume_steps;
+                    ++j->info.preemptions;
+                    to_free_.push_back(j);
+                    pending_.push_back(j->id);
+                }
+                for (Job* j : cancelled) {
+                    j->cancel_req = false;
+                    j->info.state = kJobCancelled;
+                    j->info.error = "cancelled";
+                    j->steps.clear();
+                    j->ids.clear();
+                    to_free_.push_back(j);
+                }
+                if (!preempted.empty() || !cancelled.empty()) {
+                    cv_build_.notify_all();
+                    cv_done_.notify_all();
+                }
                 for (Job* j : finished) {
                     j->info.state = kJobDone;
                     j->info.done_s = tn2;

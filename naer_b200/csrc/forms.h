@@ -57,10 +57,11 @@ struct ServerParams {
     uint32_t launch_steps = 4;     // grid steps per persistent step launch (builds run between launches)
 };
 
-enum JobState : uint32_t { kJobQueued = 0, kJobRunning = 1, kJobDone = 2, kJobFailed = 3 };
+enum JobState : uint32_t { kJobQueued = 0, kJobRunning = 1, kJobDone = 2, kJobFailed = 3, kJobCancelled = 4 };
 
 struct JobInfo {
     uint32_t state = kJobQueued;
+    uint32_t preemptions = 0;  // times the job was taken off the device and later resumed
     uint64_t duration = 0, steps_done = 0, spikes = 0, spikes_dropped = 0;
     uint64_t device_bytes = 0;
     double submit_s = 0, admit_s = 0, done_s = 0;  // seconds since the server started
@@ -98,6 +99,14 @@ public:
     bool wait(uint64_t job, double timeout_s);
     bool drain(double timeout_s);
     void release(uint64_t job);
+    // Takes a running job off the device at the next chunk boundary: its
+    // state is saved to host memory, its device memory freed, and it queues
+    // again; when re-admitted it is rebuilt, restored and continues from the
+    // same step (deterministic jobs give the raster of an uninterrupted run).
+    void preempt(uint64_t job);
+    // Ends a job that has not finished: queued or built jobs at once, a
+    // running job at the next chunk boundary.  Its raster is discarded.
+    void cancel(uint64_t job);
     ServerStats stats();
 
 private:
@@ -110,6 +119,9 @@ private:
         std::vector<uint32_t> steps, ids;
         bool freed = false;     // holds no device memory
         bool released = false;  // forgotten by the caller: erase once freed
+        bool preempt_req = false, cancel_req = false;
+        std::vector<uint8_t> saved;  // state of a pre-empted job until it is rebuilt
+        uint64_t resume_steps = 0;   // job-local step it resumes from
     };
     void loop();
     void build_loop();

@@ -196,6 +196,14 @@ class Server:
     def release(self, job: int) -> None:
         capi.call("naer_server_release", self._h, int(job))
 
+    def preempt(self, job: int) -> None:
+        """Takes a running job off the device at the next chunk boundary; it
+        queues again and resumes from the step it reached."""
+        capi.call("naer_server_preempt", self._h, int(job))
+
+    def cancel(self, job: int) -> None:
+        capi.call("naer_server_cancel", self._h, int(job))
+
     def stats(self) -> dict:
         s = capi.ServerStats()
         capi.call("naer_server_get_stats", self._h, C.byref(s))

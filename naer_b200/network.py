@@ -162,6 +162,24 @@ class Network:
         self._conns.append(con)
         return con
 
+    def connect_csr(self, source: Population, destination: Population, row_ptr, targets, weights,
+                    delays) -> Connection:
+        """Explicit connectivity: a CSR over the source population (row_ptr of
+        size+1 entries), target indices within the destination population,
+        weights and delays in grid steps."""
+        rp = np.ascontiguousarray(row_ptr, dtype=np.uint64)
+        tg = np.ascontiguousarray(targets, dtype=np.uint32)
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        d = np.ascontiguousarray(delays, dtype=np.uint8)
+        if len(rp) != source.size + 1 or not (len(tg) == len(w) == len(d) == int(rp[-1])):
+            raise ValueError("row_ptr needs size+1 entries and the synapse arrays row_ptr[-1] entries")
+        p = lambda a: a.ctypes.data_as(C.c_void_p)
+        capi.call("naer_net_add_connection_csr", self._h, source.id, destination.id, p(rp), p(tg), p(w), p(d))
+        con = Connection(source, destination, 0.0, 0.0, 0.0, 0.0, 0, capi.CONN_EXPLICIT, 0,
+                         int(d.min()) if len(d) else 1, int(d.max()) if len(d) else 1)
+        self._conns.append(con)
+        return con
+
     def compile(self) -> None:
         capi.call("naer_net_compile", self._h)
         for p in self._pops:  # Network.cpp:283-285: final addresses
@@ -283,6 +301,19 @@ class Network:
         capi.call("naer_net_read_csr", self._h, rp.ctypes.data_as(C.c_void_p), tg.ctypes.data_as(C.c_void_p),
                   w.ctypes.data_as(C.c_void_p), d.ctypes.data_as(C.c_void_p))
         return rp, tg, w, d
+
+    def checkpoint(self) -> bytes:
+        """The network's whole simulation state between steps (blocks)."""
+        n = C.c_uint64()
+        capi.call("naer_net_checkpoint_size", self._h, C.byref(n))
+        buf = C.create_string_buffer(n.value)
+        capi.call("naer_net_checkpoint", self._h, buf, n.value)
+        return buf.raw
+
+    def restore(self, data: bytes) -> None:
+        """Loads a checkpoint taken from a network of the same description."""
+        buf = C.create_string_buffer(bytes(data), len(data))
+        capi.call("naer_net_restore", self._h, buf, len(data))
 
     def set_profiling(self, on: bool) -> None:
         capi.call("naer_net_set_profiling", self._h, 1 if on else 0)

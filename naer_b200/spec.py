@@ -44,6 +44,7 @@ class ConnSpec:
     dmin: int = 1
     dmax: int = 1
     seed: int = 1
+    csr: tuple | None = None      # CONN_EXPLICIT: (row_ptr, targets, weights, delays) numpy arrays
 
 
 @dataclass
@@ -70,6 +71,16 @@ class NetSpec:
 
     def connect(self, src: int, dst: int, rule: int, weight: float, **kw) -> None:
         self.conns.append(ConnSpec(src, dst, int(rule), float(weight), **kw))
+
+    def connect_csr(self, src: int, dst: int, row_ptr, targets, weights, delays) -> None:
+        """Explicit synapses from population src to dst: a CSR over the
+        source population, targets as indices within the destination."""
+        import numpy as np
+        arrs = (np.ascontiguousarray(row_ptr, dtype=np.uint64), np.ascontiguousarray(targets, dtype=np.uint32),
+                np.ascontiguousarray(weights, dtype=np.float32), np.ascontiguousarray(delays, dtype=np.uint8))
+        d = arrs[3]
+        self.conns.append(ConnSpec(src, dst, capi.CONN_EXPLICIT, 0.0, dmin=int(d.min()) if len(d) else 1,
+                                   dmax=int(d.max()) if len(d) else 1, csr=arrs))
 
     @property
     def neurons(self) -> int:
@@ -116,6 +127,9 @@ def describe(spec: NetSpec, device: int = -1) -> Network:
                       drive_seed=p.drive_seed)
             pops.append(net.addPopulation(NeuronType(p.type), p.size, **kw))
         for c in spec.conns:
+            if c.csr is not None:
+                net.connect_csr(pops[c.src], pops[c.dst], *c.csr)
+                continue
             net.connect(pops[c.src], pops[c.dst], rule=c.rule, weight=c.weight, probability=c.probability,
                         degree=c.degree, wmin=c.wmin, wmax=c.wmax, delay=(c.dmin, c.dmax), seed=c.seed)
     except Exception:

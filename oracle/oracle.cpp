@@ -137,11 +137,15 @@ struct OrPop {
 };
 
 struct OrConn {
-    uint32_t src, dst, rule, degree;
+    uint32_t src, dst, rule, degree;  // rule 3: explicit synapses (the arrays below)
     double p;
     float weight, wmin, wmax;
     uint32_t dmin, dmax, pad;
     uint64_t seed;
+    const uint64_t* rp;  // explicit: CSR over the source population (valid until the build)
+    const uint32_t* tg;  // target index within the destination population
+    const float* wv;
+    const uint8_t* dv;
 };
 
 struct OrParams {
@@ -267,6 +271,8 @@ void build_csr(Net& net) {
             }
         } else if (c.rule == 2) {
             std::fill(cnt[ci].begin(), cnt[ci].end(), c.degree);
+        } else if (c.rule == 3) {
+            for (uint32_t s = 0; s < sp.size; ++s) cnt[ci][s] = (uint32_t)(c.rp[s + 1] - c.rp[s]);
         } else {
             for (uint32_t i = 0; i < dp.size; ++i)
                 for (uint32_t b = 0; b < (c.degree + 3) / 4; ++b) {
@@ -310,6 +316,15 @@ void build_csr(Net& net) {
                     ++o;
                 }
             }
+        } else if (c.rule == 3) {
+            // explicit synapses, each row in the given order
+            for (uint32_t s = 0; s < sp.size; ++s)
+                for (uint64_t j = c.rp[s]; j < c.rp[s + 1]; ++j) {
+                    const uint64_t q = cur[sb + s] + (j - c.rp[s]);
+                    net.tgt[q] = db + c.tg[j];
+                    net.w[q] = c.wv[j];
+                    net.dly[q] = c.dv[j];
+                }
         } else if (c.rule == 2) {
 #pragma omp parallel for schedule(static)
             for (int64_t s = 0; s < (int64_t)sp.size; ++s) {

@@ -26,7 +26,8 @@ class OrPop(C.Structure):
 class OrConn(C.Structure):
     _fields_ = [("src", C.c_uint32), ("dst", C.c_uint32), ("rule", C.c_uint32), ("degree", C.c_uint32),
                 ("p", C.c_double), ("weight", C.c_float), ("wmin", C.c_float), ("wmax", C.c_float),
-                ("dmin", C.c_uint32), ("dmax", C.c_uint32), ("pad", C.c_uint32), ("seed", C.c_uint64)]
+                ("dmin", C.c_uint32), ("dmax", C.c_uint32), ("pad", C.c_uint32), ("seed", C.c_uint64),
+                ("rp", C.c_void_p), ("tg", C.c_void_p), ("wv", C.c_void_p), ("dv", C.c_void_p)]
 
 
 class OrParams(C.Structure):
@@ -134,6 +135,8 @@ class OracleNet:
         for i, c in enumerate(spec.conns):
             conns[i] = OrConn(c.src, c.dst, c.rule, c.degree, c.probability, c.weight, c.wmin, c.wmax, c.dmin,
                               c.dmax, 0, c.seed & 0xFFFFFFFFFFFFFFFF)
+            if getattr(c, "csr", None) is not None:  # explicit synapses: arrays alive through the build below
+                conns[i].rp, conns[i].tg, conns[i].wv, conns[i].dv = (a.ctypes.data for a in c.csr)
         self._lib = lib
         self._h = lib.oracle_net_create(C.byref(prm), pops, len(spec.pops), conns, len(spec.conns))
         lib.oracle_net_build(self._h)

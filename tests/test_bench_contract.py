@@ -10,7 +10,7 @@ ROOT = Path(__file__).resolve().parent.parent
 
 def test_reference_arm_json_line():
     out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--neurons", "4000",
-                          "--degree", "100", "--steps", "2", "--warmup", "1", "--cpu-steps", "40",
+                          "--degree", "100", "--steps", "2", "--warmup", "1", "--chunk", "50", "--cpu-steps", "40",
                           "--cpu-warmup", "20"], capture_output=True, text=True, timeout=600, check=True).stdout
     lines = [l for l in out.splitlines() if l.startswith("{")]
     assert len(lines) == 1

@@ -71,3 +71,40 @@ def test_device_probe_figures(lib):
         assert 1e9 < p[k] < 1e14, (k, p[k])
     assert 500 < p["stream_gbs"] < 20_000
     assert 0.05 < p["barrier_us_1"] < 100 and 0.05 < p["barrier_us_2"] < 100
+
+
+def test_allocation_failure_reported_and_released(lib):
+    """An out-of-memory injected at every allocation of a compile in turn:
+    each attempt returns NAER_E_OOM with nothing left allocated by it (the
+    same handle then compiles to the footprint of a fresh one), and the
+    network steps like one that never failed."""
+    s = S.plastic_indegree(n=2000, k=100, drive_weight=21.0).with_(deterministic=True)
+    with S.build(s) as ref:
+        ref_bytes = ref.stats()["device_bytes"]
+        ref.run(200)
+        ref.finish()
+        ref_raster = ref.read_spikes()
+    hits = 0
+    try:
+        for k in range(400):
+            net = S.describe(s, device=0)
+            try:
+                capi.call("naer_test_fail_allocation", k)
+                rc = lib.naer_net_compile(net.handle)
+                capi.call("naer_test_fail_allocation", -1)
+                if rc == capi.NAER_OK:
+                    break
+                assert rc == capi.NAER_E_OOM, (k, rc, capi.last_error())
+                assert "injected" in capi.last_error()
+                hits += 1
+                net.compile()  # the injection fired once: the same handle compiles now
+                assert net.stats()["device_bytes"] == ref_bytes, k
+                net.run(200)
+                net.finish()
+                st, ids = net.read_spikes()
+                assert np.array_equal(st, ref_raster[0]) and np.array_equal(ids, ref_raster[1]), k
+            finally:
+                net.close()
+    finally:
+        capi.call("naer_test_fail_allocation", -1)
+    assert hits > 10  # every allocation of the build, the tables and the queues was hit

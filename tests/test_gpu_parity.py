@@ -325,3 +325,45 @@ def test_silent_and_empty_networks(O):
         net.run(100)
         net.finish()
         assert net.stats()["spikes"] == 0 and net.stats()["events"] == 0
+
+
+def explicit_net(seed=9):
+    """POISSON -> E by a rule, explicit random E -> I and I -> E synapses
+    (multapses, delays 1-7, weights of both signs), deterministic mode."""
+    rng = np.random.default_rng(seed)
+    s = S.NetSpec(poisson_seed=seed, deterministic=True)
+    P = s.add_pop(S.POISSON, 500, rate_hz=40.0)
+    E = s.add_pop(S.NOP, 900, drive_rate_hz=20.0, drive_weight=18.0, drive_seed=4)
+    I = s.add_pop(S.NOP, 230)
+    s.connect(P, E, capi.CONN_FIXED_OUTDEGREE, 3.0, degree=40, dmin=1, dmax=3, seed=seed)
+    for src, n_src, dst, n_dst, sign in [(E, 900, I, 230, 1.0), (I, 230, E, 900, -1.0)]:
+        lens = rng.integers(0, 60, n_src)
+        rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+        nnz = int(rp[-1])
+        s.connect_csr(src, dst, rp, rng.integers(0, n_dst, nnz), sign * rng.uniform(0.5, 4.0, nnz),
+                      rng.integers(1, 8, nnz))
+    return s
+
+
+def test_explicit_connectivity_bit_exact(O):
+    """Connectivity uploaded by the caller (naer_net_add_connection_csr)
+    next to a generated one: the CSR, raster and state match the oracle."""
+    s = explicit_net()
+    net, o = run_both(O, s, 1500)
+    with net:
+        assert net.getSynapses() == o.S
+        assert_csr_equal(net, o)
+        assert assert_same_run(net, o) > 500
+
+
+def test_explicit_connectivity_rejects_bad_input(lib):
+    from naer_b200 import Network, NaerError
+    with Network() as net:
+        a = net.addPopulation(NeuronType.NOP, 4)
+        b = net.addPopulation(NeuronType.NOP, 3)
+        with pytest.raises(NaerError, match="outside the destination"):
+            net.connect_csr(a, b, [0, 1, 1, 1, 1], [3], [1.0], [1])
+        with pytest.raises(NaerError, match="delays"):
+            net.connect_csr(a, b, [0, 1, 1, 1, 1], [0], [1.0], [0])
+        with pytest.raises(NaerError, match="decrease"):
+            net.connect_csr(a, b, [0, 2, 1, 1, 2], [0, 1], [1.0, 1.0], [1, 1])

@@ -386,3 +386,30 @@ def test_event_mode_reference_brunel_deterministic(oracle_mod):
     tb, ib = b.event_spikes()
     assert np.array_equal(ta, tb) and np.array_equal(ia, ib)
     assert len(ia) > 1000
+
+
+def test_explicit_csr_reproduces_a_rule(oracle_mod):
+    """A rule's connectivity given back as explicit synapses (the CSR the
+    oracle generated) runs exactly like the rule-generated network."""
+    O = oracle_mod
+    a = S.NetSpec(poisson_seed=5)
+    P = a.add_pop(S.POISSON, 400, rate_hz=60.0)
+    E = a.add_pop(S.NOP, 300)
+    a.connect(P, E, capi.CONN_FIXED_OUTDEGREE, 0.0, wmin=4.0, wmax=9.0, degree=30, dmin=1, dmax=6, seed=3)
+    oa = O.OracleNet(a, deterministic=True)
+    rp, tg, w, d = oa.csr()
+    base_p, base_e = oa.population_base(P), oa.population_base(E)
+    rows = rp[base_p:base_p + 401] - rp[base_p]
+    lo, hi = int(rp[base_p]), int(rp[base_p + 400])
+    b = S.NetSpec(poisson_seed=5)
+    P2 = b.add_pop(S.POISSON, 400, rate_hz=60.0)
+    E2 = b.add_pop(S.NOP, 300)
+    b.connect_csr(P2, E2, rows, tg[lo:hi] - base_e, w[lo:hi], d[lo:hi])
+    ob = O.OracleNet(b, deterministic=True)
+    for x, y in zip(oa.csr(), ob.csr()):
+        assert np.array_equal(x, y)
+    oa.run(500)
+    ob.run(500)
+    sa, ia = oa.spikes()
+    sb, ib = ob.spikes()
+    assert len(ia) > 100 and np.array_equal(sa, sb) and np.array_equal(ia, ib)
