@@ -305,6 +305,19 @@ NAER_API int naer_test_set_barrier_skew(naer_net* net, uint64_t skew);
  * whatever it had allocated. */
 NAER_API int naer_test_fail_allocation(int64_t after);
 
+/* The bounds-checked build (libnaer_b200_checked.so, compiled with
+ * NAER_CHECKED; no counterpart in the reference).  Its step kernels check
+ * every global access at a computed index against the buffer it falls in
+ * and skip it when outside; the first such index is recorded.  *checked =
+ * 1 in that build, 0 in the normal one. */
+NAER_API int naer_build_checked(int* checked);
+/* First out-of-bounds access the checked build recorded for the network's
+ * launches (*code 0 = none; 1 synapse arrays, 2 ring cell, 3 spike list,
+ * 4 raster, 5 neuron state, 6 Poisson-count slot, 7 plasticity state,
+ * 8 deterministic event list) and its index.  Always 0 in the normal
+ * build.  Blocks like finish(). */
+NAER_API int naer_net_check_report(naer_net* net, uint32_t* code, uint64_t* index);
+
 /* ---- device probe ------------------------------------------------------
  * No counterpart in the reference.  Measures, on `device`, the ceilings the
  * step kernel is judged against: random-address fp32 reductions
@@ -326,6 +339,15 @@ typedef struct naer_device_probe {
 } naer_device_probe;
 
 NAER_API int naer_probe_device(int device, uint64_t ring_cells, uint64_t small_cells, naer_device_probe* out);
+
+/* The Poisson generator's inter-event interval in µs, (uint)(log(1 - x) /
+ * -(rate * 1e-6)) with x = z / 0xFFFFFFFF (random.cl:26-30 and the cast of
+ * input_neuron_group.cl:29,37), computed on `device` exactly as the drive
+ * kernels do, for z = z_first + i * z_step (mod 2^32), i < count.  For
+ * comparing the device's logarithm with a host's at the truncation
+ * boundary (no counterpart in the reference). */
+NAER_API int naer_probe_intervals(int device, double rate_hz, uint32_t z_first, uint32_t z_step, uint64_t count,
+                                  uint32_t* out);
 
 /* ---- batched form ------------------------------------------------------
  * No counterpart in the reference (one Network per device queue there).

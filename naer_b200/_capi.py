@@ -11,6 +11,8 @@ import os
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libnaer_b200.so"
+# NAER_CHECKED=1 in the environment loads the bounds-checked build instead
+LIB_CHECKED_PATH = Path(__file__).resolve().parent / "libnaer_b200_checked.so"
 
 NAER_OK = 0
 NAER_E_INVALID = -1
@@ -217,7 +219,10 @@ PROTOTYPES = {
     "naer_net_set_wait_limit": [_vp, C.c_uint64],
     "naer_test_set_barrier_skew": [_vp, C.c_uint64],
     "naer_test_fail_allocation": [C.c_int64],
+    "naer_build_checked": [_P(C.c_int)],
+    "naer_net_check_report": [_vp, _P(C.c_uint32), _P(C.c_uint64)],
     "naer_probe_device": [C.c_int, C.c_uint64, C.c_uint64, _P(DeviceProbe)],
+    "naer_probe_intervals": [C.c_int, C.c_double, C.c_uint32, C.c_uint32, C.c_uint64, _vp],
     "naer_net_autotune": [_vp, C.c_uint32, _P(Tuning)],
     "naer_net_set_tuning": [_vp, _P(Tuning)],
     "naer_net_get_tuning": [_vp, _P(Tuning)],
@@ -261,7 +266,7 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    p = Path(path) if path else (LIB_CHECKED_PATH if os.environ.get("NAER_CHECKED") == "1" else LIB_PATH)
     if not p.exists():
         raise RuntimeError(
             f"naer_b200 CUDA library not found at {p}; build it with `python -m naer_b200.build`")

@@ -365,6 +365,39 @@ int naer_test_set_barrier_skew(naer_net* net, uint64_t skew) {
     });
 }
 
+int naer_probe_intervals(int device, double rate_hz, uint32_t z_first, uint32_t z_step, uint64_t count,
+                         uint32_t* out) {
+    return guarded([&] {
+        need(out != nullptr || count == 0, NAER_E_INVALID, "null argument");
+        need(rate_hz > 0.0, NAER_E_INVALID, "rate must be positive");
+        int n = 0;
+        NAER_CK(cudaGetDeviceCount(&n));
+        need(device >= 0 && device < n, NAER_E_INVALID, "device index out of range");
+        naer::probe_intervals(device, rate_hz, z_first, z_step, count, out);
+    });
+}
+
+int naer_build_checked(int* checked) {
+    return guarded([&] {
+        need(checked != nullptr, NAER_E_INVALID, "null argument");
+#ifdef NAER_CHECKED
+        *checked = 1;
+#else
+        *checked = 0;
+#endif
+    });
+}
+
+int naer_net_check_report(naer_net* net, uint32_t* code, uint64_t* index) {
+    return guarded([&] {
+        need_compiled(net);
+        need(code != nullptr && index != nullptr, NAER_E_INVALID, "null argument");
+        const naer::Ctl c = net->eng->read_ctl();
+        *code = c.chk_code;
+        *index = c.chk_index;
+    });
+}
+
 int naer_test_fail_allocation(int64_t after) {
     return guarded([&] {
         need(after >= -1, NAER_E_INVALID, "after must be >= -1");

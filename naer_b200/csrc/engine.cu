@@ -634,6 +634,7 @@ void Engine::build_arrays(NetHost& n) {
     d.e_minus = n.e_minus;
     d.start_step = 0;
     d.end_step = ~0ull;
+    d.syn_cap = std::max<uint64_t>(n.syn_capacity, n.synapses_padded);
     d.n_storage = Ns;
     d.ring_slots = n.ring_slots;
     d.dt_us = P.dt_us;

@@ -105,6 +105,7 @@ uint64_t state_bytes(const NetHost& n);
 
 // Device probe (probe.cu), see naer_probe_device.
 void probe_device(int device, uint64_t ring_cells, uint64_t small_cells, naer_device_probe* out);
+void probe_intervals(int device, double rate_hz, uint32_t z_first, uint32_t z_step, uint64_t count, uint32_t* out);
 
 // Launch geometry of the persistent step loop (all choices leave the
 // simulated results unchanged).

@@ -91,6 +91,7 @@ struct NetDev {
     uint64_t start_step;    // engine step at which this net's step 0 runs
     uint64_t end_step;      // first engine step at which this net no longer runs (~0 = never)
     uint64_t ring_key_base; // first ring cell of this net in the deterministic key space
+    uint64_t syn_cap;       // entries of tgt / w / dly (bounds of the checked build)
     uint32_t n_storage;     // multiple of 4
     uint32_t ring_slots;    // D = max delay + 1
     uint32_t dt_us;         // grid step in microseconds
@@ -148,6 +149,9 @@ struct Ctl {
     unsigned int qtail[4];          // k_step: spikes queued in step s, slot s & 3 (zeroed with bar_arrive)
     unsigned int error;
     unsigned int pad_;
+    unsigned int chk_code;          // NAER_CHECKED build: first out-of-bounds access (CheckCode), 0 = none
+    unsigned int pad2_;
+    unsigned long long chk_index;   // its index
     unsigned long long bar_limit_ns;  // bounded wait of one grid barrier (0 = kBarrierLimitNs)
     unsigned long long bar_skew;      // added to every barrier target: 0, except when a test makes the
                                       // wait unsatisfiable to exercise the timeout (naer_test_set_barrier_skew)

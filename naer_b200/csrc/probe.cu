@@ -19,6 +19,7 @@
 
 #include "engine.h"
 #include "grid_sync.cuh"
+#include "philox.cuh"
 
 namespace naer {
 
@@ -77,6 +78,15 @@ __global__ void __launch_bounds__(256) k_probe_barrier(Ctl* ctl, uint32_t n) {
         target += gridDim.x;
         if (!grid_barrier(ctl, target, cfg)) return;
     }
+}
+
+// The Poisson generator's interval (input_neuron_group.cl:29,37 through
+// random.cl:26-30) of generator outputs z = z_first + i * z_step (mod 2^32),
+// exactly as the drive kernels compute it on the device.
+__global__ void k_probe_intervals(double rate, uint32_t z_first, uint32_t z_step, uint64_t count, uint32_t* out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = ref_exp_interval_us(z_first + (uint32_t)i * z_step, rate);
 }
 
 struct Timer {
@@ -205,6 +215,25 @@ void probe_device(int device, uint64_t ring_cells, uint64_t small_cells, naer_de
     cudaFree(sink);
     cudaStreamDestroy(st);
     cudaSetDevice(prev);
+}
+
+void probe_intervals(int device, double rate_hz, uint32_t z_first, uint32_t z_step, uint64_t count,
+                     uint32_t* out) {
+    int prev = -1;
+    NAER_CK(cudaGetDevice(&prev));
+    NAER_CK(cudaSetDevice(device));
+    uint32_t* d = nullptr;
+    const cudaError_t e = cudaMalloc(&d, std::max<uint64_t>(count, 1) * 4ull);
+    if (e != cudaSuccess) {
+        cudaSetDevice(prev);
+        NAER_CK(e);
+    }
+    k_probe_intervals<<<1184, 256>>>(rate_hz, z_first, z_step, count, d);
+    cudaError_t e2 = cudaGetLastError();
+    if (e2 == cudaSuccess && count) e2 = cudaMemcpy(out, d, count * 4ull, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    cudaSetDevice(prev);
+    NAER_CK(e2);
 }
 
 }  // namespace naer

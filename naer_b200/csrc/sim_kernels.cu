@@ -8,6 +8,7 @@
 // counter) and publishes one count; each scatter block prefix-sums the
 // counts in shared memory.  The only global atomics are the ring
 // reductions themselves.
+#include "check.cuh"
 #include "grid_sync.cuh"
 #include "sim_kernels.cuh"
 
@@ -98,13 +99,13 @@ constexpr uint32_t kDriveQueue = 160;
 // over the zero bytes the common path stored for them.  The warp barriers
 // order those stores and the queue's shared-memory accesses.
 __device__ __forceinline__ void drive_resolve(const PopDev& p, uint8_t* drive, uint32_t Ns, uint32_t dt_us,
-                                              const DriveWindow* q, uint32_t n, uint32_t lane) {
+                                              const DriveWindow* q, uint32_t n, uint32_t lane, Ctl* ctl) {
     __syncwarp();
     if (lane < n) {
         const DriveWindow w = q[lane];
         const uint32_t idx = (p.type == kPOISSON ? p.rng_idx_base : 0u) + (w.i - p.storage_base);
         const uint32_t cnt = poisson_exact_call(p.rate_hz, p.rng_seed, p.rng_n, idx, w.z0, w.t0, w.t0 + dt_us);
-        __stcg(drive + (size_t)w.slot * Ns + w.i, (unsigned char)cnt);
+        if (NAER_IN_BOUNDS(ctl, w.i, Ns, kChkDrive)) __stcg(drive + (size_t)w.slot * Ns + w.i, (unsigned char)cnt);
     }
     __syncwarp();
 }
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_DRIVE_MIN_BLOCKS)
     for (uint64_t it = it0; it < it_end; ++it, (++k == nsteps ? (k = 0, ++c) : 0)) {
         if (c != cur) {
             if (qn) {  // the previous chunk's windows, with its descriptors
-                drive_resolve(p, drive, Ns, dt_us, q, qn, lane);
+                drive_resolve(p, drive, Ns, dt_us, q, qn, lane, eng.ctl);
                 qn = 0;
             }
             cur = c;
@@ -174,7 +175,8 @@ __global__ void __launch_bounds__(kLifThreads, NAER_DRIVE_MIN_BLOCKS)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
             if (act && i0 + j < cend && !poisson_quiet(p, z[j], t0)) rare |= 1u << j;
-        if (act) __stcg(reinterpret_cast<unsigned int*>(drive + (size_t)slot * Ns + i0), 0u);
+        if (act && NAER_IN_BOUNDS(eng.ctl, i0 + 3, Ns, kChkDrive))
+            __stcg(reinterpret_cast<unsigned int*>(drive + (size_t)slot * Ns + i0), 0u);
         if (__any_sync(0xFFFFFFFFu, rare != 0)) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -185,11 +187,11 @@ __global__ void __launch_bounds__(kLifThreads, NAER_DRIVE_MIN_BLOCKS)
             }
             while (qn >= 32) {
                 qn -= 32;
-                drive_resolve(p, drive, Ns, dt_us, q + qn, 32, lane);
+                drive_resolve(p, drive, Ns, dt_us, q + qn, 32, lane, eng.ctl);
             }
         }
     }
-    if (qn) drive_resolve(p, drive, Ns, dt_us, q, qn, lane);
+    if (qn) drive_resolve(p, drive, Ns, dt_us, q, qn, lane, eng.ctl);
 }
 
 // ---------------------------------------------------------------------------
@@ -776,7 +778,7 @@ template __global__ void k_run<false>(EngineDev, unsigned long long, uint32_t);
 // (STDP update first for plastic synapses of plastic sources).
 __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, const SpikeRec& r, uint64_t lo,
                                              uint64_t hi, uint32_t piece, uint32_t split, uint32_t psz,
-                                             uint32_t lane, unsigned long long& ev, uint32_t& ovf) {
+                                             uint32_t lane, unsigned long long& ev, uint32_t& ovf, Ctl* ctl) {
     const uint32_t D = np->ring_slots;
     const uint32_t tmod = tl % D;
     const uint32_t Ns = np->n_storage;
@@ -796,7 +798,7 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
 #pragma unroll
         for (int u = 0; u < (int)kScatterUnroll; ++u) {
             const uint64_t off = base + (uint64_t)(u * 32 + lane) * 4ull;
-            if (off < hi && (uint32_t)u * 128u < psz) {
+            if (off < hi && (uint32_t)u * 128u < psz && NAER_IN_BOUNDS(ctl, off + 3, np->syn_cap, kChkSynapse)) {
                 tg[u] = ld_stream_u4(tgt_a + off);
                 ww[u] = __ldcg(reinterpret_cast<const float4*>(w_a + off));  // STDP may rewrite
                 dd[u] = ld_stream_u32(d_a + off);
@@ -812,7 +814,7 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const uint32_t tgt = u4_get(tg[u], j);
-                if (tgt == kTgtSentinel) continue;
+                if (tgt == kTgtSentinel || !NAER_IN_BOUNDS(ctl, tgt, Ns, kChkRing)) continue;
                 float w = f4_get(ww[u], j);
                 const uint32_t d = (dd[u] >> (8 * j)) & 0xFFu;
                 if (plastic_src && tgt < n_plastic) {
@@ -830,7 +832,7 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
 // deliver_span for a static source (no plasticity): the deferred rest.
 __device__ __forceinline__ void deliver_static_span(const NetDev* np, uint32_t tl, int32_t aux0, uint64_t lo,
                                                     uint64_t hi, uint32_t piece, uint32_t split, uint32_t psz,
-                                                    uint32_t lane, unsigned long long& ev) {
+                                                    uint32_t lane, unsigned long long& ev, Ctl* ctl) {
     const uint32_t D = np->ring_slots;
     const uint32_t tmod = tl % D;
     const uint32_t Ns = np->n_storage;
@@ -846,7 +848,7 @@ __device__ __forceinline__ void deliver_static_span(const NetDev* np, uint32_t t
 #pragma unroll
         for (int u = 0; u < (int)kScatterUnroll; ++u) {
             const uint64_t off = base + (uint64_t)(u * 32 + lane) * 4ull;
-            if (off < hi && (uint32_t)u * 128u < psz) {
+            if (off < hi && (uint32_t)u * 128u < psz && NAER_IN_BOUNDS(ctl, off + 3, np->syn_cap, kChkSynapse)) {
                 tg[u] = ld_stream_u4(tgt_a + off);
                 ww[u] = __ldcs(reinterpret_cast<const float4*>(w_a + off));
                 dd[u] = ld_stream_u32(d_a + off);
@@ -861,7 +863,7 @@ __device__ __forceinline__ void deliver_static_span(const NetDev* np, uint32_t t
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const uint32_t tgt = u4_get(tg[u], j);
-                if (tgt == kTgtSentinel) continue;
+                if (tgt == kTgtSentinel || !NAER_IN_BOUNDS(ctl, tgt, Ns, kChkRing)) continue;
                 float w = f4_get(ww[u], j);
                 if (mult != 1.0f) w = __fmul_rn(w, mult);
                 red_add_f32(ring + (size_t)ring_slot(tmod, (dd[u] >> (8 * j)) & 0xFFu, D) * Ns + tgt, w);
@@ -1000,7 +1002,7 @@ __device__ __forceinline__ void rest_item(const EngineDev& eng, const RestWork& 
     const ulonglong2 rb = row_bounds(np->row_ptr, src);
     const uint64_t mid = rb.x + __ldg(np->row_mid + src);
     deliver_static_span(np, (uint32_t)(rw.step - np->start_step), rv.z, mid, rb.y, piece, split, eng.scatter_piece,
-                        lane, ev);
+                        lane, ev, eng.ctl);
 }
 
 // Chunk descriptors, membrane potentials and refractory counters of the
@@ -1033,7 +1035,9 @@ __device__ __forceinline__ void load_chunk_state(const EngineDev& eng, uint32_t 
     __syncthreads();
     for (uint32_t j = 0; j < own; ++j) {
         const uint32_t i0 = s_cc[j].first + threadIdx.x * kLifPerThread;
-        if (i0 < s_cc[j].end) {
+        // a chunk lies inside its net's state arrays (checked once per launch:
+        // every later access of the chunk stays within [first, end))
+        if (i0 < s_cc[j].end && NAER_IN_BOUNDS(eng.ctl, s_cc[j].end, (uint64_t)s_cc[j].Ns + 1, kChkState)) {
             const uint32_t si = j * kLifThreads + threadIdx.x;
             sV[si] = *reinterpret_cast<const float4*>(s_cc[j].v + i0);
             sR[si] = *reinterpret_cast<const uchar4*>(s_cc[j].refr + i0);
@@ -1274,10 +1278,12 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
                 if (piece == 0 && lane == 0 && eng.record && rbase + e < eng.raster_cap)
                     __stcg(eng.raster + rbase + e, make_uint2((uint32_t)s, __ldcg(qid + e)));
                 const NetDev* np = (r.net == 0) ? &s_net0 : eng.nets + r.net;
+                if (!NAER_IN_BOUNDS(eng.ctl, r.src, np->n_storage, kChkQueue)) continue;
                 const ulonglong2 rb = row_bounds(np->row_ptr, r.src);
                 const bool plastic_src = np->stdp_on && r.src < np->n_plastic;
                 const uint64_t hi = plastic_src ? rb.y : rb.x + __ldg(np->row_mid + r.src);
-                deliver_span(np, (uint32_t)(s - np->start_step), r, rb.x, hi, piece, split, psz, lane, ev, ovf);
+                deliver_span(np, (uint32_t)(s - np->start_step), r, rb.x, hi, piece, split, psz, lane, ev, ovf,
+                             eng.ctl);
             }
         }
         if (wib != 0) {
@@ -1430,8 +1436,9 @@ __device__ __forceinline__ void det_item(const EngineDev& eng, const SpikeRec* _
     for (uint64_t base = rb.x + (uint64_t)piece * psz; base < rb.y; base += (uint64_t)split * psz) {
         const uint64_t top = rb.y < base + psz ? rb.y : base + psz;
         for (uint64_t j = base + lane; j < top; j += 32) {
+            if (!NAER_IN_BOUNDS(eng.ctl, j, np->syn_cap, kChkEventList)) continue;
             const uint32_t tgt = __ldcg(tgt_a + j);
-            if (tgt == kTgtSentinel) continue;
+            if (tgt == kTgtSentinel || !NAER_IN_BOUNDS(eng.ctl, tgt, Ns, kChkRing)) continue;
             const uint32_t cell = ring_slot(tmod, __ldcg(d_a + j), D) * Ns + tgt;
             if (pass == 0) {
                 float w = __ldcg(w_a + j);

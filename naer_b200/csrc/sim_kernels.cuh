@@ -4,6 +4,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "check.cuh"
 #include "engine_types.cuh"
 #include "philox.cuh"
 

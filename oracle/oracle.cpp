@@ -112,6 +112,22 @@ uint32_t poisson_window(uint32_t idx, uint32_t n, uint32_t seed, double rate, ui
 
 extern "C" {
 
+// exp_interval_us of generator outputs z = z_first + i * z_step (mod 2^32),
+// with the host's (glibc) logarithm.
+void oracle_intervals(double rate, uint32_t z_first, uint32_t z_step, uint64_t count, uint32_t* out) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)count; ++i) {
+        const uint32_t z = z_first + (uint32_t)i * z_step;
+        if (z == 0xFFFFFFFFu) {
+            out[i] = 0xFFFFFFFFu;
+            continue;
+        }
+        const double x = (double)z / 4294967295.0;
+        const double dt = std::log(1.0 - x) / (-(rate / 1000000.0));
+        out[i] = dt < 4294967296.0 ? (uint32_t)dt : 0xFFFFFFFFu;
+    }
+}
+
 double oracle_uniform_rand(uint32_t gid, uint32_t seed, uint32_t iteration) {
     return uniform_rand(gid, seed, iteration);
 }

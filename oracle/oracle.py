@@ -59,6 +59,7 @@ def load() -> C.CDLL:
             "oracle_exp_interval_us": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double]),
             "oracle_poisson_window": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32,
                                                    C.c_uint32, _vp]),
+            "oracle_intervals": (None, [C.c_double, C.c_uint32, C.c_uint32, C.c_uint64, _vp]),
             "oracle_net_create": (_vp, [C.POINTER(OrParams), C.POINTER(OrPop), C.c_uint32, C.POINTER(OrConn),
                                         C.c_uint32]),
             "oracle_net_destroy": (None, [_vp]),
@@ -251,6 +252,13 @@ class OracleNet:
         self._lib.oracle_reintegrate_fp64_ex(self._h, int(nsteps), _ptr(st), _ptr(ii), len(st), _ptr(v), _ptr(w),
                                              C.byref(mis), 1, C.byref(lost))
         return v, w, mis.value, lost.value
+
+
+def intervals(rate: float, z_first: int, z_step: int, count: int) -> np.ndarray:
+    """The Poisson interval (µs) of z = z_first + i * z_step with glibc's log."""
+    out = np.empty(count, dtype=np.uint32)
+    load().oracle_intervals(float(rate), int(z_first), int(z_step), int(count), out.ctypes.data_as(C.c_void_p))
+    return out
 
 
 def max_threads() -> int:
