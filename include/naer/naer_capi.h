@@ -312,8 +312,8 @@ NAER_API int naer_test_fail_allocation(int64_t after);
  * 1 in that build, 0 in the normal one. */
 NAER_API int naer_build_checked(int* checked);
 /* First out-of-bounds access the checked build recorded for the network's
- * launches (*code 0 = none; 1 synapse arrays, 2 ring cell, 3 spike list,
- * 4 raster, 5 neuron state, 6 Poisson-count slot, 7 plasticity state,
+ * launches (*code 0 = none; 1 synapse arrays, 2 ring cell, 3 source of a
+ * queued spike, 5 neuron state of a LIF chunk, 6 Poisson-count slot,
  * 8 deterministic event list) and its index.  Always 0 in the normal
  * build.  Blocks like finish(). */
 NAER_API int naer_net_check_report(naer_net* net, uint32_t* code, uint64_t* index);

@@ -15,12 +15,10 @@ enum CheckCode : uint32_t {
     kChkNone = 0,
     kChkSynapse = 1,    // synapse array offset (target / weight / delay)
     kChkRing = 2,       // ring cell
-    kChkQueue = 3,      // spike list position
-    kChkRaster = 4,     // raster record
-    kChkState = 5,      // neuron state / ring slot of a LIF chunk
+    kChkQueue = 3,      // source of a queued spike
+    kChkState = 5,      // neuron state of a LIF chunk
     kChkDrive = 6,      // Poisson-count slot
-    kChkPlastic = 7,    // post row / pre trace of a plastic neuron
-    kChkEventList = 8,  // deterministic event list (synapse slot or cell head)
+    kChkEventList = 8,  // deterministic event list (synapse slot)
 };
 
 #ifdef NAER_CHECKED
