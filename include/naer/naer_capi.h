@@ -371,6 +371,10 @@ typedef struct naer_tuning {
     uint32_t neuron_state;    /* NAER_STATE_*: where the step kernel keeps membrane potentials and
                                  refractory counters during a launch */
     uint32_t step_kernel;     /* NAER_KERNEL_*: which persistent step kernel runs */
+    uint32_t bins;            /* SPLIT kernel: entries (a power of two, 64..8192) of the per-block
+                                 shared-memory table that folds ring reductions to the same cell
+                                 before they reach L2; 0 = every event reduces in L2 directly */
+    uint32_t pad_;
 } naer_tuning;
 
 /* naer_tuning.step_kernel.  SPLIT: one contiguous spike list per step,

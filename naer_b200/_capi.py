@@ -114,6 +114,8 @@ class Tuning(C.Structure):
         ("scatter_piece", C.c_uint32),
         ("neuron_state", C.c_uint32),
         ("step_kernel", C.c_uint32),
+        ("bins", C.c_uint32),
+        ("pad_", C.c_uint32),
     ]
 
 

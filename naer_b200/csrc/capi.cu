@@ -668,6 +668,7 @@ static void fill_tuning(naer_tuning* out, const naer::Tuning& t, uint32_t graph_
     out->scatter_piece = t.scatter_piece;
     out->neuron_state = t.neuron_state;
     out->step_kernel = t.step_kernel;
+    out->bins = t.bins;
     out->graph_launches = graph_launches;
 }
 
@@ -708,6 +709,7 @@ int naer_net_set_tuning(naer_net* net, const naer_tuning* tuning) {
         t.scatter_piece = tuning->scatter_piece;
         t.neuron_state = tuning->neuron_state;
         t.step_kernel = tuning->step_kernel;
+        t.bins = tuning->bins;
         net->eng->set_tuning(t);
     });
 }
@@ -731,6 +733,7 @@ int naer_batch_set_tuning(naer_batch* batch, const naer_tuning* tuning) {
         t.scatter_piece = tuning->scatter_piece;
         t.neuron_state = tuning->neuron_state;
         t.step_kernel = tuning->step_kernel;
+        t.bins = tuning->bins;
         batch->b->engine().set_tuning(t);
         batch->graph_launches = tuning->graph_launches;
     });

@@ -269,7 +269,7 @@ uint32_t Engine::fast_chunk_capacity(uint32_t aggregation) {
     const int bps_hi = tuning_.blocks_per_sm ? (int)std::min<uint32_t>(tuning_.blocks_per_sm, 4) : 4;
     auto fits = [&](int bps, uint32_t own) {
         const uint32_t grid = (uint32_t)bps * (uint32_t)sm_count_;
-        const size_t smem = split ? step_smem_bytes(own, true) : run_smem_bytes(grid, own, true);
+        const size_t smem = split ? step_smem_bytes(own, true, det ? 0u : tuning_.bins) : run_smem_bytes(grid, own, true);
         if (smem > (size_t)optin) return false;
         int occ = 0;
         NAER_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kLifThreads, smem));
@@ -786,8 +786,9 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
                                 : split_kernel_ ? (const void*)k_step<true> : (const void*)k_run<true>;
     const void* kern_glob = det ? (const void*)k_det_step<false>
                                 : split_kernel_ ? (const void*)k_step<false> : (const void*)k_run<false>;
+    const uint32_t bins = split_kernel_ ? tuning_.bins : 0u;
     auto smem_of = [&](uint32_t grid, uint32_t own, bool state) {
-        return list_kernel ? step_smem_bytes(own, state) : run_smem_bytes(grid, own, state);
+        return list_kernel ? step_smem_bytes(own, state, bins) : run_smem_bytes(grid, own, state);
     };
     det_scratch_ = kScratchNone;  // the next deterministic call points the new tables at its scratch
     int dev_smem_optin = 0;
@@ -901,6 +902,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     eng_.split_rest = (uint32_t)std::min<uint64_t>(cap_split, std::max<uint64_t>(1, (max_rest + psz - 1) / psz));
     if (tuning_.scatter_split) eng_.split_first = eng_.split_rest = std::min<uint32_t>(tuning_.scatter_split, 64);
     eng_.queue_cap = (uint32_t)qentries;
+    eng_.bins = bins;
     if (qentries * std::max(eng_.split_first, eng_.split_rest) > 0xFFFFFFFFull)
         throw Error(NAER_E_OVERFLOW, "spike list times warps per spike exceeds 2^32 work items");
     NAER_CK(cudaStreamSynchronize(stream_));  // tables and buffers complete for every stream
@@ -915,6 +917,8 @@ void Engine::set_tuning(const Tuning& t) {
         throw Error(NAER_E_INVALID, "scatter_piece must be 0, 128 or 256");
     if (v.neuron_state > NAER_STATE_GLOBAL) throw Error(NAER_E_INVALID, "unknown neuron_state");
     if (v.step_kernel > NAER_KERNEL_TWO_BARRIER) throw Error(NAER_E_INVALID, "unknown step_kernel");
+    if (v.bins != 0 && (v.bins < 64 || v.bins > 8192 || (v.bins & (v.bins - 1))))
+        throw Error(NAER_E_INVALID, "bins must be 0 or a power of two in 64..8192");
     tuning_ = v;
     if (!nets_.empty()) install(std::vector<NetHost*>(nets_), inst_raster_cap_, inst_record_, aggregation_);
 }
@@ -961,6 +965,9 @@ TuneResult Engine::autotune(uint32_t trial_steps) {
                     }
                     if (bps == 1 && L == kDriveSlots && sp == 0 && aggregation_ != NAER_AGG_DETERMINISTIC)
                         t.step_kernel = NAER_KERNEL_TWO_BARRIER;
+                    // shared-memory binning of the ring reductions
+                    if (bps == 0 && L == kDriveSlots / 2 && sp == 0 && aggregation_ != NAER_AGG_DETERMINISTIC)
+                        t.bins = 2048;
                     const double us = trial(t);
                     if (us < r.best_us_per_step) {
                         r.best_us_per_step = us;

@@ -116,6 +116,7 @@ struct Tuning {
     uint32_t scatter_piece = 0;            // synapses per warp iteration: 128, 256, 0 = 128 with STDP else 256
     uint32_t neuron_state = 0;             // NAER_STATE_AUTO / _SHARED / _GLOBAL: where the step kernel keeps V
     uint32_t step_kernel = 0;              // NAER_KERNEL_SPLIT (k_step) / NAER_KERNEL_TWO_BARRIER (k_run)
+    uint32_t bins = 0;                     // k_step shared-memory binning table entries (0 = off)
 };
 
 struct TuneResult {

@@ -192,6 +192,7 @@ struct EngineDev {
     uint32_t split_first;
     uint32_t split_rest;
     uint32_t queue_cap;             // entries of queue[i] / qid[i]
+    uint32_t bins;                  // k_step: shared-memory binning table entries (power of 2), 0 = off
 };
 
 }  // namespace naer

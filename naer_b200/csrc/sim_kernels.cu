@@ -201,10 +201,10 @@ __global__ void __launch_bounds__(kLifThreads, NAER_DRIVE_MIN_BLOCKS)
 // counts).
 //
 // Grid-mode restatement of neuron_dynamics (include/naer/kernels/lif.cl:15-34)
-// on a fixed step: V <- fp32(fp64(V) * exp(-dt/tau)); V += ring input; V +=
-// drive weight once per Poisson drive event; spike iff V > v_th, then
-// V = v_reset and t_ref steps of refractoriness, during which input is
-// discarded.  POISSON populations emit the step's count of their reference
+// on a fixed step: V <- fp32(fp64(V) * exp(-dt/tau) + ring input + m * drive
+// weight) for m Poisson drive events, in double with one rounding
+// (lif_update); spike iff V > v_th, then V = v_reset and t_ref steps of
+// refractoriness, during which input is discarded.  POISSON populations emit the step's count of their reference
 // generator (input_neuron_group.cl:6-45), drawn ahead by drive_chunks.
 //
 // Spikes are compacted with one ballot per neuron slot and one shared-memory
@@ -269,9 +269,7 @@ __device__ __forceinline__ void lif_chunk(const EngineDev& eng, uint32_t c, unsi
                 rr[j] -= 1;
                 continue;
             }
-            float v = __double2float_rn(__dmul_rn((double)vv[j], p.prop));
-            v = __fadd_rn(v, f4_get(I, j));
-            for (uint32_t k = 0; k < drive[j]; ++k) v = __fadd_rn(v, p.drive_w);
+            float v = lif_update(vv[j], p.prop, f4_get(I, j), drive[j], p.drive_w);
             if (v > p.v_th) {
                 v = p.v_reset;
                 rr[j] = p.t_ref_steps;
@@ -536,9 +534,7 @@ __device__ __forceinline__ void lif_chunk_smem(const EngineDev& eng, const Chunk
                 rr[k] -= 1;
                 continue;
             }
-            float v = __double2float_rn(__dmul_rn((double)vv[k], prop));
-            v = __fadd_rn(v, f4_get(I, k));
-            for (uint32_t m = 0; m < dd[k]; ++m) v = __fadd_rn(v, dw);
+            float v = lif_update(vv[k], prop, f4_get(I, k), dd[k], dw);
             if (v > v_th) {
                 v = v_reset;
                 rr[k] = cc.p.t_ref_steps;
@@ -773,12 +769,68 @@ template __global__ void k_run<false>(EngineDev, unsigned long long, uint32_t);
 // Every delivery is a red.add into the ring as in k_run; only the time at
 // which a synapse is delivered moves, never its ring slot.
 
+// Shared-memory binning of ring reductions (tuning `bins`, 0 = off).  A
+// block folds events into an open-addressing table keyed by ring-cell
+// address (shared-memory atomics), and a flush issues one global reduction
+// per occupied entry before the block publishes its deliveries at a grid
+// barrier.  Events whose probe finds no entry go to global memory directly.
+// It pays where many events of a block hit the same cells (convergent or
+// hub targets, whose global reductions to one address serialize in L2); on
+// uniformly random targets it only adds work.
+struct BinTable {
+    unsigned long long* key;  // ring-cell address, 0 = empty
+    float* sum;
+    uint32_t mask;            // entries - 1; 0 = binning off
+};
+
+constexpr int kBinProbes = 4;
+
+__device__ __forceinline__ void ring_add(const BinTable& bt, float* addr, float w) {
+    if (bt.mask) {
+        const unsigned long long a = (unsigned long long)addr;
+        uint32_t h = (uint32_t)(((a >> 2) * 0x9E3779B97F4A7C15ull) >> 40) & bt.mask;
+#pragma unroll
+        for (int p = 0; p < kBinProbes; ++p) {
+            const unsigned long long k = *(volatile unsigned long long*)(bt.key + h);
+            if (k == a) {
+                atomicAdd(bt.sum + h, w);
+                return;
+            }
+            if (k == 0ull) {
+                const unsigned long long old = atomicCAS(bt.key + h, 0ull, a);
+                if (old == 0ull || old == a) {
+                    atomicAdd(bt.sum + h, w);
+                    return;
+                }
+            }
+            h = (h + 1) & bt.mask;
+        }
+    }
+    red_add_f32(addr, w);
+}
+
+// Every thread of the block: issues the table's sums and empties it.
+__device__ __forceinline__ void flush_bins(const BinTable& bt) {
+    if (!bt.mask) return;  // uniform over the block
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i <= bt.mask; i += blockDim.x) {
+        const unsigned long long a = bt.key[i];
+        if (a) {
+            red_add_f32(reinterpret_cast<float*>(a), bt.sum[i]);
+            bt.key[i] = 0ull;
+            bt.sum[i] = 0.0f;
+        }
+    }
+    __syncthreads();
+}
+
 // Delivers the synapses [lo, hi) of one spike's row: warp pieces piece,
 // piece + split, ... of psz synapses, 128-bit loads, red.add into the ring
 // (STDP update first for plastic synapses of plastic sources).
 __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, const SpikeRec& r, uint64_t lo,
                                              uint64_t hi, uint32_t piece, uint32_t split, uint32_t psz,
-                                             uint32_t lane, unsigned long long& ev, uint32_t& ovf, Ctl* ctl) {
+                                             uint32_t lane, unsigned long long& ev, uint32_t& ovf, Ctl* ctl,
+                                             const BinTable& bt) {
     const uint32_t D = np->ring_slots;
     const uint32_t tmod = tl % D;
     const uint32_t Ns = np->n_storage;
@@ -822,7 +874,7 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
                     __stcg(w_a + off + j, w);
                 }
                 if (mult != 1.0f) w = __fmul_rn(w, mult);
-                red_add_f32(ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w);
+                ring_add(bt, ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w);
                 ++ev;
             }
         }
@@ -832,7 +884,8 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
 // deliver_span for a static source (no plasticity): the deferred rest.
 __device__ __forceinline__ void deliver_static_span(const NetDev* np, uint32_t tl, int32_t aux0, uint64_t lo,
                                                     uint64_t hi, uint32_t piece, uint32_t split, uint32_t psz,
-                                                    uint32_t lane, unsigned long long& ev, Ctl* ctl) {
+                                                    uint32_t lane, unsigned long long& ev, Ctl* ctl,
+                                                    const BinTable& bt) {
     const uint32_t D = np->ring_slots;
     const uint32_t tmod = tl % D;
     const uint32_t Ns = np->n_storage;
@@ -866,7 +919,7 @@ __device__ __forceinline__ void deliver_static_span(const NetDev* np, uint32_t t
                 if (tgt == kTgtSentinel || !NAER_IN_BOUNDS(ctl, tgt, Ns, kChkRing)) continue;
                 float w = f4_get(ww[u], j);
                 if (mult != 1.0f) w = __fmul_rn(w, mult);
-                red_add_f32(ring + (size_t)ring_slot(tmod, (dd[u] >> (8 * j)) & 0xFFu, D) * Ns + tgt, w);
+                ring_add(bt, ring + (size_t)ring_slot(tmod, (dd[u] >> (8 * j)) & 0xFFu, D) * Ns + tgt, w);
                 ++ev;
             }
         }
@@ -906,10 +959,7 @@ __device__ __forceinline__ uint32_t lif_flags_smem(const ChunkCache& cc, uint32_
             rr[k] -= 1;
             continue;
         }
-        float v = __double2float_rn(__dmul_rn((double)vv[k], prop));
-        v = __fadd_rn(v, f4_get(I, k));
-        const uint32_t m = (Dw >> (8 * k)) & 0xFFu;
-        for (uint32_t q = 0; q < m; ++q) v = __fadd_rn(v, dw);
+        float v = lif_update(vv[k], prop, f4_get(I, k), (Dw >> (8 * k)) & 0xFFu, dw);
         if (v > v_th) {
             v = v_reset;
             rr[k] = tref;
@@ -991,7 +1041,7 @@ struct RestWork {
 };
 
 __device__ __forceinline__ void rest_item(const EngineDev& eng, const RestWork& rw, uint32_t it, const NetDev* net0,
-                                          uint32_t lane, unsigned long long& ev) {
+                                          uint32_t lane, unsigned long long& ev, const BinTable& bt) {
     const uint32_t split = eng.split_rest;
     const uint32_t e = it / split;
     const uint32_t piece = it - e * split;
@@ -1002,7 +1052,7 @@ __device__ __forceinline__ void rest_item(const EngineDev& eng, const RestWork& 
     const ulonglong2 rb = row_bounds(np->row_ptr, src);
     const uint64_t mid = rb.x + __ldg(np->row_mid + src);
     deliver_static_span(np, (uint32_t)(rw.step - np->start_step), rv.z, mid, rb.y, piece, split, eng.scatter_piece,
-                        lane, ev, eng.ctl);
+                        lane, ev, eng.ctl, bt);
 }
 
 // Chunk descriptors, membrane potentials and refractory counters of the
@@ -1155,10 +1205,7 @@ __device__ __forceinline__ void lif_phase(const EngineDev& eng, unsigned long lo
                             rr[q] -= 1;
                             continue;
                         }
-                        float v = __double2float_rn(__dmul_rn((double)vv[q], p.prop));
-                        v = __fadd_rn(v, f4_get(Iv, q));
-                        const uint32_t m = (Dw >> (8 * q)) & 0xFFu;
-                        for (uint32_t z = 0; z < m; ++z) v = __fadd_rn(v, p.drive_w);
+                        float v = lif_update(vv[q], p.prop, f4_get(Iv, q), (Dw >> (8 * q)) & 0xFFu, p.drive_w);
                         if (v > p.v_th) {
                             v = p.v_reset;
                             rr[q] = p.t_ref_steps;
@@ -1216,7 +1263,15 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         s_bar_target = 0;
     }
     const uint32_t own_max = eng.region_cap / kLifChunk;
-    const size_t off_cc = 16;
+    BinTable bt;
+    bt.key = reinterpret_cast<unsigned long long*>(s_dyn + 16);
+    bt.sum = reinterpret_cast<float*>(bt.key + eng.bins);
+    bt.mask = eng.bins ? eng.bins - 1 : 0u;
+    for (uint32_t i = threadIdx.x; i < eng.bins; i += blockDim.x) {
+        bt.key[i] = 0ull;
+        bt.sum[i] = 0.0f;
+    }
+    const size_t off_cc = step_smem_offset(eng.bins);
     ChunkCache* s_cc = reinterpret_cast<ChunkCache*>(s_dyn + off_cc);
     const size_t off_v = off_cc + (((size_t)own_max * sizeof(ChunkCache) + 15) & ~(size_t)15);
     float4* sV = reinterpret_cast<float4*>(s_dyn + off_v);
@@ -1253,7 +1308,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         } else {
             while (rit < s_rw.n) {
                 if (*(volatile int*)&s_flag) break;
-                rest_item(eng, s_rw, rit, &s_net0, lane, ev);
+                rest_item(eng, s_rw, rit, &s_net0, lane, ev, bt);
                 rit += WR;
             }
         }
@@ -1283,11 +1338,11 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
                 const bool plastic_src = np->stdp_on && r.src < np->n_plastic;
                 const uint64_t hi = plastic_src ? rb.y : rb.x + __ldg(np->row_mid + r.src);
                 deliver_span(np, (uint32_t)(s - np->start_step), r, rb.x, hi, piece, split, psz, lane, ev, ovf,
-                             eng.ctl);
+                             eng.ctl, bt);
             }
         }
         if (wib != 0) {
-            for (; rit < s_rw.n; rit += WR) rest_item(eng, s_rw, rit, &s_net0, lane, ev);
+            for (; rit < s_rw.n; rit += WR) rest_item(eng, s_rw, rit, &s_net0, lane, ev, bt);
         }
         {
             const unsigned long long cap = eng.record ? eng.raster_cap : 0ull;
@@ -1295,6 +1350,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
             if (eng.record && threadIdx.x == 0) s_dropped += Q - kept;
             rbase += kept;
         }
+        flush_bins(bt);  // everything binned since the last barrier, before this block's arrival
         __syncthreads();
         const unsigned long long tb2 = timer ? globaltimer_ns() : 0ull;
         // ---- 4. B2: warps 1.. deliver step s's rest while warp 0 waits for it
@@ -1314,7 +1370,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         } else {
             while (rit < s_rw.n) {
                 if (*(volatile int*)&s_flag) break;
-                rest_item(eng, s_rw, rit, &s_net0, lane, ev);
+                rest_item(eng, s_rw, rit, &s_net0, lane, ev, bt);
                 rit += WR;
             }
         }
@@ -1331,7 +1387,8 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
     }
     // the last step's rest (the next launch's LIF reads it in stream order)
     if (s_ok && wib != 0)
-        for (; rit < s_rw.n; rit += WR) rest_item(eng, s_rw, rit, &s_net0, lane, ev);
+        for (; rit < s_rw.n; rit += WR) rest_item(eng, s_rw, rit, &s_net0, lane, ev, bt);
+    flush_bins(bt);
     if (kSmem) store_chunk_state(own, s_cc, sV, sR);
     finish_counters(eng, ev, ovf, lane, &s_ev, &s_ovf);
     if (timer) {
@@ -1557,8 +1614,8 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
 template __global__ void k_det_step<true>(EngineDev, unsigned long long, uint32_t);
 template __global__ void k_det_step<false>(EngineDev, unsigned long long, uint32_t);
 
-size_t step_smem_bytes(uint32_t own_max, bool smem_state) {
-    const size_t off_cc = 16;
+size_t step_smem_bytes(uint32_t own_max, bool smem_state, uint32_t bins) {
+    const size_t off_cc = step_smem_offset(bins);
     if (!smem_state) return off_cc;
     const size_t off_v = off_cc + (((size_t)own_max * sizeof(ChunkCache) + 15) & ~(size_t)15);
     return off_v + (size_t)own_max * kLifThreads * (sizeof(float4) + sizeof(uchar4));

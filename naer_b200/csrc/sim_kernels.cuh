@@ -52,6 +52,18 @@ __device__ __forceinline__ uint32_t poisson_count(const PopDev& p, uint32_t idx,
     return poisson_exact(p.rate_hz, p.rng_seed, p.rng_n, idx, key0, z0, t0, t1);
 }
 
+// One grid step of a neuron that is not refractory: exponential decay by
+// the fp64 propagator, the ring input and m Poisson drive events of weight
+// dw, all in double arithmetic (m * dw is exact) and rounded to fp32 once.
+// One rounding per step keeps the fp32 state within 1e-5 relative of an
+// fp64 integration even when large drive weights pass through the sum.
+__device__ __forceinline__ float lif_update(float v, double prop, float I, uint32_t m, float dw) {
+    double x = __dmul_rn((double)v, prop);
+    x = __dadd_rn(x, (double)I);
+    if (m) x = __dadd_rn(x, __dmul_rn((double)m, (double)dw));
+    return __double2float_rn(x);
+}
+
 __device__ __forceinline__ float decay_lookup(const float* table, uint32_t len, int32_t k) {
     return (k >= 0 && (uint32_t)k < len) ? __ldg(table + k) : 0.0f;
 }
@@ -188,8 +200,13 @@ template <bool kSmem>
 __global__ void k_det_step(EngineDev eng, unsigned long long s0, uint32_t nsteps);
 // dynamic shared memory of k_run for a grid and a number of owned chunks per block
 size_t run_smem_bytes(uint32_t grid, uint32_t own_max, bool smem_state);
-// dynamic shared memory of k_step / k_det_step for a number of owned chunks per block
-size_t step_smem_bytes(uint32_t own_max, bool smem_state);
+// dynamic shared memory of k_step / k_det_step for a number of owned chunks
+// per block and a binning table of `bins` entries (k_step only; 0 = none)
+size_t step_smem_bytes(uint32_t own_max, bool smem_state, uint32_t bins = 0);
+// offset of the chunk caches in that memory: 16 bytes, then the table
+__host__ __device__ inline size_t step_smem_offset(uint32_t bins) {
+    return 16 + ((((size_t)bins * 12) + 15) & ~(size_t)15);
+}
 // Poisson counts of up to kDriveSlots steps ahead
 __global__ void k_drive(EngineDev eng, unsigned long long s_first, uint32_t nsteps);
 

@@ -70,10 +70,10 @@ class Batch:
         return {k: getattr(t, k) for k, _ in capi.Tuning._fields_ if k != "pad_"}
 
     def set_tuning(self, blocks_per_sm=0, launch_steps=64, scatter_split=0, graph_launches=16,
-                   scatter_piece=0, neuron_state=capi.STATE_AUTO, step_kernel=capi.KERNEL_SPLIT) -> None:
+                   scatter_piece=0, neuron_state=capi.STATE_AUTO, step_kernel=capi.KERNEL_SPLIT, bins=0) -> None:
         t = capi.Tuning(blocks_per_sm=blocks_per_sm, launch_steps=launch_steps, scatter_split=scatter_split,
                         graph_launches=graph_launches, scatter_piece=scatter_piece, neuron_state=neuron_state,
-                        step_kernel=step_kernel)
+                        step_kernel=step_kernel, bins=bins)
         capi.call("naer_batch_set_tuning", self._h, C.byref(t))
 
     def stats(self) -> dict:

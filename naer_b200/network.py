@@ -214,9 +214,9 @@ class Network:
 
     def set_tuning(self, blocks_per_sm: int = 0, launch_steps: int = 64, scatter_split: int = 0,
                    scatter_piece: int = 0, neuron_state: int = capi.STATE_AUTO,
-                   step_kernel: int = capi.KERNEL_SPLIT) -> None:
+                   step_kernel: int = capi.KERNEL_SPLIT, bins: int = 0) -> None:
         t = capi.Tuning(blocks_per_sm=blocks_per_sm, launch_steps=launch_steps, scatter_split=scatter_split,
-                        scatter_piece=scatter_piece, neuron_state=neuron_state, step_kernel=step_kernel)
+                        scatter_piece=scatter_piece, neuron_state=neuron_state, step_kernel=step_kernel, bins=bins)
         capi.call("naer_net_set_tuning", self._h, C.byref(t))
 
     def get_tuning(self) -> dict:

@@ -518,13 +518,15 @@ void grid_step(Net& net) {
                 net.refr[i] -= 1;
                 continue;
             }
-            float v = (float)((double)net.v[i] * prop[pi]);
-            v = v + I;
+            // decay, ring input and drive in double, one rounding to fp32
+            double x = (double)net.v[i] * prop[pi];
+            x = x + (double)I;
             if (pop.drive_rate_hz > 0.0f) {
                 const uint32_t m = poisson_window(i - net.base[pi], pop.size, pop.drive_seed,
                                                   (double)pop.drive_rate_hz, t0, t1, nullptr);
-                for (uint32_t k = 0; k < m; ++k) v = v + pop.drive_weight;
+                if (m) x = x + (double)m * (double)pop.drive_weight;
             }
+            float v = (float)x;
             if (v > pop.v_th) {
                 v = pop.v_reset;
                 net.refr[i] = tref[pi];
