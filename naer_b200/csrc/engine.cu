@@ -136,6 +136,7 @@ Engine::~Engine() {
     for (int i = 0; i < 2; ++i) {
         f(d_queue_[i]);
         f(d_qid_[i]);
+        f(d_qrow_[i]);
         f(d_counts_[i]);
     }
     f(d_ev_part_);
@@ -839,6 +840,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     for (int i = 0; i < 2; ++i) {
         regrow(reinterpret_cast<void*&>(d_queue_[i]), queue_bytes_[i], qentries * sizeof(SpikeRec));
         regrow(reinterpret_cast<void*&>(d_qid_[i]), qid_bytes_[i], qentries * sizeof(uint32_t));
+        regrow(reinterpret_cast<void*&>(d_qrow_[i]), qrow_bytes_[i], qentries * sizeof(uint4));
         regrow(reinterpret_cast<void*&>(d_counts_[i]), counts_bytes_[i], (lif_grid_ + 1) * sizeof(uint32_t));
         NAER_CK(cudaMemsetAsync(d_counts_[i], 0, (lif_grid_ + 1) * sizeof(uint32_t), stream_));
     }
@@ -864,6 +866,7 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     for (int i = 0; i < 2; ++i) {
         eng_.queue[i] = d_queue_[i];
         eng_.qid[i] = d_qid_[i];
+        eng_.qrow[i] = d_qrow_[i];
         eng_.counts[i] = d_counts_[i];
     }
     eng_.ev_part = d_ev_part_;

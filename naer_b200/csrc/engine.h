@@ -244,6 +244,8 @@ private:
     Ctl* d_ctl_ = nullptr;
     SpikeRec* d_queue_[2] = {nullptr, nullptr};
     uint32_t* d_qid_[2] = {nullptr, nullptr};
+    uint4* d_qrow_[2] = {nullptr, nullptr};
+    size_t qrow_bytes_[2] = {0, 0};
     uint32_t* d_counts_[2] = {nullptr, nullptr};
     unsigned long long* d_ev_part_ = nullptr;
     unsigned long long* d_ovf_part_ = nullptr;

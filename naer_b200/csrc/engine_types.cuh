@@ -174,6 +174,8 @@ struct EngineDev {
     const ChunkDev* chunks;
     SpikeRec* queue[2];
     uint32_t* qid[2];               // reference address of each queued spike
+    uint4* qrow[2];                 // k_step / k_det_step: row of each queued spike {begin lo, begin hi,
+                                    // delay-1 part length, row length}, written with the record
     uint32_t* counts[2];            // [lif_grid] spikes per LIF block region
     unsigned long long* ev_part;    // [scatter_grid] events delivered, per scatter block
     unsigned long long* ovf_part;   // [scatter_grid] lazy-LTP history overflows, per block

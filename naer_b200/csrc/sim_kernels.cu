@@ -450,6 +450,8 @@ __device__ __forceinline__ void scatter_step(const EngineDev& eng, unsigned long
 // memory for the whole launch.
 struct ChunkCache {
     PopDev p;
+    const uint64_t* row_ptr;  // the net's CSR rows (queued spikes carry their bounds)
+    const uint32_t* row_mid;
     float* ring;
     float* v;
     uint8_t* refr;
@@ -809,6 +811,20 @@ __device__ __forceinline__ void ring_add(const BinTable& bt, float* addr, float 
     red_add_f32(addr, w);
 }
 
+// One warp, while the block's other warps may still add to the table:
+// issues every entry's sum taken by atomic exchange (an add racing with it
+// lands before, in this flush, or after, in the next); keys stay.
+__device__ __forceinline__ void flush_bins_warp(const BinTable& bt, uint32_t lane) {
+    if (!bt.mask) return;
+    for (uint32_t i = lane; i <= bt.mask; i += 32) {
+        const unsigned long long a = *(volatile unsigned long long*)(bt.key + i);
+        if (a) {
+            const float v = atomicExch(bt.sum + i, 0.0f);
+            if (v != 0.0f) red_add_f32(reinterpret_cast<float*>(a), v);
+        }
+    }
+}
+
 // Every thread of the block: issues the table's sums and empties it.
 __device__ __forceinline__ void flush_bins(const BinTable& bt) {
     if (!bt.mask) return;  // uniform over the block
@@ -992,16 +1008,29 @@ __device__ __forceinline__ uint32_t reserve_places(Ctl* ctl, unsigned long long 
 
 // Writes one spike record: POISSON sources carry their multiplicity,
 // plastic neurons run their post-spike bookkeeping here.
+// Row of a spiking neuron: {begin lo, begin hi, delay-1 part length, row
+// length}, read once at LIF time so that the scatter's first load already
+// names the synapses.
+__device__ __forceinline__ uint4 row_of(const uint64_t* row_ptr, const uint32_t* row_mid, uint32_t i) {
+    const unsigned long long b = __ldg(reinterpret_cast<const unsigned long long*>(row_ptr) + i);
+    const unsigned long long e = __ldg(reinterpret_cast<const unsigned long long*>(row_ptr) + i + 1);
+    const uint32_t m = __ldg(row_mid + i);
+    return make_uint4((uint32_t)b, (uint32_t)(b >> 32), m, (uint32_t)(e - b));
+}
+
 __device__ __forceinline__ void write_spike(const EngineDev& eng, SpikeRec* __restrict__ queue,
                                             uint32_t* __restrict__ qid, uint32_t pos, uint32_t net, uint32_t i,
-                                            const PopDev& p, bool plastic, uint32_t tl, uint32_t count) {
+                                            const PopDev& p, bool plastic, uint32_t tl, uint32_t count,
+                                            const uint4 row) {
     int32_t aux0 = 0;
     float aux1 = 0.0f;
     if (p.type == kPOISSON) aux0 = (int32_t)count;
     else if (plastic) stdp_post_spike(eng.nets + net, i, (int32_t)tl, aux0, aux1);
     if (pos < eng.queue_cap) {
+        const uint32_t qb = (uint32_t)(queue == eng.queue[1]);
         __stcg(reinterpret_cast<int4*>(queue + pos), make_int4((int)net, (int)i, aux0, __float_as_int(aux1)));
         __stcg(qid + pos, p.id_base + (i - p.storage_base));
+        __stcg(eng.qrow[qb] + pos, row);
     } else {
         atomicCAS(&eng.ctl->error, 0u, (unsigned int)(-NAER_STATUS_OVERFLOW));
     }
@@ -1046,13 +1075,13 @@ __device__ __forceinline__ void rest_item(const EngineDev& eng, const RestWork& 
     const uint32_t e = it / split;
     const uint32_t piece = it - e * split;
     const int4 rv = __ldcg(reinterpret_cast<const int4*>(eng.queue[rw.qb] + e));
+    const uint4 row = __ldcg(eng.qrow[rw.qb] + e);  // issued with the record: no dependent row lookup
     const uint32_t net = (uint32_t)rv.x, src = (uint32_t)rv.y;
     const NetDev* np = net == 0 ? net0 : eng.nets + net;
     if (np->stdp_on && src < np->n_plastic) return;  // plastic rows went whole with the first part
-    const ulonglong2 rb = row_bounds(np->row_ptr, src);
-    const uint64_t mid = rb.x + __ldg(np->row_mid + src);
-    deliver_static_span(np, (uint32_t)(rw.step - np->start_step), rv.z, mid, rb.y, piece, split, eng.scatter_piece,
-                        lane, ev, eng.ctl, bt);
+    const uint64_t beg = ((uint64_t)row.y << 32) | row.x;
+    deliver_static_span(np, (uint32_t)(rw.step - np->start_step), rv.z, beg + row.z, beg + row.w, piece, split,
+                        eng.scatter_piece, lane, ev, eng.ctl, bt);
 }
 
 // Chunk descriptors, membrane potentials and refractory counters of the
@@ -1066,6 +1095,8 @@ __device__ __forceinline__ void load_chunk_state(const EngineDev& eng, uint32_t 
         const NetDev* np = eng.nets + ch.net;
         ChunkCache c;
         c.p = eng.pops[ch.pop];
+        c.row_ptr = np->row_ptr;
+        c.row_mid = np->row_mid;
         c.ring = np->ring;
         c.v = np->v;
         c.refr = np->refr;
@@ -1150,7 +1181,16 @@ __device__ __forceinline__ void lif_phase(const EngineDev& eng, unsigned long lo
             for (uint32_t b = 0; b < kLifBatch; ++b)
                 if (j0 + b < own) mask |= lif_flags_smem(s_cc[j0 + b], j0 + b, s, sV, sR, I[b], Dw[b]) << (4 * b);
             if (__any_sync(0xFFFFFFFFu, mask != 0)) {
+                // the row of the lane's first spike is loaded while the
+                // reservation's atomic is in flight (most lanes have one)
+                uint4 row0 = make_uint4(0, 0, 0, 0);
+                if (mask) {
+                    const uint32_t bit = __ffs(mask) - 1u;
+                    const ChunkCache& cc = s_cc[j0 + (bit >> 2)];
+                    row0 = row_of(cc.row_ptr, cc.row_mid, cc.first + threadIdx.x * kLifPerThread + (bit & 3u));
+                }
                 uint32_t pos = reserve_places(ctl, s, __popc(mask), lane);
+                bool first = true;
 #pragma unroll
                 for (uint32_t b = 0; b < kLifBatch; ++b) {
                     const uint32_t m4 = (mask >> (4 * b)) & 0xFu;
@@ -1160,9 +1200,12 @@ __device__ __forceinline__ void lif_phase(const EngineDev& eng, unsigned long lo
                     const uint32_t tl = (uint32_t)(s - cc.start);
 #pragma unroll
                     for (int q = 0; q < 4; ++q)
-                        if ((m4 >> q) & 1u)
+                        if ((m4 >> q) & 1u) {
+                            const uint4 row = first ? row0 : row_of(cc.row_ptr, cc.row_mid, i0 + q);
+                            first = false;
                             write_spike(eng, queue, qid, pos++, cc.net, i0 + q, cc.p, cc.plastic != 0, tl,
-                                        (Dw[b] >> (8 * q)) & 0xFFu);
+                                        (Dw[b] >> (8 * q)) & 0xFFu, row);
+                        }
                 }
             }
         }
@@ -1223,8 +1266,9 @@ __device__ __forceinline__ void lif_phase(const EngineDev& eng, unsigned long lo
                 const bool plastic = p.type == kSTDP && np->stdp_on;
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    if ((f >> q) & 1u) write_spike(eng, queue, qid, pos++, ch.net, i0 + q, p, plastic, tl,
-                                                   (Dw >> (8 * q)) & 0xFFu);
+                    if ((f >> q) & 1u)
+                        write_spike(eng, queue, qid, pos++, ch.net, i0 + q, p, plastic, tl, (Dw >> (8 * q)) & 0xFFu,
+                                    row_of(np->row_ptr, np->row_mid, i0 + q));
             }
         }
     }
@@ -1239,7 +1283,8 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
     __shared__ NetDev s_net0;  // descriptor of the first net (the only one in the plain form)
     __shared__ BarrierCfg bcfg;
     __shared__ int s_flag, s_ok;
-    __shared__ RestWork s_rw;                        // deferred work of the previous step
+    __shared__ RestWork s_rw[2];                     // deferred work of steps by parity
+    __shared__ uint32_t s_done, s_q;                 // warps done with a step's due work; its list size
     __shared__ unsigned long long s_ph[5], s_dropped;  // thread 0 only
     __shared__ unsigned long long s_bar_target;      // thread 0 only
     const uint32_t G = gridDim.x;
@@ -1257,7 +1302,10 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         s_ovf = 0;
         s_ok = 1;
         s_flag = 0;
-        s_rw = RestWork{0, 0, 0};  // nothing deferred at launch start
+        s_rw[0] = RestWork{0, 0, 0};  // nothing deferred at launch start
+        s_rw[1] = RestWork{0, 0, 0};
+        s_done = 0;
+        s_q = 0;
         for (int q = 0; q < 5; ++q) s_ph[q] = 0;
         s_dropped = 0;
         s_bar_target = 0;
@@ -1298,17 +1346,24 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         __syncthreads();
         const unsigned long long ta2 = timer ? globaltimer_ns() : 0ull;
         // ---- 2. B1: the step's list is complete; warps 1.. work off step s-1's rest meanwhile
+        const RestWork& rw_prev = s_rw[(s + 1) & 1ull];  // step s-1
         if (threadIdx.x == 0) {
             s_bar_target += G;
             arrive_barrier(ctl);
         }
         if (wib == 0) {
-            if (lane == 0) poll_barrier(ctl, s_bar_target, bcfg, &s_flag, &s_ok);
+            if (lane == 0) {
+                poll_barrier(ctl, s_bar_target, bcfg, &s_flag, &s_ok);
+                // the list of step s is complete: its rest becomes the next deferred work
+                const uint32_t Q = __ldcg(&ctl->qtail[s & 3ull]);
+                s_rw[s & 1ull] = RestWork{s, Q * eng.split_rest, qb};
+                s_q = Q;
+            }
             __syncwarp();
         } else {
-            while (rit < s_rw.n) {
+            while (rit < rw_prev.n) {
                 if (*(volatile int*)&s_flag) break;
-                rest_item(eng, s_rw, rit, &s_net0, lane, ev, bt);
+                rest_item(eng, rw_prev, rit, &s_net0, lane, ev, bt);
                 rit += WR;
             }
         }
@@ -1316,7 +1371,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         if (!s_ok) break;
         const unsigned long long tb = timer ? globaltimer_ns() : 0ull;
         // ---- 3. first parts of step s, then the rest of step s-1 that is left
-        const uint32_t Q = __ldcg(&ctl->qtail[s & 3ull]);
+        const uint32_t Q = s_q;
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->qtail[(s + 2) & 3ull] = 0u;  // reused by step s+2
         {
             const uint32_t split = eng.split_first, psz = eng.scatter_piece;
@@ -1325,6 +1380,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
                 const uint32_t e = (uint32_t)(it / split);
                 const uint32_t piece = (uint32_t)(it - (uint64_t)e * split);
                 const int4 rv = __ldcg(reinterpret_cast<const int4*>(queue + e));
+                const uint4 row = __ldcg(eng.qrow[qb] + e);  // with the record: no dependent row lookup
                 SpikeRec r;
                 r.net = (uint32_t)rv.x;
                 r.src = (uint32_t)rv.y;
@@ -1334,15 +1390,15 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
                     __stcg(eng.raster + rbase + e, make_uint2((uint32_t)s, __ldcg(qid + e)));
                 const NetDev* np = (r.net == 0) ? &s_net0 : eng.nets + r.net;
                 if (!NAER_IN_BOUNDS(eng.ctl, r.src, np->n_storage, kChkQueue)) continue;
-                const ulonglong2 rb = row_bounds(np->row_ptr, r.src);
+                const uint64_t beg = ((uint64_t)row.y << 32) | row.x;
                 const bool plastic_src = np->stdp_on && r.src < np->n_plastic;
-                const uint64_t hi = plastic_src ? rb.y : rb.x + __ldg(np->row_mid + r.src);
-                deliver_span(np, (uint32_t)(s - np->start_step), r, rb.x, hi, piece, split, psz, lane, ev, ovf,
+                const uint64_t hi = beg + (plastic_src ? row.w : row.z);
+                deliver_span(np, (uint32_t)(s - np->start_step), r, beg, hi, piece, split, psz, lane, ev, ovf,
                              eng.ctl, bt);
             }
         }
         if (wib != 0) {
-            for (; rit < s_rw.n; rit += WR) rest_item(eng, s_rw, rit, &s_net0, lane, ev, bt);
+            for (; rit < rw_prev.n; rit += WR) rest_item(eng, rw_prev, rit, &s_net0, lane, ev, bt);
         }
         {
             const unsigned long long cap = eng.record ? eng.raster_cap : 0ull;
@@ -1350,32 +1406,46 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
             if (eng.record && threadIdx.x == 0) s_dropped += Q - kept;
             rbase += kept;
         }
-        flush_bins(bt);  // everything binned since the last barrier, before this block's arrival
-        __syncthreads();
-        const unsigned long long tb2 = timer ? globaltimer_ns() : 0ull;
-        // ---- 4. B2: warps 1.. deliver step s's rest while warp 0 waits for it
-        if (threadIdx.x == 0) {
-            s_flag = 0;
-            s_bar_target += G;
-            arrive_barrier(ctl);
-            s_rw.step = s;
-            s_rw.qb = qb;
-            s_rw.n = Q * eng.split_rest;
-        }
-        rit = gr;
-        __syncthreads();
+        // ---- 4. B2.  A warp whose part of the above is done says so (its
+        // reductions ordered before the count) and, if it is not warp 0,
+        // starts on step s's rest at once; warp 0 waits for every warp's
+        // count, issues what the bins hold, arrives, and waits for the grid
+        // while the others keep working until the barrier completes.
+        __threadfence();  // every lane's reductions, before the warp's count
+        __syncwarp();
+        if (lane == 0) atomicAdd(&s_done, 1u);
+        unsigned long long tb2 = 0ull;
         if (wib == 0) {
-            if (lane == 0) poll_barrier(ctl, s_bar_target, bcfg, &s_flag, &s_ok);
+            if (lane == 0)
+                while (*(volatile uint32_t*)&s_done < nw_block) {
+                }
+            __syncwarp();
+            __threadfence_block();
+            flush_bins_warp(bt, lane);  // the block's binned deliveries since the last barrier
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) {
+                tb2 = timer ? globaltimer_ns() : 0ull;
+                s_bar_target += G;
+                arrive_barrier(ctl);
+                poll_barrier(ctl, s_bar_target, bcfg, &s_flag, &s_ok);
+            }
             __syncwarp();
         } else {
-            while (rit < s_rw.n) {
+            const RestWork& rw_cur = s_rw[s & 1ull];
+            rit = gr;
+            while (rit < rw_cur.n) {
                 if (*(volatile int*)&s_flag) break;
-                rest_item(eng, s_rw, rit, &s_net0, lane, ev, bt);
+                rest_item(eng, rw_cur, rit, &s_net0, lane, ev, bt);
                 rit += WR;
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) s_flag = 0;
+        flush_bins(bt);  // empties the table (keys included) while the block is synchronised
+        if (threadIdx.x == 0) {
+            s_flag = 0;
+            s_done = 0;
+        }
         if (!s_ok) break;
         if (timer) {
             const unsigned long long tc = globaltimer_ns();
@@ -1386,8 +1456,10 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         }
     }
     // the last step's rest (the next launch's LIF reads it in stream order)
-    if (s_ok && wib != 0)
-        for (; rit < s_rw.n; rit += WR) rest_item(eng, s_rw, rit, &s_net0, lane, ev, bt);
+    if (s_ok && wib != 0 && k > 0) {
+        const RestWork& rw_last = s_rw[(s0 + k - 1) & 1ull];
+        for (; rit < rw_last.n; rit += WR) rest_item(eng, rw_last, rit, &s_net0, lane, ev, bt);
+    }
     flush_bins(bt);
     if (kSmem) store_chunk_state(own, s_cc, sV, sR);
     finish_counters(eng, ev, ovf, lane, &s_ev, &s_ovf);
@@ -1478,7 +1550,9 @@ __device__ __forceinline__ void det_item(const EngineDev& eng, const SpikeRec* _
     const NetDev* np = r.net == 0 ? net0 : eng.nets + r.net;
     const uint32_t tl = (uint32_t)(s - np->start_step);
     const uint32_t D = np->ring_slots, tmod = tl % D, Ns = np->n_storage;
-    const ulonglong2 rb = row_bounds(np->row_ptr, r.src);
+    const uint4 row = __ldcg(eng.qrow[(uint32_t)(queue == eng.queue[1])] + e);
+    const uint64_t row_beg = ((uint64_t)row.y << 32) | row.x;
+    const ulonglong2 rb = make_ulonglong2(row_beg, row_beg + row.w);
     const uint32_t* __restrict__ tgt_a = np->tgt;
     const uint8_t* __restrict__ d_a = np->dly;
     float* __restrict__ w_a = np->w;
