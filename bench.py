@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--step-kernel", default="split", choices=["split", "two_barrier"],
                     help="persistent step kernel of the plain runs")
     ap.add_argument("--no-det", action="store_true", help="skip the deterministic-mode measurements")
+    ap.add_argument("--no-bins", action="store_true", help="skip the binned-aggregation comparison")
+    ap.add_argument("--bins-steps", type=int, default=2000, help="timed grid steps per binning trial")
     ap.add_argument("--no-saturated", action="store_true", help="skip the served form's saturation run")
     return ap.parse_args()
 
@@ -392,6 +394,41 @@ def bench_served(args, local, deterministic=False, saturate=False):
     }
 
 
+def bench_bins(args, local, stream_of):
+    """Shared-memory binning of the ring reductions (tuning `bins`) against
+    direct L2 reductions, device time per grid step: on the roofline
+    workload (uniform random targets: nothing to fold) and on a convergent
+    one (every neuron also drives a 64-neuron readout: each step's readout
+    events hit 64 ring cells)."""
+    import torch
+    from naer_b200 import spec as S
+    out = {}
+    for name, spec in [("roofline workload", workload(args)),
+                       ("hub readout 200k + 64", S.hub_readout(n=200_000, k=100, readout=64))]:
+        spec.raster_capacity = 1 << 24
+        net = S.build(spec, device=local)
+        stream = stream_of(net)
+        row = {"synapses": int(net.getSynapses())}
+        for bins in (0, 2048):
+            net.set_tuning(bins=bins)
+            net.run(256)
+            net.finish()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            ev0 = net.stats()["events"]
+            e0.record(stream)
+            net.run(args.bins_steps)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            ev = net.stats()["events"] - ev0
+            row[f"bins_{bins}"] = {"us_per_step": 1e3 * ms / args.bins_steps, "events_per_s": ev / (ms / 1e3)}
+        row["speedup_binned"] = row["bins_0"]["us_per_step"] / row["bins_2048"]["us_per_step"]
+        net.close()
+        out[name] = row
+    return out
+
+
 def bench_deterministic(args, local, stream_of):
     """The roofline workload in deterministic aggregation (bit-reproducible
     rasters): events/s over the timed steps, CUDA events on its stream."""
@@ -570,6 +607,9 @@ def run_ours(args):
         if not args.no_det:
             forms["batched_deterministic"] = bench_batched(args, local, deterministic=True)
             forms["served_deterministic"] = bench_served(args, local, deterministic=True, saturate=True)
+    if rank == 0 and world == 1 and not args.no_bins:
+        forms["binned_aggregation"] = bench_bins(
+            args, local, lambda n: torch.cuda.ExternalStream(n.stream(), device=torch.device("cuda", local)))
     if rank == 0 and world == 1 and not args.no_det:
         forms["deterministic"] = bench_deterministic(
             args, local, lambda n: torch.cuda.ExternalStream(n.stream(), device=torch.device("cuda", local)))

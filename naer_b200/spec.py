@@ -200,6 +200,21 @@ def scatter_outdegree(n: int = 1_000_000, k: int = 1000, seed: int = 1, drive_ra
     return _all_targets(s, E, I, k, seed)
 
 
+def hub_readout(n: int = 200_000, k: int = 100, readout: int = 64, seed: int = 1) -> NetSpec:
+    """A convergent network: N LIF (80/20) as in scatter_outdegree (fixed
+    out-degree k over all neurons, delays 1-16 steps, 20 Hz drive) plus a
+    readout population of `readout` LIF neurons that every neuron projects
+    to with delay 1 (weight 0.01 mV).  Each step's events to the readout
+    land on only `readout` ring cells: the case where shared-memory binning
+    of the ring reductions pays."""
+    s = scatter_outdegree(n=n, k=k, seed=seed)
+    s.name = f"hub_readout(N={n},K={k},readout={readout})"
+    R = s.add_pop(NOP, readout)
+    for src in (0, 1):
+        s.connect(src, R, capi.CONN_FIXED_OUTDEGREE, 0.01, degree=readout, dmin=1, dmax=1, seed=seed * 7919 + 31 + src)
+    return s
+
+
 def _all_targets(s: NetSpec, E: int, I: int, k: int, seed: int) -> NetSpec:
     # out-degree k over all neurons: split each source's k draws between the
     # E and I target populations in proportion to their sizes

@@ -146,3 +146,33 @@ def test_plastic_workload_fp64(O):
         x64 = np.asarray(x64, dtype=np.float64)
         err = np.abs(np.asarray(x32, dtype=np.float64) - x64) / np.maximum(np.abs(x64), floor)
         assert err.max() <= 1e-5, err.max()
+
+
+@pytest.mark.parametrize("bins", [64, 2048])
+def test_binned_aggregation_exact(O, bins):
+    """Shared-memory binning of the ring reductions: integer weights make
+    every fold order give the same sums, so runs with a small (overflowing)
+    and a large table match the oracle bit for bit, on a network whose
+    readout population concentrates each step's events on a few cells."""
+    s = integer_weight_net(n=20000, k=60, seed=6)
+    R = s.add_pop(S.NOP, 32, drive_rate_hz=0.0)
+    for src in (0, 1):
+        s.connect(src, R, capi.CONN_FIXED_OUTDEGREE, 1.0, degree=16, dmin=1, dmax=2, seed=70 + src)
+    o = O.OracleNet(s, deterministic=True)
+    o.run(700)
+    with S.build(s) as net:
+        net.set_tuning(bins=bins)
+        assert net.get_tuning()["bins"] == bins
+        net.run(300)
+        net.run(400)
+        net.finish()
+        assert assert_same_run(net, o) > 1000
+    o.close()
+
+
+def test_bins_validation(lib):
+    from naer_b200 import NaerError
+    with S.build(integer_weight_net(n=2000, k=50)) as net:
+        for bad in (3, 32, 100, 16384):
+            with pytest.raises(NaerError, match="bins"):
+                net.set_tuning(bins=bad)
