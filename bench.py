@@ -57,6 +57,7 @@ def parse():
                     help="persistent step kernel of the plain runs")
     ap.add_argument("--no-det", action="store_true", help="skip the deterministic-mode measurements")
     ap.add_argument("--no-bins", action="store_true", help="skip the binned-aggregation comparison")
+    ap.add_argument("--no-probe", action="store_true", help="skip the device probe (ceilings)")
     ap.add_argument("--bins-steps", type=int, default=2000, help="timed grid steps per binning trial")
     ap.add_argument("--no-saturated", action="store_true", help="skip the served form's saturation run")
     return ap.parse_args()
@@ -539,6 +540,8 @@ def run_ours(args):
     # stores, streaming read, one grid barrier
     probe = None
     try:
+        if args.no_probe:
+            raise RuntimeError("skipped (--no-probe)")
         from naer_b200 import _capi as capi
         st_ = net.stats()
         probe = capi.probe_device(local, ring_cells=st_["ring_slots"] * args.neurons,

@@ -125,7 +125,8 @@ typedef struct naer_stats {
     uint64_t events;            /* synaptic events delivered */
     uint64_t spikes;            /* spikes recorded in the raster */
     uint64_t raster_dropped;    /* spikes not recorded: raster full */
-    uint64_t stdp_hist_overflow;/* lazy-LTP lookups that hit the history limit */
+    uint64_t stdp_hist_overflow;/* lazy-LTP lookups that lost pairs: a post spike that had left the
+                                   post-spike history still fell after the source's last spike */
     uint64_t synapses;          /* synapses (unpadded) */
     uint64_t device_bytes;      /* device memory held by the handle */
     uint32_t neurons;

@@ -75,9 +75,10 @@ struct NetDev {
     // pair-based STDP state, one entry per plastic storage index
     // Packed post-synaptic row of each plastic neuron, post_stride int32
     // words (a multiple of 4, so one row is read with int4 loads): [0] step
-    // of the latest post spike (-1 = none), [1] post trace right after it
-    // (float bits), [2, 2 + hist_len) post spike steps, newest first (-1 =
-    // none).
+    // of the newest post spike that has left the history (-1 = none), [1]
+    // post trace right after the latest post spike (float bits), [2, 2 +
+    // hist_len) post spike steps, newest first (-1 = none); [2] is the
+    // latest post spike.
     int32_t* post;
     int2* pre;              // {step of the latest pre spike (-1 = none), pre trace after it (float bits)}
     const float* e_plus;    // [e_len] exp(-k dt / tau_plus) as float

@@ -129,7 +129,9 @@ __device__ __forceinline__ float stdp_update(const StdpView& n, float w, uint32_
             run = run && k < n.hist_len && r[2 + k] > pre_last;
             c += run ? 1u : 0u;
         }
-        if (c == n.hist_len) ++overflow;
+        // a pair is lost only if a post spike that left the history (the
+        // newest one that did is kept in word 0) still falls after pre_last
+        if (c == n.hist_len && r[0] > pre_last) ++overflow;
         float e[kMaxStdpHistory];
 #pragma unroll
         for (uint32_t k = 0; k < kMaxStdpHistory; ++k)
@@ -142,7 +144,7 @@ __device__ __forceinline__ float stdp_update(const StdpView& n, float w, uint32_
             }
         }
     }
-    const int32_t lp = r[0];
+    const int32_t lp = r[2];  // the newest history entry is the last post spike
     if (lp >= 0) {
         const float y = __fmul_rn(__int_as_float(r[1]), decay_lookup(n.e_minus, n.e_len, t - lp));
         w = fmaxf(__fsub_rn(w, __fmul_rn(n.a_minus, y)), 0.0f);
@@ -162,9 +164,13 @@ __device__ __forceinline__ void stdp_post_spike(const NetDev* np, uint32_t i, in
     int32_t r[kPostWordsMax];
     load_post_row(row, stride, r);
     const int2 pq = __ldcg(pre);
-    const int32_t lp = r[0];
+    const int32_t lp = r[2];
     const float y = lp >= 0 ? __fmul_rn(__int_as_float(r[1]), decay_lookup(e_minus, e_len, t - lp)) : 0.0f;
-    r[0] = t;
+    int32_t evicted = r[0];
+#pragma unroll
+    for (uint32_t q = 0; q < kMaxStdpHistory; ++q)
+        if (q + 1 == hist_len && r[2 + q] >= 0) evicted = r[2 + q];  // the entry shifted out below
+    r[0] = evicted;
     r[1] = __float_as_int(__fadd_rn(y, 1.0f));
 #pragma unroll
     for (int q = (int)kMaxStdpHistory - 1; q > 0; --q)

@@ -207,6 +207,7 @@ struct Net {
     std::vector<uint32_t> refr;
     std::vector<float> ring;          // [D][n]
     std::vector<int32_t> last_post, last_pre, hist;
+    std::vector<int32_t> evicted;  // newest post spike that has left the history (-1 = none)
     std::vector<float> y_post, x_pre, e_plus, e_minus;
     uint32_t e_len = 0;
     bool plastic_on = false;
@@ -414,6 +415,7 @@ void init_state(Net& net) {
     net.plastic_on = P.stdp_enabled && n_stdp > 0;
     if (net.plastic_on) {
         net.last_post.assign(net.n, -1);
+        net.evicted.assign(net.n, -1);
         net.last_pre.assign(net.n, -1);
         net.y_post.assign(net.n, 0.0f);
         net.x_pre.assign(net.n, 0.0f);
@@ -452,7 +454,8 @@ float stdp(Net& net, float wv, uint32_t tgt, int32_t t, int32_t pre_last, float 
         const int32_t* h = &net.hist[(size_t)tgt * P.stdp_history];
         uint32_t c = 0;
         while (c < P.stdp_history && h[c] > pre_last) ++c;
-        if (c == P.stdp_history) ++ovf;
+        // lost pairs: a post spike that left the history still falls after pre_last
+        if (c == P.stdp_history && net.evicted[tgt] > pre_last) ++ovf;
         for (int k = (int)c - 1; k >= 0; --k) {
             const float x = pre_x * decay(net.e_plus, h[k] - pre_last);
             const float inc = ap * x;
@@ -538,6 +541,7 @@ void grid_step(Net& net) {
                     net.y_post[i] = y + 1.0f;
                     net.last_post[i] = ts;
                     int32_t* h = &net.hist[(size_t)i * P.stdp_history];
+                    if (h[P.stdp_history - 1] >= 0) net.evicted[i] = h[P.stdp_history - 1];
                     for (int k = (int)P.stdp_history - 1; k > 0; --k) h[k] = h[k - 1];
                     h[0] = ts;
                     sp.pre_last = net.last_pre[i];
