@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-det", action="store_true", help="skip the deterministic-mode measurements")
     ap.add_argument("--no-bins", action="store_true", help="skip the binned-aggregation comparison")
     ap.add_argument("--no-probe", action="store_true", help="skip the device probe (ceilings)")
+    ap.add_argument("--tuning", default="", help='launch geometry of the plain runs as JSON, e.g. {"blocks_per_sm": 1}')
     ap.add_argument("--bins-steps", type=int, default=2000, help="timed grid steps per binning trial")
     ap.add_argument("--no-saturated", action="store_true", help="skip the served form's saturation run")
     return ap.parse_args()
@@ -82,6 +83,7 @@ def workload_config(args, synapses):
         "aggregation": "atomic",
         "l2": "inputs larger than L2 (9 B x synapses streamed; 126 MB L2)",
         "parallelism": "replicas",
+        "tuning": args.tuning or "default",
     }
 
 
@@ -469,8 +471,9 @@ def run_ours(args):
     net = S.build(spec, device=local)
     from naer_b200 import _capi as capi_
     kern = capi_.KERNEL_SPLIT if args.step_kernel == "split" else capi_.KERNEL_TWO_BARRIER
-    if kern != capi_.KERNEL_SPLIT:
-        net.set_tuning(step_kernel=kern)
+    extra_tuning = json.loads(args.tuning) if args.tuning else {}
+    if kern != capi_.KERNEL_SPLIT or extra_tuning:
+        net.set_tuning(step_kernel=kern, **extra_tuning)
     stream = torch.cuda.ExternalStream(net.stream(), device=torch.device("cuda", local))
     chunk = args.chunk
 

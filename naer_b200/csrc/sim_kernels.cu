@@ -811,20 +811,6 @@ __device__ __forceinline__ void ring_add(const BinTable& bt, float* addr, float 
     red_add_f32(addr, w);
 }
 
-// One warp, while the block's other warps may still add to the table:
-// issues every entry's sum taken by atomic exchange (an add racing with it
-// lands before, in this flush, or after, in the next); keys stay.
-__device__ __forceinline__ void flush_bins_warp(const BinTable& bt, uint32_t lane) {
-    if (!bt.mask) return;
-    for (uint32_t i = lane; i <= bt.mask; i += 32) {
-        const unsigned long long a = *(volatile unsigned long long*)(bt.key + i);
-        if (a) {
-            const float v = atomicExch(bt.sum + i, 0.0f);
-            if (v != 0.0f) red_add_f32(reinterpret_cast<float*>(a), v);
-        }
-    }
-}
-
 // Every thread of the block: issues the table's sums and empties it.
 __device__ __forceinline__ void flush_bins(const BinTable& bt) {
     if (!bt.mask) return;  // uniform over the block
@@ -1284,7 +1270,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
     __shared__ BarrierCfg bcfg;
     __shared__ int s_flag, s_ok;
     __shared__ RestWork s_rw[2];                     // deferred work of steps by parity
-    __shared__ uint32_t s_done, s_q;                 // warps done with a step's due work; its list size
+    __shared__ uint32_t s_q;                         // size of the step's list
     __shared__ unsigned long long s_ph[5], s_dropped;  // thread 0 only
     __shared__ unsigned long long s_bar_target;      // thread 0 only
     const uint32_t G = gridDim.x;
@@ -1304,7 +1290,6 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         s_flag = 0;
         s_rw[0] = RestWork{0, 0, 0};  // nothing deferred at launch start
         s_rw[1] = RestWork{0, 0, 0};
-        s_done = 0;
         s_q = 0;
         for (int q = 0; q < 5; ++q) s_ph[q] = 0;
         s_dropped = 0;
@@ -1406,34 +1391,25 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
             if (eng.record && threadIdx.x == 0) s_dropped += Q - kept;
             rbase += kept;
         }
-        // ---- 4. B2.  A warp whose part of the above is done says so (its
-        // reductions ordered before the count) and, if it is not warp 0,
-        // starts on step s's rest at once; warp 0 waits for every warp's
-        // count, issues what the bins hold, arrives, and waits for the grid
-        // while the others keep working until the barrier completes.
-        __threadfence();  // every lane's reductions, before the warp's count
-        __syncwarp();
-        if (lane == 0) atomicAdd(&s_done, 1u);
-        unsigned long long tb2 = 0ull;
+        flush_bins(bt);  // everything binned since the last barrier, before this block's arrival
+        __syncthreads();
+        const unsigned long long tb2 = timer ? globaltimer_ns() : 0ull;
+        // ---- 4. B2: warps 1.. deliver step s's rest while warp 0 waits for
+        // it.  (Starting that work as soon as a warp's due deliveries are
+        // done was measured slower: the bulk reductions then contend in L2
+        // with the delay-1 ones the barrier waits for.)
+        if (threadIdx.x == 0) {
+            s_flag = 0;
+            s_bar_target += G;
+            arrive_barrier(ctl);
+        }
+        rit = gr;
+        __syncthreads();
         if (wib == 0) {
-            if (lane == 0)
-                while (*(volatile uint32_t*)&s_done < nw_block) {
-                }
-            __syncwarp();
-            __threadfence_block();
-            flush_bins_warp(bt, lane);  // the block's binned deliveries since the last barrier
-            __threadfence();
-            __syncwarp();
-            if (lane == 0) {
-                tb2 = timer ? globaltimer_ns() : 0ull;
-                s_bar_target += G;
-                arrive_barrier(ctl);
-                poll_barrier(ctl, s_bar_target, bcfg, &s_flag, &s_ok);
-            }
+            if (lane == 0) poll_barrier(ctl, s_bar_target, bcfg, &s_flag, &s_ok);
             __syncwarp();
         } else {
             const RestWork& rw_cur = s_rw[s & 1ull];
-            rit = gr;
             while (rit < rw_cur.n) {
                 if (*(volatile int*)&s_flag) break;
                 rest_item(eng, rw_cur, rit, &s_net0, lane, ev, bt);
@@ -1441,11 +1417,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
             }
         }
         __syncthreads();
-        flush_bins(bt);  // empties the table (keys included) while the block is synchronised
-        if (threadIdx.x == 0) {
-            s_flag = 0;
-            s_done = 0;
-        }
+        if (threadIdx.x == 0) s_flag = 0;
         if (!s_ok) break;
         if (timer) {
             const unsigned long long tc = globaltimer_ns();
