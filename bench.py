@@ -530,7 +530,8 @@ def run_ours(args):
     ph = prof["phases_ms"]
     ph_tot = sum(ph.values()) or 1.0
     traffic = None
-    tfile = ROOT / "profiles" / "k_run_traffic.json"
+    kname = "k_step" if args.step_kernel == "split" else "k_run"
+    tfile = ROOT / "profiles" / f"{kname}_traffic.json"
     if tfile.exists():
         try:
             t = json.loads(tfile.read_text())
@@ -628,13 +629,12 @@ def run_ours(args):
             "config": workload_config(args, int(st1["synapses"])),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
-                         "kernel": ("k_step" if args.step_kernel == "split" else "k_run")
-                                   + " (persistent step kernel: LIF + scatter)",
+                         "kernel": kname + " (persistent step kernel: LIF + scatter)",
                          "peak_source": peak_src,
-                         "note": f"{BYTES_PER_EVENT} B x {pev} events over {launches} k_run launches "
+                         "note": f"{BYTES_PER_EVENT} B x {pev} events over {launches} {kname} launches "
                                  f"({args.profile_steps} grid steps), {prof['step_kernel_ms']:.2f} ms of the step kernel "
                                  f"(CUDA events); Poisson-draw kernel {prof['drive_kernel_ms']:.2f} ms; "
-                                 f"phase split of k_run (block 0): "
+                                 f"phase split of {kname} (block 0): "
                                  + ", ".join(f"{k} {v / ph_tot:.0%}" for k, v in ph.items())},
             "scatter_phase": scatter_phase,
             "device_probe": probe,

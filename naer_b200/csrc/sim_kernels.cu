@@ -1,13 +1,16 @@
-// Grid-mode simulation step: LIF update with fused Poisson input and
-// warp-ballot spike compaction, warp-per-spike CSR scatter into the delay
-// ring buffer with fused pair-based STDP, and the deterministic
-// (sorted segmented-reduce) aggregation kernels.
-//
-// No global atomic counter sits on the hot path: each LIF block compacts
-// its spikes into its own queue region (ballots plus a shared-memory
-// counter) and publishes one count; each scatter block prefix-sums the
-// counts in shared memory.  The only global atomics are the ring
-// reductions themselves.
+// Grid-mode simulation step: Poisson draws ahead of the simulation
+// (k_drive), and three persistent cooperative step kernels that run up to 64
+// grid steps per launch, each step = LIF with fused Poisson input and
+// warp-ballot spike compaction, then a warp-per-row CSR scatter into the
+// delay ring with fused pair-based STDP:
+//   k_step      atomic aggregation, one spike list per step, scatter split
+//               by deadline (default);
+//   k_run       atomic aggregation, per-block spike regions and two grid
+//               barriers per step (kept as a tuning choice);
+//   k_det_step  deterministic aggregation through per-cell event lists
+//               folded in canonical (source, synapse) order.
+// The ring reductions and one list reservation per warp and step are the
+// only global atomics on the hot path.
 #include "check.cuh"
 #include "grid_sync.cuh"
 #include "sim_kernels.cuh"
