@@ -452,11 +452,22 @@ def bench_deterministic(args, local, stream_of):
     e1.synchronize()
     st1 = net.stats()
     ms = e0.elapsed_time(e1)
+    # block 0's split of k_det_step (after the timed region): LIF + first
+    # barrier, linking pass + second barrier, folding pass + third barrier
+    net.set_profiling(True)
+    net.run(min(args.det_steps, 512))
+    net.finish()
+    prof = net.profile()
     net.close()
+    ph = prof["phases_ms"]
+    split = {"lif_barrier": ph["lif"], "link_barrier": ph["scatter"], "fold_barrier": ph["scatter_wait"]}
+    tot = sum(split.values()) or 1.0
     ev = st1["events"] - st0["events"]
     return {"workload": workload_config(args, int(st1["synapses"]))["workload"],
             "aggregation": "deterministic", "steps": args.det_steps, "ms": ms,
-            "events_per_s": ev / (ms / 1e3), "ms_per_simulated_s": ms * 1e4 / args.det_steps}
+            "events_per_s": ev / (ms / 1e3), "ms_per_simulated_s": ms * 1e4 / args.det_steps,
+            "kernel": "k_det_step", "step_kernel_ms": prof["step_kernel_ms"], "drive_kernel_ms": prof["drive_kernel_ms"],
+            "profiled_steps": prof["steps"], "phase_split": {k: round(v / tot, 3) for k, v in split.items()}}
 
 
 def run_ours(args):

@@ -1073,6 +1073,32 @@ __device__ __forceinline__ void rest_item(const EngineDev& eng, const RestWork& 
                         eng.scatter_piece, lane, ev, eng.ctl, bt);
 }
 
+// One first-part item of k_step (piece `piece` of spike e's due part: the
+// delay-1 synapses of a static source, the whole row of a plastic one);
+// the piece-0 warp appends the spike to the raster at rbase + e.
+__device__ __forceinline__ void first_item(const EngineDev& eng, const SpikeRec* __restrict__ queue,
+                                           const uint32_t* __restrict__ qid, uint32_t qb, uint32_t e,
+                                           uint32_t piece, uint32_t split, unsigned long long s,
+                                           unsigned long long rbase, const NetDev* net0, uint32_t lane,
+                                           unsigned long long& ev, uint32_t& ovf, const BinTable& bt) {
+    const int4 rv = __ldcg(reinterpret_cast<const int4*>(queue + e));
+    const uint4 row = __ldcg(eng.qrow[qb] + e);  // with the record: no dependent row lookup
+    SpikeRec r;
+    r.net = (uint32_t)rv.x;
+    r.src = (uint32_t)rv.y;
+    r.aux0 = rv.z;
+    r.aux1 = __int_as_float(rv.w);
+    if (piece == 0 && lane == 0 && eng.record && rbase + e < eng.raster_cap)
+        __stcg(eng.raster + rbase + e, make_uint2((uint32_t)s, __ldcg(qid + e)));
+    const NetDev* np = (r.net == 0) ? net0 : eng.nets + r.net;
+    if (!NAER_IN_BOUNDS(eng.ctl, r.src, np->n_storage, kChkQueue)) return;
+    const uint64_t beg = ((uint64_t)row.y << 32) | row.x;
+    const bool plastic_src = np->stdp_on && r.src < np->n_plastic;
+    const uint64_t hi = beg + (plastic_src ? row.w : row.z);
+    deliver_span(np, (uint32_t)(s - np->start_step), r, beg, hi, piece, split, eng.scatter_piece, lane, ev, ovf,
+                 eng.ctl, bt);
+}
+
 // Chunk descriptors, membrane potentials and refractory counters of the
 // block's owned chunks into shared memory (start of a persistent launch) and
 // back (end of it).
@@ -1362,27 +1388,12 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         const uint32_t Q = s_q;
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->qtail[(s + 2) & 3ull] = 0u;  // reused by step s+2
         {
-            const uint32_t split = eng.split_first, psz = eng.scatter_piece;
+            const uint32_t split = eng.split_first;
             const uint64_t n1 = (uint64_t)Q * split;
             for (uint64_t it = gw; it < n1; it += W) {
                 const uint32_t e = (uint32_t)(it / split);
-                const uint32_t piece = (uint32_t)(it - (uint64_t)e * split);
-                const int4 rv = __ldcg(reinterpret_cast<const int4*>(queue + e));
-                const uint4 row = __ldcg(eng.qrow[qb] + e);  // with the record: no dependent row lookup
-                SpikeRec r;
-                r.net = (uint32_t)rv.x;
-                r.src = (uint32_t)rv.y;
-                r.aux0 = rv.z;
-                r.aux1 = __int_as_float(rv.w);
-                if (piece == 0 && lane == 0 && eng.record && rbase + e < eng.raster_cap)
-                    __stcg(eng.raster + rbase + e, make_uint2((uint32_t)s, __ldcg(qid + e)));
-                const NetDev* np = (r.net == 0) ? &s_net0 : eng.nets + r.net;
-                if (!NAER_IN_BOUNDS(eng.ctl, r.src, np->n_storage, kChkQueue)) continue;
-                const uint64_t beg = ((uint64_t)row.y << 32) | row.x;
-                const bool plastic_src = np->stdp_on && r.src < np->n_plastic;
-                const uint64_t hi = beg + (plastic_src ? row.w : row.z);
-                deliver_span(np, (uint32_t)(s - np->start_step), r, beg, hi, piece, split, psz, lane, ev, ovf,
-                             eng.ctl, bt);
+                first_item(eng, queue, qid, qb, e, (uint32_t)(it - (uint64_t)e * split), split, s, rbase, &s_net0,
+                           lane, ev, ovf, bt);
             }
         }
         if (wib != 0) {
@@ -1510,6 +1521,94 @@ __device__ __forceinline__ float fold_cell(const float* __restrict__ ev_w, const
     return sum;
 }
 
+// Deterministic path over the pieces of a static source's row, kDetBatch
+// synapses per lane at a time (out of line, so that it has its own register
+// budget): every load of a batch is issued before any result is used, the
+// batch's list exchanges are issued back to back (their results are only
+// stored), and a list of one event (the usual case) is folded from the
+// weight loaded with its head, so a batch costs two or three dependent
+// round trips instead of that many per synapse.  Same results as the
+// per-synapse loop of det_item.
+constexpr uint32_t kDetBatch = 4;
+
+__device__ __noinline__ uint32_t det_static_span(const NetDev* np, uint64_t row_lo, uint64_t row_hi, uint32_t piece,
+                                                 uint32_t split, uint32_t psz, uint32_t tmod, float mult,
+                                                 uint32_t lane, int pass, Ctl* ctl) {
+    uint32_t ev = 0;  // events linked (pass 0)
+    const uint32_t* __restrict__ tgt_a = np->tgt;
+    const uint8_t* __restrict__ d_a = np->dly;
+    const float* __restrict__ w_a = np->w;
+    float* __restrict__ ev_w = np->ev_w;
+    uint32_t* __restrict__ ev_next = np->ev_next;
+    uint32_t* __restrict__ head = np->cell_head;
+    float* __restrict__ ring = np->ring;
+    const uint32_t D = np->ring_slots, Ns = np->n_storage;
+    constexpr uint32_t kSpan = 32 * kDetBatch;  // synapses of one batch of the warp
+    for (uint64_t base = row_lo + (uint64_t)piece * psz; base < row_hi; base += (uint64_t)split * psz) {
+        const uint64_t top = row_hi < base + psz ? row_hi : base + psz;
+        for (uint64_t b0 = base; b0 < top; b0 += kSpan) {
+            uint32_t cell[kDetBatch];
+            uint32_t aux[kDetBatch];  // pass 0: weight bits; pass 1: next event
+            uint8_t dl[kDetBatch];
+#pragma unroll
+            for (uint32_t u = 0; u < kDetBatch; ++u) {
+                const uint64_t j = b0 + lane + 32u * u;
+                cell[u] = kTgtSentinel;
+                if (j < top && NAER_IN_BOUNDS(ctl, j, np->syn_cap, kChkEventList)) {
+                    cell[u] = __ldcg(tgt_a + j);
+                    dl[u] = __ldcg(d_a + j);
+                    aux[u] = pass == 0 ? __float_as_uint(__ldcg(w_a + j)) : __ldcg(ev_next + j);
+                }
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < kDetBatch; ++u)
+                if (cell[u] != kTgtSentinel) {
+                    cell[u] = NAER_IN_BOUNDS(ctl, cell[u], Ns, kChkRing) ? ring_slot(tmod, dl[u], D) * Ns + cell[u]
+                                                                       : kTgtSentinel;
+                }
+            if (pass == 0) {
+                uint32_t old[kDetBatch];
+#pragma unroll
+                for (uint32_t u = 0; u < kDetBatch; ++u)
+                    if (cell[u] != kTgtSentinel) {
+                        const uint32_t j = (uint32_t)(b0 + lane + 32u * u);
+                        float w = __uint_as_float(aux[u]);
+                        if (mult != 1.0f) w = __fmul_rn(w, mult);
+                        __stcg(ev_w + j, w);
+                        old[u] = atomicExch(head + cell[u], j);
+                    }
+#pragma unroll
+                for (uint32_t u = 0; u < kDetBatch; ++u)
+                    if (cell[u] != kTgtSentinel) {
+                        __stcg(ev_next + (b0 + lane + 32u * u), old[u]);
+                        ++ev;
+                    }
+            } else {
+                // the event that started its cell's list (next == none) folds it
+                uint32_t hd[kDetBatch];
+                float wj[kDetBatch], rv[kDetBatch];
+#pragma unroll
+                for (uint32_t u = 0; u < kDetBatch; ++u)
+                    if (cell[u] != kTgtSentinel && aux[u] == kNoEvent) {
+                        hd[u] = __ldcg(head + cell[u]);
+                        wj[u] = __ldcg(ev_w + (b0 + lane + 32u * u));
+                        rv[u] = __ldcg(ring + cell[u]);
+                    }
+#pragma unroll
+                for (uint32_t u = 0; u < kDetBatch; ++u)
+                    if (cell[u] != kTgtSentinel && aux[u] == kNoEvent) {
+                        const uint32_t j = (uint32_t)(b0 + lane + 32u * u);
+                        // head == j: the list holds this event alone
+                        const float sum = hd[u] == j ? wj[u] : fold_cell(ev_w, ev_next, hd[u]);
+                        __stcg(ring + cell[u], __fadd_rn(rv[u], sum));
+                        __stcg(head + cell[u], kNoEvent);
+                    }
+            }
+        }
+    }
+    return ev;
+}
+
 // One (spike, piece) item of the deterministic path: pass 0 links events,
 // pass 1 folds the lists whose first event lies in the item.
 __device__ __forceinline__ void det_item(const EngineDev& eng, const SpikeRec* __restrict__ queue, uint32_t e,
@@ -1539,6 +1638,10 @@ __device__ __forceinline__ void det_item(const EngineDev& eng, const SpikeRec* _
     StdpView sv;
     if (pass == 0 && plastic_src) sv = stdp_view(*np);
     const float mult = (!plastic_src && r.aux0 > 1) ? (float)r.aux0 : 1.0f;
+    if (!plastic_src) {
+        ev += det_static_span(np, rb.x, rb.y, piece, split, psz, tmod, mult, lane, pass, eng.ctl);
+        return;
+    }
     for (uint64_t base = rb.x + (uint64_t)piece * psz; base < rb.y; base += (uint64_t)split * psz) {
         const uint64_t top = rb.y < base + psz ? rb.y : base + psz;
         for (uint64_t j = base + lane; j < top; j += 32) {
