@@ -1477,8 +1477,9 @@ template __global__ void k_step<false>(EngineDev, unsigned long long, uint32_t);
 //     atomicExch(cell_head[cell], j) (STDP updates first, as in the atomic
 //     path: they do not depend on the order);
 //  3. grid barrier; the event that started a list (ev_next == kNoEvent)
-//     walks it, orders its events by j and adds their left fold to the ring
-//     cell, then empties the head;
+//     takes the head and empties it in one exchange, walks the list, orders
+//     its events by j and adds their left fold to the ring cell (one
+//     reduction: no other event adds to that cell in this pass);
 //  4. grid barrier (the next LIF reads the ring).
 // The oracle folds each (step, cell) in the same order, so rings, membrane
 // potentials, weights and rasters are bit-identical; no sort, no host
@@ -1555,9 +1556,17 @@ __device__ __noinline__ uint32_t det_static_span(const NetDev* np, uint64_t row_
                 const uint64_t j = b0 + lane + 32u * u;
                 cell[u] = kTgtSentinel;
                 if (j < top && NAER_IN_BOUNDS(ctl, j, np->syn_cap, kChkEventList)) {
-                    cell[u] = __ldcg(tgt_a + j);
-                    dl[u] = __ldcg(d_a + j);
-                    aux[u] = pass == 0 ? __float_as_uint(__ldcg(w_a + j)) : __ldcg(ev_next + j);
+                    // the linking pass leaves the step's synapses in L2 for the
+                    // folding pass, which reads them for the last time
+                    if (pass == 0) {
+                        cell[u] = __ldcg(tgt_a + j);
+                        dl[u] = __ldcg(d_a + j);
+                        aux[u] = __float_as_uint(__ldcs(w_a + j));
+                    } else {
+                        cell[u] = __ldcs(tgt_a + j);
+                        dl[u] = __ldcs(d_a + j);
+                        aux[u] = __ldcs(ev_next + j);
+                    }
                 }
             }
 #pragma unroll
@@ -1584,15 +1593,18 @@ __device__ __noinline__ uint32_t det_static_span(const NetDev* np, uint64_t row_
                         ++ev;
                     }
             } else {
-                // the event that started its cell's list (next == none) folds it
+                // the event that started its cell's list (next == none) takes
+                // the head and empties it in one exchange, folds the list and
+                // adds the fold to the cell: the only addition to that cell in
+                // this pass, so a reduction gives the value a load, add and
+                // store would
                 uint32_t hd[kDetBatch];
-                float wj[kDetBatch], rv[kDetBatch];
+                float wj[kDetBatch];
 #pragma unroll
                 for (uint32_t u = 0; u < kDetBatch; ++u)
                     if (cell[u] != kTgtSentinel && aux[u] == kNoEvent) {
-                        hd[u] = __ldcg(head + cell[u]);
-                        wj[u] = __ldcg(ev_w + (b0 + lane + 32u * u));
-                        rv[u] = __ldcg(ring + cell[u]);
+                        hd[u] = atomicExch(head + cell[u], kNoEvent);
+                        wj[u] = __ldcs(ev_w + (b0 + lane + 32u * u));
                     }
 #pragma unroll
                 for (uint32_t u = 0; u < kDetBatch; ++u)
@@ -1600,8 +1612,7 @@ __device__ __noinline__ uint32_t det_static_span(const NetDev* np, uint64_t row_
                         const uint32_t j = (uint32_t)(b0 + lane + 32u * u);
                         // head == j: the list holds this event alone
                         const float sum = hd[u] == j ? wj[u] : fold_cell(ev_w, ev_next, hd[u]);
-                        __stcg(ring + cell[u], __fadd_rn(rv[u], sum));
-                        __stcg(head + cell[u], kNoEvent);
+                        red_add_f32(ring + cell[u], sum);
                     }
             }
         }
@@ -1660,10 +1671,8 @@ __device__ __forceinline__ void det_item(const EngineDev& eng, const SpikeRec* _
                 __stcg(ev_next + j, atomicExch(head + cell, (uint32_t)j));
                 ++ev;
             } else if (__ldcg(ev_next + j) == kNoEvent) {
-                float* ring = np->ring + cell;
-                const float sum = fold_cell(ev_w, ev_next, __ldcg(head + cell));
-                __stcg(ring, __fadd_rn(__ldcg(ring), sum));
-                __stcg(head + cell, kNoEvent);
+                // as in det_static_span: take and empty the head, add the fold
+                red_add_f32(np->ring + cell, fold_cell(ev_w, ev_next, atomicExch(head + cell, kNoEvent)));
             }
         }
     }
