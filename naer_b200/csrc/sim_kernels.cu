@@ -1522,6 +1522,42 @@ __device__ __forceinline__ float fold_cell(const float* __restrict__ ev_w, const
     return sum;
 }
 
+// Fold of the list whose first event is j (weight wj), started from the
+// head hd: every other event's next link and weight are loaded together, and
+// the walk stops at j (its link is known to be the end), so a list of two
+// costs one round trip.  Same order and result as fold_cell.
+__device__ __forceinline__ float fold_from_start(const float* __restrict__ ev_w,
+                                                 const uint32_t* __restrict__ ev_next, uint32_t hd, uint32_t j,
+                                                 float wj) {
+    uint32_t idx[kFoldRegs];
+    float wv[kFoldRegs];
+    uint32_t n = 0;
+    for (uint32_t h = hd; h != j;) {
+        if (n + 1 >= kFoldRegs || h == kNoEvent) return fold_cell(ev_w, ev_next, hd);  // long list
+        const uint32_t nx = __ldcg(ev_next + h);
+        wv[n] = __ldcg(ev_w + h);
+        idx[n++] = h;
+        h = nx;
+    }
+    idx[n] = j;
+    wv[n++] = wj;
+    for (uint32_t a = 1; a < n; ++a) {  // insertion sort by synapse index
+        const uint32_t x = idx[a];
+        const float y = wv[a];
+        uint32_t b = a;
+        while (b > 0 && idx[b - 1] > x) {
+            idx[b] = idx[b - 1];
+            wv[b] = wv[b - 1];
+            --b;
+        }
+        idx[b] = x;
+        wv[b] = y;
+    }
+    float sum = wv[0];
+    for (uint32_t a = 1; a < n; ++a) sum = __fadd_rn(sum, wv[a]);
+    return sum;
+}
+
 // Deterministic path over the pieces of a static source's row, kDetBatch
 // synapses per lane at a time (out of line, so that it has its own register
 // budget): every load of a batch is issued before any result is used, the
@@ -1611,7 +1647,7 @@ __device__ __noinline__ uint32_t det_static_span(const NetDev* np, uint64_t row_
                     if (cell[u] != kTgtSentinel && aux[u] == kNoEvent) {
                         const uint32_t j = (uint32_t)(b0 + lane + 32u * u);
                         // head == j: the list holds this event alone
-                        const float sum = hd[u] == j ? wj[u] : fold_cell(ev_w, ev_next, hd[u]);
+                        const float sum = hd[u] == j ? wj[u] : fold_from_start(ev_w, ev_next, hd[u], j, wj[u]);
                         red_add_f32(ring + cell[u], sum);
                     }
             }
