@@ -358,6 +358,7 @@ def bench_served(args, local, deterministic=False, saturate=False):
     import numpy as np
     from naer_b200 import spec as S
     from naer_b200.forms import Server
+    from naer_b200 import _capi as capi_
     jobs = S.served_jobs(count=args.served_jobs, seed=1)
     jobs = [(ta, spec.with_(deterministic=deterministic), steps) for ta, spec, steps in jobs]
     srv = Server(device=local, budget_bytes=150 * 10**9, chunk_steps=256, deterministic=deterministic)
@@ -371,6 +372,7 @@ def bench_served(args, local, deterministic=False, saturate=False):
     ok = srv.drain(1800.0)
     wall = time.perf_counter() - t0
     st = srv.stats()
+    errors = sorted({srv.error(j) for j in ids if srv.info(j)["state"] == capi_.JOB_FAILED})[:3]
     rng = np.random.default_rng(11)
     pick = rng.choice(len(jobs), min(args.plain_sample, len(jobs)), replace=False)
     identical = None
@@ -386,7 +388,7 @@ def bench_served(args, local, deterministic=False, saturate=False):
         "aggregation": "deterministic" if deterministic else "atomic",
         "sims_per_s": st["sims_per_s"],
         "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
-        "drained": ok, "wall_s": wall, "done": st["done"], "failed": st["failed"],
+        "drained": ok, "wall_s": wall, "done": st["done"], "failed": st["failed"], "failure_messages": errors,
         "peak_device_gb": st["peak_bytes"] / 1e9, "chunks": st["chunks"], "raster_dropped": st["raster_dropped"],
         "thread_s": {k: round(st[k], 2) for k in ("build_s", "install_s", "step_s", "drain_s")},
         "plain_sims_per_s": 1.0 / float(np.mean(all_s)),

@@ -291,7 +291,7 @@ uint32_t Engine::fast_chunk_capacity(uint32_t aggregation) {
     return 0;
 }
 
-uint64_t estimate_device_bytes(const NetHost& description) {
+uint64_t estimate_device_bytes(const NetHost& description, bool deterministic) {
     NetHost n;
     n.params = description.params;
     n.pops = description.pops;
@@ -315,7 +315,8 @@ uint64_t estimate_device_bytes(const NetHost& description) {
         rows += n.pops[c.src].size;
     }
     const uint64_t Ns = n.n_storage;
-    uint64_t b = (uint64_t)std::ceil(syn) * 9ull + (rows + Ns) * 6ull * 9ull;  // entries + padding
+    const uint64_t entries = (uint64_t)std::ceil(syn) + (rows + Ns) * 6ull;  // synapses + padding
+    uint64_t b = entries * 9ull;
     b += (Ns + 1) * 8ull + Ns * 4ull;                                          // row_ptr, row_mid
     b += Ns * (4ull + 1ull + kDriveSlots + 4ull * n.ring_slots);                // V, refr, drive, ring
     if (n.params.stdp_enabled && n.n_plastic) {
@@ -324,6 +325,9 @@ uint64_t estimate_device_bytes(const NetHost& description) {
         const double tmax = std::max(n.params.tau_plus_ms, n.params.tau_minus_ms) * 1000.0;
         b += 8ull * (uint64_t)std::min<double>(std::ceil(104.0 * tmax / n.params.dt_us) + 1.0, 1 << 24);
     }
+    // deterministic aggregation: event weight and link per padded synapse,
+    // list head per ring cell (allocated by the first deterministic step)
+    if (deterministic) b += entries * 8ull + (uint64_t)n.ring_slots * Ns * 4ull;
     return b;
 }
 
@@ -891,17 +895,17 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     if (tuning_.scatter_split) eng_.scatter_split = std::min<uint32_t>(tuning_.scatter_split, 64);
     // k_step: the part delivered before the next LIF (delay-1 synapses;
     // whole rows of plastic sources) and the deferred rest
-    uint64_t max_first = 0, max_rest = 0;
+    // (plastic rows go in pieces of kPlasticPiece: one synapse per lane)
+    uint64_t first_pieces = 1, max_rest = 0;
     for (NetHost* n : nets) {
-        if (n->dev.stdp_on) {
-            max_first = std::max<uint64_t>(max_first, n->max_row_padded);
-        } else {
-            max_first = std::max<uint64_t>(max_first, n->max_first_padded);
-            max_rest = std::max<uint64_t>(max_rest, n->max_rest_padded);
-        }
+        if (n->dev.stdp_on)
+            first_pieces = std::max<uint64_t>(first_pieces, (n->max_row_padded + kPlasticPiece - 1) / kPlasticPiece);
+        first_pieces = std::max<uint64_t>(first_pieces, (n->max_first_padded + psz - 1) / psz);
+        // (a plastic net's static sources defer their rows' rest too)
+        max_rest = std::max<uint64_t>(max_rest, n->max_rest_padded);
     }
     const uint64_t cap_split = any_stdp ? 32 : 16;
-    eng_.split_first = (uint32_t)std::min<uint64_t>(cap_split, std::max<uint64_t>(1, (max_first + psz - 1) / psz));
+    eng_.split_first = (uint32_t)std::min<uint64_t>(cap_split, first_pieces);
     eng_.split_rest = (uint32_t)std::min<uint64_t>(cap_split, std::max<uint64_t>(1, (max_rest + psz - 1) / psz));
     if (tuning_.scatter_split) eng_.split_first = eng_.split_rest = std::min<uint32_t>(tuning_.scatter_split, 64);
     eng_.queue_cap = (uint32_t)qentries;

@@ -90,7 +90,7 @@ struct NetHost {
 // Device bytes a network will hold once built (synapse arrays, state, ring,
 // drive slots, plasticity state), from its description alone.  Also
 // validates the description (the checks compile makes).
-uint64_t estimate_device_bytes(const NetHost& description);
+uint64_t estimate_device_bytes(const NetHost& description, bool deterministic = false);
 
 // LIF work items (chunks of up to 1,024 neurons of one population) a
 // network adds to an engine, from its description alone.

@@ -26,6 +26,7 @@ constexpr uint32_t kLifChunk = kLifThreads * kLifPerThread;  // neurons per LIF 
 constexpr uint32_t kScatterThreads = 256;
 constexpr uint32_t kScatterUnroll = 2;  // 128-synapse slices in flight per warp
 constexpr uint32_t kScatterPiece = 128 * kScatterUnroll;  // synapses per warp iteration
+constexpr uint32_t kPlasticPiece = 32;  // k_step: synapses per warp iteration of a plastic source's row
 // Steps of Poisson counts drawn ahead (ring of slots); small enough that the
 // counts and the delay ring stay resident in L2 together.
 #ifndef NAER_DRIVE_SLOTS

@@ -128,7 +128,7 @@ uint64_t Server::submit(const NetHost& description, uint64_t duration_steps) {
     if (duration_steps == 0) throw Error(NAER_E_INVALID, "duration must be at least one step");
     auto j = std::make_unique<Job>();
     j->net = clone_description(description);
-    j->est_bytes = estimate_device_bytes(*j->net);
+    j->est_bytes = estimate_device_bytes(*j->net, prm_.aggregation == NAER_AGG_DETERMINISTIC);
     j->chunks = lif_chunks(*j->net);
     if (j->est_bytes > prm_.budget_bytes)
         throw Error(NAER_E_OVERFLOW, "job needs about " + std::to_string(j->est_bytes) +

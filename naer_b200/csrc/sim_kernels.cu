@@ -845,9 +845,28 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
     const uint8_t* __restrict__ d_a = np->dly;
     const uint32_t n_plastic = np->n_plastic;
     const bool plastic_src = np->stdp_on && r.src < n_plastic;
-    StdpView sv;
-    if (plastic_src) sv = stdp_view(*np);
-    const float mult = (!plastic_src && r.aux0 > 1) ? (float)r.aux0 : 1.0f;
+    if (plastic_src) {
+        // one synapse per lane: each weight update waits on its target's
+        // post row, so a lane takes one of them per piece of kPlasticPiece
+        const StdpView sv = stdp_view(*np);
+        for (uint64_t base = lo + (uint64_t)piece * kPlasticPiece; base < hi;
+             base += (uint64_t)split * kPlasticPiece) {
+            const uint64_t j = base + lane;
+            if (j >= hi || !NAER_IN_BOUNDS(ctl, j, np->syn_cap, kChkSynapse)) continue;
+            const uint32_t tgt = __ldcs(tgt_a + j);
+            if (tgt == kTgtSentinel || !NAER_IN_BOUNDS(ctl, tgt, Ns, kChkRing)) continue;
+            float w = __ldcg(w_a + j);
+            const uint32_t d = __ldcs(d_a + j);
+            if (tgt < n_plastic) {
+                w = stdp_update(sv, w, tgt, (int32_t)tl, r.aux0, r.aux1, ovf);
+                __stcg(w_a + j, w);
+            }
+            ring_add(bt, ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w);
+            ++ev;
+        }
+        return;
+    }
+    const float mult = r.aux0 > 1 ? (float)r.aux0 : 1.0f;
     for (uint64_t base = lo + (uint64_t)piece * psz; base < hi; base += (uint64_t)split * psz) {
         uint4 tg[kScatterUnroll];
         float4 ww[kScatterUnroll];
@@ -857,7 +876,7 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
             const uint64_t off = base + (uint64_t)(u * 32 + lane) * 4ull;
             if (off < hi && (uint32_t)u * 128u < psz && NAER_IN_BOUNDS(ctl, off + 3, np->syn_cap, kChkSynapse)) {
                 tg[u] = ld_stream_u4(tgt_a + off);
-                ww[u] = __ldcg(reinterpret_cast<const float4*>(w_a + off));  // STDP may rewrite
+                ww[u] = __ldcg(reinterpret_cast<const float4*>(w_a + off));
                 dd[u] = ld_stream_u32(d_a + off);
             } else {
                 tg[u] = make_uint4(kTgtSentinel, kTgtSentinel, kTgtSentinel, kTgtSentinel);
@@ -867,17 +886,12 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
         }
 #pragma unroll
         for (int u = 0; u < (int)kScatterUnroll; ++u) {
-            const uint64_t off = base + (uint64_t)(u * 32 + lane) * 4ull;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const uint32_t tgt = u4_get(tg[u], j);
                 if (tgt == kTgtSentinel || !NAER_IN_BOUNDS(ctl, tgt, Ns, kChkRing)) continue;
                 float w = f4_get(ww[u], j);
                 const uint32_t d = (dd[u] >> (8 * j)) & 0xFFu;
-                if (plastic_src && tgt < n_plastic) {
-                    w = stdp_update(sv, w, tgt, (int32_t)tl, r.aux0, r.aux1, ovf);
-                    __stcg(w_a + off + j, w);
-                }
                 if (mult != 1.0f) w = __fmul_rn(w, mult);
                 ring_add(bt, ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w);
                 ++ev;
