@@ -125,7 +125,9 @@ def test_server_preempt_resume_and_cancel(lib):
 def test_server_cancel_queued_job(lib):
     """A job still waiting for memory is cancelled before it is built."""
     big = S.plastic_indegree(n=20000, k=300, seed=41).with_(deterministic=True)
-    with Server(budget_bytes=90 * 10**6, chunk_steps=64, deterministic=True) as srv:
+    # the footprint estimate of one job is about 114 MB (with the deterministic
+    # aggregation's event lists): the budget holds one
+    with Server(budget_bytes=150 * 10**6, chunk_steps=64, deterministic=True) as srv:
         a = srv.submit(big, 2000)
         b = srv.submit(big.with_(name="second"), 2000)  # waits: the budget holds one
         wait_running(srv, a, 1)

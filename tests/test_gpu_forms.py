@@ -105,9 +105,10 @@ def test_server_deterministic_jobs_match_alone(lib):
     job's raster equals its raster alone."""
     jobs = [(m, d) for m, d in zip(small_members(count=6, seed=7), [150, 700, 333, 64, 500, 260])]
     # an upper bound of the library's footprint estimate of each job (9 B per
-    # synapse, per-neuron arrays, decay tables); 1.5x the largest lets one or
-    # two jobs run at a time
-    est = max(9 * m.neurons * sum(c.degree for c in m.conns) // 2 + 330 * m.neurons + 170_000 for m, _ in jobs)
+    # synapse, 8 more for the deterministic aggregation's event lists,
+    # per-neuron arrays with the list heads, decay tables); 1.5x the largest
+    # lets one or two jobs run at a time
+    est = max(17 * m.neurons * sum(c.degree for c in m.conns) // 2 + 480 * m.neurons + 170_000 for m, _ in jobs)
     with Server(budget_bytes=int(1.5 * est), chunk_steps=64, deterministic=True) as srv:
         ids = []
         for m, d in jobs:
