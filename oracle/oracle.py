@@ -114,6 +114,11 @@ def uniform_rand(gid: int, seed: int, iteration: int) -> float:
     return load().oracle_uniform_rand(gid, seed, iteration)
 
 
+def exp_interval_us(gid: int, seed: int, iteration: int, rate: float) -> int:
+    """(uint)exprnd(rate) of random.cl:26-30 (saturated where x = 1)."""
+    return load().oracle_exp_interval_us(gid, seed, iteration, rate)
+
+
 def poisson_window(idx: int, n: int, seed: int, rate: float, t0: int, t1: int) -> np.ndarray:
     times = np.empty(10, dtype=np.uint32)
     c = load().oracle_poisson_window(idx, n, seed, rate, t0 & 0xFFFFFFFF, t1 & 0xFFFFFFFF, _ptr(times))
