@@ -4,13 +4,18 @@
 // the smoke check and the CPU baseline of the benchmark as the checker.  It
 // is never linked into, loaded by or called from the product library.
 //
-// Parity status: the reference cannot run in this environment (no OpenCL
-// runtime; several included .cl files and the Random123 submodule are not
-// in the reference tree), so this restatement is pinned only where a third
-// implementation exists: Philox4x32-10 is checked against cuRAND's
-// Philox4_32_10 (golden vectors under tests/golden).  The kernel semantics
-// below are otherwise restated from the reference source ("parity
-// unpinned" for those parts).
+// Parity status: the reference's whole path cannot run in this environment
+// (no OpenCL runtime; several included .cl files and the Random123
+// submodule are not in the reference tree).  Its complete kernels
+// random.cl, input_neuron_group.cl, lif.cl and network.cl are compiled as C
+// under a host work-group shim (oracle/ref/, built into oracle/_ref/), and
+// this restatement's Philox draws, Poisson windows, event-mode neuron
+// update and Bernoulli connectivity are checked against them bit for bit
+// (tests/test_ref_kernels.py, fixture tests/golden/ref_kernels.npz);
+// Philox4x32-10 is also checked against cuRAND's Philox4_32_10.  The
+// grid-mode semantics (fixed dt, per-synapse delays, ring aggregation, the
+// configurations' pair STDP) have no counterpart in those kernels and are
+// restated from the configurations ("parity unpinned" for those parts).
 //
 // Everything is written independently of the product sources: its own
 // Philox, its own layout (reference addresses, no padding), scalar loops.
