@@ -122,6 +122,24 @@ def test_roofline_workload_statistics(O):
         assert cv == pytest.approx(ocv, rel=0.02)
 
 
+def test_roofline_workload_deterministic_exact(O):
+    """The roofline workload itself (1M LIF, 1e9 synapses) in deterministic
+    aggregation: raster, membrane potentials, refractory counters and event
+    count equal the oracle's bit for bit over 300 grid steps (about 3e8
+    events, every per-cell fold in canonical order)."""
+    s = S.scatter_outdegree().with_(deterministic=True)
+    s.raster_capacity = 1 << 22
+    steps = 300
+    with S.build(s) as net:
+        net.run(steps)
+        net.finish()
+        o = O.OracleNet(s, deterministic=True)
+        o.run(steps)
+        n = assert_same_run(net, o)
+        o.close()
+    assert n > 10_000
+
+
 def test_plastic_workload_fp64(O):
     """100k LIF, fixed in-degree 1,000 (1e8 synapses), delays 1-20, pair
     STDP on E->E, 1,000 steps: membrane potentials and weights within 1e-5
