@@ -321,7 +321,7 @@ NAER_API int naer_net_check_report(naer_net* net, uint32_t* code, uint64_t* inde
 
 /* ---- device probe ------------------------------------------------------
  * No counterpart in the reference.  Measures, on `device`, the ceilings the
- * step kernel is judged against: random-address fp32 reductions
+ * step kernel is measured against: random-address fp32 reductions
  * (red.global.add.f32, the atomic mode's ring accumulation) into
  * ring_cells and small_cells cells, random 4-byte stores into ring_cells
  * cells, a streaming read of 4 GiB with evict-first 128-bit loads, and one

@@ -1,5 +1,5 @@
 """bench.py's output contract, on the CPU: the reference arm (the oracle
-port of the reference's step) prints one JSON line with the driver's keys."""
+port of the reference's step) prints one JSON line with the benchmark contract's keys."""
 import json
 import subprocess
 import sys
