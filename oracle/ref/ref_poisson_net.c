@@ -5,6 +5,7 @@
  * oracle's restatement is compared with.  Test infrastructure only. */
 #define _GNU_SOURCE
 #include <pthread.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -52,8 +53,12 @@ void clshim_run(size_t groups, size_t local_size, void (*item)(void*), void* arg
             ta[l].id.local_size = local_size;
             ta[l].item = item;
             ta[l].arg = arg;
-            if (local_size == 1) clshim_thread_main(&ta[l]);
-            else pthread_create(&th[l], NULL, clshim_thread_main, &ta[l]);
+            if (local_size == 1) {
+                clshim_thread_main(&ta[l]);
+            } else if (pthread_create(&th[l], NULL, clshim_thread_main, &ta[l]) != 0) {
+                fprintf(stderr, "clshim: cannot start work-item thread %zu of %zu\n", l, local_size);
+                abort();  /* the group's barrier could never complete */
+            }
         }
         if (local_size > 1)
             for (size_t l = 0; l < local_size; ++l) pthread_join(th[l], NULL);
