@@ -434,6 +434,44 @@ def bench_bins(args, local, stream_of):
     return out
 
 
+def bench_exact(args, local, stream_of):
+    """The roofline workload in exact-sum aggregation (fixed-point weights,
+    integer ring sums: bit-reproducible rasters from the atomic kernel):
+    events/s over the timed steps, CUDA events on its stream, and whether a
+    second run reproduces the first's raster."""
+    import numpy as np
+    import torch
+    from naer_b200 import spec as S
+    spec = workload(args).with_(exact=True)
+    spec.raster_capacity = 1 << 24
+    rasters = []
+    out = {}
+    for rep in range(2):
+        net = S.build(spec, device=local)
+        stream = stream_of(net)
+        net.run(256)
+        net.finish()
+        st0 = net.stats()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        net.run(args.det_steps)
+        e1.record(stream)
+        e1.synchronize()
+        st1 = net.stats()
+        ms = e0.elapsed_time(e1)
+        rasters.append(net.read_spikes())
+        net.close()
+        if rep == 0:
+            ev = st1["events"] - st0["events"]
+            out = {"workload": workload_config(args, int(st1["synapses"]))["workload"], "aggregation": "exact",
+                   "steps": args.det_steps, "ms": ms, "events_per_s": ev / (ms / 1e3),
+                   "ms_per_simulated_s": ms * 1e4 / args.det_steps}
+    out["second_run_identical"] = bool(np.array_equal(rasters[0][0], rasters[1][0])
+                                       and np.array_equal(rasters[0][1], rasters[1][1]))
+    return out
+
+
 def bench_deterministic(args, local, stream_of):
     """The roofline workload in deterministic aggregation (bit-reproducible
     rasters): events/s over the timed steps, CUDA events on its stream."""
@@ -632,6 +670,8 @@ def run_ours(args):
             args, local, lambda n: torch.cuda.ExternalStream(n.stream(), device=torch.device("cuda", local)))
     if rank == 0 and world == 1 and not args.no_det:
         forms["deterministic"] = bench_deterministic(
+            args, local, lambda n: torch.cuda.ExternalStream(n.stream(), device=torch.device("cuda", local)))
+        forms["exact"] = bench_exact(
             args, local, lambda n: torch.cuda.ExternalStream(n.stream(), device=torch.device("cuda", local)))
 
     if rank == 0:

@@ -65,6 +65,15 @@ extern "C" {
  * in ascending (source, synapse) order; bit-reproducible. */
 #define NAER_AGG_ATOMIC 0u
 #define NAER_AGG_DETERMINISTIC 1u
+/* Exact-sum aggregation (no counterpart in the reference): every delivered
+ * weight is rounded to the nearest multiple of 2^-S and the ring holds
+ * int32 sums, which no summation order changes, so runs are bit-identical
+ * at the atomic mode's speed.  S (at most 30) is chosen per network from
+ * its largest possible ring-cell sum (in-degree x max |w|, w_max for STDP,
+ * x 10 with POISSON sources); a network whose bound leaves no S >= 0 gets
+ * NAER_E_OVERFLOW at compile.  Inputs differ from the float sums by at most
+ * 2^-(S+1) per event. */
+#define NAER_AGG_EXACT 2u
 
 /* Connection rules.  REF_BERNOULLI is the reference's pairwise Philox test
  * (include/naer/kernels/network.cl:14-107); the fixed-degree rules draw

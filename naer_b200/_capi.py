@@ -35,7 +35,7 @@ STATUS_NAMES = {
 
 NEURON_STDP, NEURON_NOP, NEURON_POISSON = 0, 1, 2
 MODE_GRID, MODE_EVENT = 0, 1
-AGG_ATOMIC, AGG_DETERMINISTIC = 0, 1
+AGG_ATOMIC, AGG_DETERMINISTIC, AGG_EXACT = 0, 1, 2
 CONN_REF_BERNOULLI, CONN_FIXED_INDEGREE, CONN_FIXED_OUTDEGREE, CONN_EXPLICIT = 0, 1, 2, 3
 
 

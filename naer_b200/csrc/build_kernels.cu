@@ -305,4 +305,30 @@ __global__ void k_row_stats(const uint64_t* len, const uint64_t* padded, const u
     }
 }
 
+// Bounds of the exact-sum aggregation's fixed-point grid: in[t] += 1 for
+// every synapse into storage index t, out[0] = max |w| (as bits: the order
+// of non-negative floats), over the padded synapse array (padding skipped).
+__global__ void k_exact_inputs(const uint32_t* tgt, const float* w, uint64_t n, uint32_t* in,
+                               unsigned int* maxw_bits) {
+    unsigned int mx = 0;
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = tgt[j];
+        if (t == kTgtSentinel) continue;
+        atomicAdd(in + t, 1u);
+        mx = max(mx, __float_as_uint(fabsf(w[j])));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    if ((threadIdx.x & 31u) == 0 && mx) atomicMax(maxw_bits, mx);
+}
+
+// out = max of a[0..n)
+__global__ void k_max_u32(const uint32_t* a, uint32_t n, unsigned int* out) {
+    unsigned int mx = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) mx = max(mx, a[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    if ((threadIdx.x & 31u) == 0 && mx) atomicMax(out, mx);
+}
+
 }  // namespace naer

@@ -87,6 +87,9 @@ __global__ void k_pad_fill(const uint64_t* row_ptr, const uint64_t* len, uint32_
 __global__ void k_count_d1(const uint64_t* row_ptr, const uint64_t* len, uint32_t n, const uint8_t* dly,
                            uint32_t* n1);
 __global__ void k_row_pad_split(const uint64_t* len, const uint32_t* n1, uint32_t n, uint64_t* padded);
+__global__ void k_exact_inputs(const uint32_t* tgt, const float* w, uint64_t n, uint32_t* in,
+                               unsigned int* maxw_bits);
+__global__ void k_max_u32(const uint32_t* a, uint32_t n, unsigned int* out);
 __global__ void k_partition_d1(const uint64_t* row_ptr, const uint64_t* len, const uint32_t* n1, uint32_t n,
                                const uint64_t* row_ptr2, const uint32_t* tgt, const float* w, const uint8_t* dly,
                                uint32_t* tgt2, float* w2, uint8_t* dly2, uint32_t* row_mid);

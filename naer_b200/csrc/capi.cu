@@ -125,7 +125,7 @@ int naer_net_create(int device, const naer_net_params* params, naer_net** out) {
         naer_net_params p;
         if (params) p = *params; else naer_net_params_default(&p);
         need(p.mode == NAER_MODE_GRID || p.mode == NAER_MODE_EVENT, NAER_E_INVALID, "unknown mode");
-        need(p.aggregation <= NAER_AGG_DETERMINISTIC, NAER_E_INVALID, "unknown aggregation");
+        need(p.aggregation <= NAER_AGG_EXACT, NAER_E_INVALID, "unknown aggregation");
         need(p.dt_us > 0, NAER_E_INVALID, "dt_us must be positive");
         if (p.mode == NAER_MODE_EVENT)
             throw Error(NAER_E_UNSUPPORTED, "event mode is not available in this build");

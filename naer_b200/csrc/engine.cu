@@ -260,7 +260,8 @@ uint32_t Engine::fast_chunk_capacity(uint32_t aggregation) {
     int optin = 0;
     NAER_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
     const bool det = aggregation == NAER_AGG_DETERMINISTIC;
-    const bool split = det || tuning_.step_kernel == NAER_KERNEL_SPLIT;
+    // exact-sum aggregation runs the split kernel whatever the tuning says
+    const bool split = det || tuning_.step_kernel == NAER_KERNEL_SPLIT || aggregation == NAER_AGG_EXACT;
     const void* kern = det ? (const void*)k_det_step<true>
                            : split ? (const void*)k_step<true> : (const void*)k_run<true>;
     cudaFuncAttributes fa{};
@@ -383,6 +384,7 @@ void Engine::build(NetHost& n) {
 }
 
 void Engine::build_arrays(NetHost& n) {
+    n.fx_shift = kFxUnknown;  // new weights: the exact-sum grid is recomputed when installed
     layout(n);
     const uint32_t Ns = n.n_storage;
     const uint32_t T = 256;
@@ -699,6 +701,45 @@ void Engine::free_net(NetHost& n) {
 // ---------------------------------------------------------------------------
 // descriptor tables
 
+// Shift S of the exact-sum aggregation's grid 2^-S for a built network:
+// the largest S <= 30 for which no ring-cell sum can leave int32.  A cell
+// receives at most one event per synapse into its neuron before it is
+// read, of magnitude at most max|w| (at least w_max in a plastic network)
+// times 10 (the largest POISSON multiplicity), each rounded by at most half
+// a unit.  -1: no S >= 0 holds that bound.
+int32_t Engine::exact_shift(NetHost& n) {
+    DeviceGuard g(device_);
+    const uint64_t S = n.synapses_padded;
+    uint32_t* in = static_cast<uint32_t*>(dalloc((uint64_t)n.n_storage * 4ull + 16));
+    unsigned int* out = reinterpret_cast<unsigned int*>(in + n.n_storage);  // [0] max |w| bits, [1] max in-degree
+    try {
+        NAER_CK(cudaMemsetAsync(in, 0, (uint64_t)n.n_storage * 4ull + 16, stream_));
+        const uint32_t T = 256;
+        const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((S + T - 1) / T, (uint64_t)sm_count_ * 8));
+        if (S) k_exact_inputs<<<grid, T, 0, stream_>>>(n.tgt, n.w, S, in, out);
+        const uint32_t g2 = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n.n_storage + T - 1) / T, (uint64_t)sm_count_ * 4));
+        if (n.n_storage) k_max_u32<<<g2, T, 0, stream_>>>(in, n.n_storage, out + 1);
+        NAER_CK(cudaGetLastError());
+        unsigned int h[2] = {0, 0};
+        NAER_CK(cudaMemcpyAsync(h, out, 8, cudaMemcpyDeviceToHost, stream_));
+        NAER_CK(cudaStreamSynchronize(stream_));
+        dfree(in, (uint64_t)n.n_storage * 4ull + 16);
+        in = nullptr;
+        float maxw;
+        std::memcpy(&maxw, &h[0], 4);
+        if (n.params.stdp_enabled && n.n_plastic > 0) maxw = std::max(maxw, n.params.w_max);
+        bool poisson = false;
+        for (const PopSpec& ps : n.pops) poisson = poisson || (ps.type == kPOISSON && ps.size > 0);
+        const double bound = (double)h[1] * (double)maxw * (poisson ? 10.0 : 1.0);
+        for (int32_t sh = 30; sh >= 0; --sh)
+            if (bound * std::ldexp(1.0, sh) + (double)h[1] <= 2147483647.0) return sh;
+        return -1;
+    } catch (...) {
+        if (in) dfree(in, (uint64_t)n.n_storage * 4ull + 16);
+        throw;
+    }
+}
+
 void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity, bool record,
                      uint32_t aggregation) {
     DeviceGuard g(device_);
@@ -718,6 +759,15 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     for (uint32_t ni = 0; ni < nets.size(); ++ni) {
         NetHost& n = *nets[ni];
         NetDev d = n.dev;
+        d.fx_scale = d.fx_inv = 0.0f;
+        if (aggregation == NAER_AGG_EXACT) {
+            if (n.fx_shift == kFxUnknown) n.fx_shift = exact_shift(n);
+            if (n.fx_shift < 0)
+                throw Error(NAER_E_OVERFLOW, "weights too large for exact-sum aggregation: no fixed-point grid "
+                                             "holds the largest possible ring-cell sum in 32 bits");
+            d.fx_scale = std::ldexp(1.0f, n.fx_shift);
+            d.fx_inv = std::ldexp(1.0f, -n.fx_shift);
+        }
         d.ring_key_base = key_base;
         key_base += (uint64_t)n.ring_slots * n.n_storage;
         h_nets_.push_back(d);
@@ -785,13 +835,15 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     // memory, with as many blocks per SM as its footprint allows; the
     // deterministic path's LIF uses the same queue regions.
     const bool det = aggregation == NAER_AGG_DETERMINISTIC;
-    split_kernel_ = !det && tuning_.step_kernel == NAER_KERNEL_SPLIT;
+    const bool exact = aggregation == NAER_AGG_EXACT;
+    // exact-sum aggregation: the split kernel, integer reductions, no binning
+    split_kernel_ = !det && (tuning_.step_kernel == NAER_KERNEL_SPLIT || exact);
     const bool list_kernel = det || split_kernel_;  // one contiguous spike list per step
     const void* kern_smem = det ? (const void*)k_det_step<true>
                                 : split_kernel_ ? (const void*)k_step<true> : (const void*)k_run<true>;
     const void* kern_glob = det ? (const void*)k_det_step<false>
                                 : split_kernel_ ? (const void*)k_step<false> : (const void*)k_run<false>;
-    const uint32_t bins = split_kernel_ ? tuning_.bins : 0u;
+    const uint32_t bins = split_kernel_ && !exact ? tuning_.bins : 0u;
     auto smem_of = [&](uint32_t grid, uint32_t own, bool state) {
         return list_kernel ? step_smem_bytes(own, state, bins) : run_smem_bytes(grid, own, state);
     };
@@ -970,10 +1022,10 @@ TuneResult Engine::autotune(uint32_t trial_steps) {
                     if (bps == 0 && L == kDriveSlots && sp == 0) {
                         t.scatter_piece = eng_piece_default == 128 ? kScatterPiece : 128u;
                     }
-                    if (bps == 1 && L == kDriveSlots && sp == 0 && aggregation_ != NAER_AGG_DETERMINISTIC)
+                    if (bps == 1 && L == kDriveSlots && sp == 0 && aggregation_ == NAER_AGG_ATOMIC)
                         t.step_kernel = NAER_KERNEL_TWO_BARRIER;
                     // shared-memory binning of the ring reductions
-                    if (bps == 0 && L == kDriveSlots / 2 && sp == 0 && aggregation_ != NAER_AGG_DETERMINISTIC)
+                    if (bps == 0 && L == kDriveSlots / 2 && sp == 0 && aggregation_ == NAER_AGG_ATOMIC)
                         t.bins = 2048;
                     const double us = trial(t);
                     if (us < r.best_us_per_step) {

@@ -20,6 +20,8 @@ struct Error : std::runtime_error {
 void cuda_check(cudaError_t e, const char* what);
 #define NAER_CK(x) ::naer::cuda_check((x), #x)
 
+constexpr int32_t kFxUnknown = -2;  // NetHost::fx_shift not computed yet
+
 struct PopSpec {
     uint32_t type = kNOP;
     uint32_t size = 0;
@@ -51,6 +53,7 @@ struct NetHost {
     std::vector<PopSpec> pops;
     std::vector<ConnSpec> conns;
     bool compiled = false;
+    int32_t fx_shift = kFxUnknown;  // exact-sum grid shift S, computed when an exact-mode engine installs the net
 
     // layout
     std::vector<uint32_t> pop_order;   // pops in type order
@@ -141,6 +144,7 @@ public:
     void build(NetHost& net);
     void free_net(NetHost& net);
     // Installs the nets' descriptor tables; nets must outlive the engine use.
+    int32_t exact_shift(NetHost& n);
     void install(const std::vector<NetHost*>& nets, uint64_t raster_capacity, bool record,
                  uint32_t aggregation);
 

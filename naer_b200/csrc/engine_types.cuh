@@ -106,6 +106,10 @@ struct NetDev {
     float a_minus;          // A- * w_max
     float w_max;
     uint32_t active;        // 0 = slot idle (served form)
+    // exact-sum aggregation: weights delivered as integers on the grid 2^-S
+    // (fx_scale = 2^S, fx_inv = 2^-S); both 0 when the ring holds floats
+    float fx_scale;
+    float fx_inv;
     uint32_t pad_;
 };
 

@@ -46,7 +46,7 @@ Batch::Batch(int device, uint32_t aggregation, uint64_t raster_capacity, bool re
       aggregation_(aggregation),
       raster_capacity_(raster_capacity),
       record_(record) {
-    if (aggregation > NAER_AGG_DETERMINISTIC) throw Error(NAER_E_INVALID, "unknown aggregation");
+    if (aggregation > NAER_AGG_EXACT) throw Error(NAER_E_INVALID, "unknown aggregation");
 }
 
 uint32_t Batch::add(const NetHost& description) {
@@ -95,7 +95,7 @@ uint64_t Batch::read_spikes(uint64_t first, uint64_t cap, uint32_t* member, uint
 // Server
 
 Server::Server(int device, const ServerParams& p) : device_(device), prm_(p), t0_(std::chrono::steady_clock::now()) {
-    if (p.aggregation > NAER_AGG_DETERMINISTIC) throw Error(NAER_E_INVALID, "unknown aggregation");
+    if (p.aggregation > NAER_AGG_EXACT) throw Error(NAER_E_INVALID, "unknown aggregation");
     if (p.chunk_steps == 0) throw Error(NAER_E_INVALID, "chunk_steps must be positive");
     if (p.max_jobs == 0) throw Error(NAER_E_INVALID, "max_jobs must be positive");
     if (p.raster_capacity == 0) throw Error(NAER_E_INVALID, "raster_capacity must be positive");

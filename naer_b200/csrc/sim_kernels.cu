@@ -39,6 +39,17 @@ __device__ __forceinline__ void red_add_f32(float* addr, float v) {
     asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(addr), "f"(v) : "memory");
 }
 
+// Fire-and-forget integer reduction (exact-sum aggregation).
+__device__ __forceinline__ void red_add_s32(float* addr, int v) {
+    asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(addr), "r"(v) : "memory");
+}
+
+// Ring-cell input as the neuron reads it: the float sum, or with exact-sum
+// aggregation (fx_inv != 0) the cell's integer sum times 2^-S.
+__device__ __forceinline__ float ring_input(float cell, float fx_inv) {
+    return fx_inv != 0.0f ? __fmul_rn(__int2float_rn(__float_as_int(cell)), fx_inv) : cell;
+}
+
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
@@ -272,7 +283,7 @@ __device__ __forceinline__ void lif_chunk(const EngineDev& eng, uint32_t c, unsi
                 rr[j] -= 1;
                 continue;
             }
-            float v = lif_update(vv[j], p.prop, f4_get(I, j), drive[j], p.drive_w);
+            float v = lif_update(vv[j], p.prop, ring_input(f4_get(I, j), np->fx_inv), drive[j], p.drive_w);
             if (v > p.v_th) {
                 v = p.v_reset;
                 rr[j] = p.t_ref_steps;
@@ -462,6 +473,7 @@ struct ChunkCache {
     unsigned long long start, stop;
     uint32_t first, end, net, Ns;
     uint32_t slots, dt_us, active, plastic;
+    float fx_inv;  // exact-sum aggregation: 2^-S (0: the ring holds floats)
 };
 
 // LIF of one owned chunk with V, refractory counters and Poisson counts in
@@ -539,7 +551,7 @@ __device__ __forceinline__ void lif_chunk_smem(const EngineDev& eng, const Chunk
                 rr[k] -= 1;
                 continue;
             }
-            float v = lif_update(vv[k], prop, f4_get(I, k), dd[k], dw);
+            float v = lif_update(vv[k], prop, ring_input(f4_get(I, k), cc.fx_inv), dd[k], dw);
             if (v > v_th) {
                 v = v_reset;
                 rr[k] = cc.p.t_ref_steps;
@@ -647,6 +659,7 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
             c.dt_us = np->dt_us;
             c.active = np->active;
             c.plastic = (c.p.type == kSTDP && np->stdp_on) ? 1u : 0u;
+            c.fx_inv = np->fx_inv;
             s_cc[j] = c;
         }
         __syncthreads();
@@ -790,7 +803,13 @@ struct BinTable {
 
 constexpr int kBinProbes = 4;
 
-__device__ __forceinline__ void ring_add(const BinTable& bt, float* addr, float w) {
+// qs != 0: exact-sum aggregation, the weight rounded to the nearest
+// multiple of 1/qs = 2^-S and added as an integer (binning is off then).
+__device__ __forceinline__ void ring_add(const BinTable& bt, float* addr, float w, float qs) {
+    if (qs != 0.0f) {
+        red_add_s32(addr, __float2int_rn(__fmul_rn(w, qs)));
+        return;
+    }
     if (bt.mask) {
         const unsigned long long a = (unsigned long long)addr;
         uint32_t h = (uint32_t)(((a >> 2) * 0x9E3779B97F4A7C15ull) >> 40) & bt.mask;
@@ -840,6 +859,7 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
     const uint32_t tmod = tl % D;
     const uint32_t Ns = np->n_storage;
     float* __restrict__ ring = np->ring;
+    const float qs = np->fx_scale;  // exact-sum aggregation: 2^S, else 0
     const uint32_t* __restrict__ tgt_a = np->tgt;
     float* __restrict__ w_a = np->w;
     const uint8_t* __restrict__ d_a = np->dly;
@@ -861,7 +881,7 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
                 w = stdp_update(sv, w, tgt, (int32_t)tl, r.aux0, r.aux1, ovf);
                 __stcg(w_a + j, w);
             }
-            ring_add(bt, ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w);
+            ring_add(bt, ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w, qs);
             ++ev;
         }
         return;
@@ -893,7 +913,7 @@ __device__ __forceinline__ void deliver_span(const NetDev* np, uint32_t tl, cons
                 float w = f4_get(ww[u], j);
                 const uint32_t d = (dd[u] >> (8 * j)) & 0xFFu;
                 if (mult != 1.0f) w = __fmul_rn(w, mult);
-                ring_add(bt, ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w);
+                ring_add(bt, ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w, qs);
                 ++ev;
             }
         }
@@ -909,6 +929,7 @@ __device__ __forceinline__ void deliver_static_span(const NetDev* np, uint32_t t
     const uint32_t tmod = tl % D;
     const uint32_t Ns = np->n_storage;
     float* __restrict__ ring = np->ring;
+    const float qs = np->fx_scale;  // exact-sum aggregation: 2^S, else 0
     const uint32_t* __restrict__ tgt_a = np->tgt;
     const float* __restrict__ w_a = np->w;
     const uint8_t* __restrict__ d_a = np->dly;
@@ -938,7 +959,7 @@ __device__ __forceinline__ void deliver_static_span(const NetDev* np, uint32_t t
                 if (tgt == kTgtSentinel || !NAER_IN_BOUNDS(ctl, tgt, Ns, kChkRing)) continue;
                 float w = f4_get(ww[u], j);
                 if (mult != 1.0f) w = __fmul_rn(w, mult);
-                ring_add(bt, ring + (size_t)ring_slot(tmod, (dd[u] >> (8 * j)) & 0xFFu, D) * Ns + tgt, w);
+                ring_add(bt, ring + (size_t)ring_slot(tmod, (dd[u] >> (8 * j)) & 0xFFu, D) * Ns + tgt, w, qs);
                 ++ev;
             }
         }
@@ -969,7 +990,7 @@ __device__ __forceinline__ uint32_t lif_flags_smem(const ChunkCache& cc, uint32_
     float vv[4] = {V4.x, V4.y, V4.z, V4.w};
     uint32_t rr[4] = {R4.x, R4.y, R4.z, R4.w};
     const double prop = cc.p.prop;
-    const float v_th = cc.p.v_th, v_reset = cc.p.v_reset, dw = cc.p.drive_w;
+    const float v_th = cc.p.v_th, v_reset = cc.p.v_reset, dw = cc.p.drive_w, fx_inv = cc.fx_inv;
     const uint32_t tref = cc.p.t_ref_steps, end = cc.end;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -978,7 +999,7 @@ __device__ __forceinline__ uint32_t lif_flags_smem(const ChunkCache& cc, uint32_
             rr[k] -= 1;
             continue;
         }
-        float v = lif_update(vv[k], prop, f4_get(I, k), (Dw >> (8 * k)) & 0xFFu, dw);
+        float v = lif_update(vv[k], prop, ring_input(f4_get(I, k), fx_inv), (Dw >> (8 * k)) & 0xFFu, dw);
         if (v > v_th) {
             v = v_reset;
             rr[k] = tref;
@@ -1140,6 +1161,7 @@ __device__ __forceinline__ void load_chunk_state(const EngineDev& eng, uint32_t 
         c.dt_us = np->dt_us;
         c.active = np->active;
         c.plastic = (c.p.type == kSTDP && np->stdp_on) ? 1u : 0u;
+        c.fx_inv = np->fx_inv;
         s_cc[j] = c;
     }
     __syncthreads();
@@ -1277,7 +1299,8 @@ __device__ __forceinline__ void lif_phase(const EngineDev& eng, unsigned long lo
                             rr[q] -= 1;
                             continue;
                         }
-                        float v = lif_update(vv[q], p.prop, f4_get(Iv, q), (Dw >> (8 * q)) & 0xFFu, p.drive_w);
+                        float v = lif_update(vv[q], p.prop, ring_input(f4_get(Iv, q), np->fx_inv), (Dw >> (8 * q)) & 0xFFu,
+                                             p.drive_w);
                         if (v > p.v_th) {
                             v = p.v_reset;
                             rr[q] = p.t_ref_steps;

@@ -26,10 +26,11 @@ def _description(x):
 class Batch:
     """Many networks of any sizes advanced by one set of persistent launches."""
 
-    def __init__(self, members=(), device: int = 0, deterministic: bool = False, raster_capacity: int = 1 << 24):
+    def __init__(self, members=(), device: int = 0, deterministic: bool = False, raster_capacity: int = 1 << 24,
+                 exact: bool = False):
         capi.load()
         h = C.c_void_p()
-        agg = capi.AGG_DETERMINISTIC if deterministic else capi.AGG_ATOMIC
+        agg = capi.AGG_EXACT if exact else capi.AGG_DETERMINISTIC if deterministic else capi.AGG_ATOMIC
         capi.call("naer_batch_create", int(device), agg, int(raster_capacity), C.byref(h))
         self._h = h
         self.n = 0
@@ -136,13 +137,13 @@ class Server:
 
     def __init__(self, device: int = 0, budget_bytes: int = 150 * 10**9, chunk_steps: int = 256,
                  deterministic: bool = False, max_jobs: int = 1024, raster_capacity: int = 1 << 24,
-                 blocks_per_sm: int = 0, chunk_ms: float = 10.0, launch_steps: int = 0):
+                 blocks_per_sm: int = 0, chunk_ms: float = 10.0, launch_steps: int = 0, exact: bool = False):
         capi.load()
         p = capi.ServerParams()
         capi.call("naer_server_params_default", C.byref(p))
         p.budget_bytes = int(budget_bytes)
         p.chunk_steps = int(chunk_steps)
-        p.aggregation = capi.AGG_DETERMINISTIC if deterministic else capi.AGG_ATOMIC
+        p.aggregation = capi.AGG_EXACT if exact else capi.AGG_DETERMINISTIC if deterministic else capi.AGG_ATOMIC
         p.max_jobs = int(max_jobs)
         p.raster_capacity = int(raster_capacity)
         p.blocks_per_sm = int(blocks_per_sm)

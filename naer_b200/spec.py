@@ -53,6 +53,7 @@ class NetSpec:
     conns: list = field(default_factory=list)
     dt_us: int = 100
     deterministic: bool = False
+    exact: bool = False           # exact-sum aggregation (fixed-point weights; deterministic at atomic speed)
     record: bool = True
     raster_capacity: int = 1 << 24
     poisson_seed: int = 0x15AC7EBD
@@ -107,7 +108,8 @@ def describe(spec: NetSpec, device: int = -1) -> Network:
     net = Network(
         device=device,
         dt_us=spec.dt_us,
-        aggregation=capi.AGG_DETERMINISTIC if spec.deterministic else capi.AGG_ATOMIC,
+        aggregation=(capi.AGG_EXACT if spec.exact else
+                     capi.AGG_DETERMINISTIC if spec.deterministic else capi.AGG_ATOMIC),
         record_spikes=1 if spec.record else 0,
         raster_capacity=spec.raster_capacity,
         poisson_seed=spec.poisson_seed,

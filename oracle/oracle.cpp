@@ -171,7 +171,8 @@ struct OrConn {
 
 struct OrParams {
     uint32_t dt_us;
-    uint32_t deterministic;  // 1: per-(step, cell) left fold; 0: parallel atomic adds
+    uint32_t deterministic;  // 1: per-(step, cell) left fold; 0: parallel atomic adds;
+                             // 2: exact sums of fixed-point weights (see exact_shift)
     uint32_t poisson_seed;
     uint32_t stdp_enabled;
     float tau_plus_ms, tau_minus_ms, a_plus, a_minus, w_max;
@@ -211,6 +212,8 @@ struct Net {
     std::vector<float> v;
     std::vector<uint32_t> refr;
     std::vector<float> ring;          // [D][n]
+    std::vector<int32_t> ring_q;      // [D][n] exact mode: fixed-point sums, grid 2^-fx_shift
+    int32_t fx_shift = 0;
     std::vector<int32_t> last_post, last_pre, hist;
     std::vector<int32_t> evicted;  // newest post spike that has left the history (-1 = none)
     std::vector<float> y_post, x_pre, e_plus, e_minus;
@@ -406,6 +409,32 @@ void build_csr(Net& net) {
     }
 }
 
+// Exact-sum aggregation: every delivered weight (after STDP and the POISSON
+// multiplicity) becomes the integer nearest to w * 2^S and the ring holds
+// int32 sums, which no summation order changes; the neuron reads a cell as
+// float(sum) * 2^-S.  S is the largest shift (at most 30) for which no cell
+// sum can overflow: a cell receives at most one event per synapse into its
+// neuron before it is read, each of magnitude at most max|w| (w_max for a
+// plastic net) times 10 (the largest POISSON multiplicity), plus half a unit
+// of rounding.  Returns -1 when even S = 0 cannot hold that bound.
+int32_t exact_shift(const Net& net) {
+    std::vector<uint32_t> in(net.n, 0);
+    float maxw = 0.0f;
+    for (size_t j = 0; j < net.tgt.size(); ++j) {
+        ++in[net.tgt[j]];
+        maxw = std::max(maxw, std::fabs(net.w[j]));
+    }
+    uint32_t max_in = 0;
+    for (uint32_t c : in) max_in = std::max(max_in, c);
+    if (net.plastic_on) maxw = std::max(maxw, net.prm.w_max);
+    bool poisson = false;
+    for (const OrPop& p : net.pops) poisson = poisson || (p.type == 2 && p.size > 0);
+    const double bound = (double)max_in * (double)maxw * (poisson ? 10.0 : 1.0);
+    for (int32_t S = 30; S >= 0; --S)
+        if (bound * std::ldexp(1.0, S) + (double)max_in <= 2147483647.0) return S;
+    return -1;
+}
+
 void init_state(Net& net) {
     net.v.assign(net.n, 0.0f);
     net.refr.assign(net.n, 0);
@@ -413,6 +442,7 @@ void init_state(Net& net) {
         if (net.pops[p].type != 2)
             for (uint32_t k = 0; k < net.pops[p].size; ++k) net.v[net.base[p] + k] = net.pops[p].v_init;
     net.ring.assign((size_t)net.D * net.n, 0.0f);
+    if (net.prm.deterministic == 2) net.ring_q.assign((size_t)net.D * net.n, 0);
     const OrParams& P = net.prm;
     uint32_t n_stdp = 0;
     for (const auto& p : net.pops)
@@ -520,8 +550,15 @@ void grid_step(Net& net) {
                 if (m) out.push_back(Spike{i, (int32_t)m, 0.0f});
                 continue;
             }
-            const float I = ring_slot[i];
-            ring_slot[i] = 0.0f;
+            float I;
+            if (P.deterministic == 2) {
+                int32_t& q = net.ring_q[(size_t)slot * net.n + i];
+                I = (float)q * std::ldexp(1.0f, -net.fx_shift);
+                q = 0;
+            } else {
+                I = ring_slot[i];
+                ring_slot[i] = 0.0f;
+            }
             if (net.refr[i] > 0) {
                 net.refr[i] -= 1;
                 continue;
@@ -587,7 +624,29 @@ void grid_step(Net& net) {
         return (uint64_t)sl * net.n + net.tgt[j];
     };
 
-    if (P.deterministic) {
+    if (P.deterministic == 2) {
+        // exact sums: integer additions in any order
+        const float scale = std::ldexp(1.0f, net.fx_shift);
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : ev, ovf) num_threads(nthreads)
+        for (int64_t si = 0; si < (int64_t)spikes.size(); ++si) {
+            const Spike& sp = spikes[(size_t)si];
+            uint64_t local_ovf = 0;
+            for (uint64_t j = net.row_ptr[sp.src]; j < net.row_ptr[sp.src + 1]; ++j) {
+                float wv = net.w[j];
+                const uint32_t tg = net.tgt[j];
+                const bool src_plastic = net.plastic_on && net.kind[sp.src] == 0;
+                if (src_plastic && net.kind[tg] == 0) {
+                    wv = stdp(net, wv, tg, (int32_t)t, sp.pre_last, sp.pre_x, local_ovf);
+                    net.w[j] = wv;
+                }
+                if (!src_plastic && sp.pre_last > 1) wv = wv * (float)sp.pre_last;
+                const int32_t q = (int32_t)std::nearbyint(wv * scale);
+                std::atomic_ref<int32_t>(net.ring_q[cell_of(j)]).fetch_add(q, std::memory_order_relaxed);
+                ++ev;
+            }
+            ovf += local_ovf;
+        }
+    } else if (P.deterministic) {
         // per (step, cell): left fold in (source, synapse) order, then add
         for (const auto& sp : spikes) {
             for (uint64_t j = net.row_ptr[sp.src]; j < net.row_ptr[sp.src + 1]; ++j) {
@@ -654,8 +713,14 @@ int oracle_net_build(void* h) {
     Net& net = *static_cast<Net*>(h);
     build_csr(net);
     init_state(net);
+    if (net.prm.deterministic == 2) {
+        net.fx_shift = exact_shift(net);
+        if (net.fx_shift < 0) return -1;
+    }
     return 0;
 }
+
+int32_t oracle_net_exact_shift(void* h) { return static_cast<Net*>(h)->fx_shift; }
 
 uint32_t oracle_net_neurons(void* h) { return static_cast<Net*>(h)->n; }
 uint64_t oracle_net_synapses(void* h) { return static_cast<Net*>(h)->tgt.size(); }
@@ -720,7 +785,8 @@ void oracle_net_set_state(void* h, const float* v, const uint32_t* refr) {
 
 void oracle_net_copy_ring(void* h, float* ring) {
     const Net& net = *static_cast<Net*>(h);
-    std::copy(net.ring.begin(), net.ring.end(), ring);
+    if (net.prm.deterministic == 2) std::memcpy(ring, net.ring_q.data(), net.ring_q.size() * 4);  // the sums' bits
+    else std::copy(net.ring.begin(), net.ring.end(), ring);
 }
 
 void oracle_net_copy_weights(void* h, float* w) {

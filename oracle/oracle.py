@@ -80,6 +80,7 @@ def load() -> C.CDLL:
             "oracle_net_copy_state": (None, [_vp, _vp, _vp]),
             "oracle_net_set_state": (None, [_vp, _vp, _vp]),
             "oracle_net_copy_ring": (None, [_vp, _vp]),
+            "oracle_net_exact_shift": (C.c_int32, [_vp]),
             "oracle_net_copy_weights": (None, [_vp, _vp]),
             "oracle_max_threads": (C.c_int, []),
             "oracle_reintegrate_fp64": (C.c_int, [_vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp, _vp,
@@ -129,8 +130,12 @@ class OracleNet:
     """The oracle's copy of a network described by a naer_b200.spec.NetSpec."""
 
     def __init__(self, spec, threads: int = 0, deterministic: bool | None = None):
+        """deterministic: None follows the spec (its exact-sum mode
+        included); True / False force the canonical fold / parallel adds."""
         lib = load()
-        prm = OrParams(spec.dt_us, int(spec.deterministic if deterministic is None else deterministic),
+        mode = (2 if getattr(spec, "exact", False) else int(spec.deterministic)) if deterministic is None \
+            else int(deterministic)
+        prm = OrParams(spec.dt_us, mode,
                        spec.poisson_seed, int(spec.stdp_enabled), spec.tau_plus_ms, spec.tau_minus_ms, spec.a_plus,
                        spec.a_minus, spec.w_max, spec.stdp_history, threads)
         pops = (OrPop * max(1, len(spec.pops)))()
@@ -145,7 +150,10 @@ class OracleNet:
                 conns[i].rp, conns[i].tg, conns[i].wv, conns[i].dv = (a.ctypes.data for a in c.csr)
         self._lib = lib
         self._h = lib.oracle_net_create(C.byref(prm), pops, len(spec.pops), conns, len(spec.conns))
-        lib.oracle_net_build(self._h)
+        if lib.oracle_net_build(self._h) != 0:
+            lib.oracle_net_destroy(self._h)
+            self._h = None
+            raise ValueError("weights too large for exact-sum aggregation")
         self.n = lib.oracle_net_neurons(self._h)
         self.S = lib.oracle_net_synapses(self._h)
 
@@ -159,6 +167,10 @@ class OracleNet:
             self.close()
         except Exception:
             pass
+
+    def exact_shift(self) -> int:
+        """S of the exact-sum mode: weights on the grid 2^-S."""
+        return self._lib.oracle_net_exact_shift(self._h)
 
     def population_base(self, pop: int) -> int:
         return self._lib.oracle_net_population_base(self._h, pop)

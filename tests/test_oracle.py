@@ -413,3 +413,27 @@ def test_explicit_csr_reproduces_a_rule(oracle_mod):
     sa, ia = oa.spikes()
     sb, ib = ob.spikes()
     assert len(ia) > 100 and np.array_equal(sa, sb) and np.array_equal(ia, ib)
+
+
+def test_exact_sum_mode(oracle_mod):
+    """The oracle's exact-sum mode (weights on the grid 2^-S, integer ring
+    sums): S from the largest possible cell sum, parallel runs with the
+    same bits, and potentials within 1e-5 of FP64 on the same spikes."""
+    O = oracle_mod
+    s = S.brunel_small(poisson_weight=1.0).with_(exact=True)
+    a, b = O.OracleNet(s, threads=1), O.OracleNet(s)
+    assert 10 <= a.exact_shift() <= 30
+    a.run(1500)
+    b.run(1500)
+    sa, sb = a.spikes(), b.spikes()
+    assert np.array_equal(sa[0], sb[0]) and np.array_equal(sa[1], sb[1]) and len(sa[1]) > 1000
+    v, _ = a.state()
+    assert np.array_equal(v.view(np.uint32), b.state()[0].view(np.uint32))
+    v64, _, _ = O.OracleNet(s).reintegrate_fp64(sa[0], sa[1], 1500)
+    err = np.abs(v.astype(np.float64) - v64) / np.maximum(np.abs(v64), 1.0)
+    assert err.max() <= 1e-5
+    big = S.NetSpec(exact=True)
+    A = big.add_pop(S.NOP, 500)
+    big.connect(A, A, capi.CONN_FIXED_INDEGREE, 3.0e7, degree=200, seed=2)
+    with pytest.raises(ValueError, match="exact-sum"):
+        O.OracleNet(big)
