@@ -287,7 +287,7 @@ def bench_plastic(args, local, stream_of):
             "stdp_history_overflows": int(st1["stdp_hist_overflow"])}
 
 
-def bench_batched(args, local, deterministic=False):
+def bench_batched(args, local, deterministic=False, exact=False):
     """Batched form: independent networks of uneven sizes (log-uniform 2k-50k
     neurons, in-degree 100-1000, own seeds, Poisson 5-30 Hz, STDP on half)
     packed into one engine, autotuned, CUDA-graph step loop, 2 s simulated
@@ -297,12 +297,13 @@ def bench_batched(args, local, deterministic=False):
     import numpy as np
     from naer_b200 import spec as S
     from naer_b200.forms import Batch
-    members = [m.with_(deterministic=deterministic) for m in S.batch_members(count=args.batch_members, seed=1)]
+    members = [m.with_(deterministic=deterministic, exact=exact)
+               for m in S.batch_members(count=args.batch_members, seed=1)]
     for m in members:
         m.raster_capacity = 1 << 22
     steps = args.batch_steps
     t0 = time.perf_counter()
-    b = Batch(members, device=local, deterministic=deterministic, raster_capacity=1 << 27).compile()
+    b = Batch(members, device=local, deterministic=deterministic, exact=exact, raster_capacity=1 << 27).compile()
     t1 = time.perf_counter()
     st0 = b.stats()
     t2 = time.perf_counter()
@@ -315,7 +316,7 @@ def bench_batched(args, local, deterministic=False):
     rng = np.random.default_rng(7)
     pick = rng.choice(len(members), min(args.plain_sample, len(members)), replace=False)
     identical = None
-    if deterministic:
+    if deterministic or exact:
         sp = b.read_spikes()
         run_s, all_s, alone = plain_runs([(members[int(i)], steps) for i in pick], local, rasters=True)
         identical = all(same_raster(b.member_spikes(int(i), sp), a) for i, a in zip(pick, alone))
@@ -328,7 +329,7 @@ def bench_batched(args, local, deterministic=False):
     return {
         "workload": f"{len(members)} networks, {st0['neurons']} neurons, {st0['synapses']} synapses in total; "
                     f"{steps} grid steps (2 s) each",
-        "aggregation": "deterministic" if deterministic else "atomic",
+        "aggregation": "exact" if exact else "deterministic" if deterministic else "atomic",
         "sims_per_s": len(members) / sim_s,
         "sims_per_s_with_build": len(members) / (sim_s + t1 - t0),
         "events_per_s": (st1["events"] - st0["events"]) / sim_s,
@@ -346,7 +347,7 @@ def bench_batched(args, local, deterministic=False):
     }
 
 
-def bench_served(args, local, deterministic=False, saturate=False):
+def bench_served(args, local, deterministic=False, saturate=False, exact=False):
     """Served form: a seeded Poisson stream of jobs (50/s; 1k-200k neurons
     log-uniform, in-degree 100-1000, 100 ms - 2 s, 30 % STDP) submitted on
     schedule to the continuous-batching server (150 GB budget); p50/p99
@@ -360,8 +361,8 @@ def bench_served(args, local, deterministic=False, saturate=False):
     from naer_b200.forms import Server
     from naer_b200 import _capi as capi_
     jobs = S.served_jobs(count=args.served_jobs, seed=1)
-    jobs = [(ta, spec.with_(deterministic=deterministic), steps) for ta, spec, steps in jobs]
-    srv = Server(device=local, budget_bytes=150 * 10**9, chunk_steps=256, deterministic=deterministic)
+    jobs = [(ta, spec.with_(deterministic=deterministic, exact=exact), steps) for ta, spec, steps in jobs]
+    srv = Server(device=local, budget_bytes=150 * 10**9, chunk_steps=256, deterministic=deterministic, exact=exact)
     ids = []
     t0 = time.perf_counter()
     for ta, spec, steps in jobs:
@@ -376,7 +377,7 @@ def bench_served(args, local, deterministic=False, saturate=False):
     rng = np.random.default_rng(11)
     pick = rng.choice(len(jobs), min(args.plain_sample, len(jobs)), replace=False)
     identical = None
-    if deterministic:
+    if deterministic or exact:
         run_s, all_s, alone = plain_runs([(jobs[int(i)][1], jobs[int(i)][2]) for i in pick], local, rasters=True)
         identical = all(same_raster(srv.spikes(ids[int(i)]), a) for i, a in zip(pick, alone))
     else:
@@ -385,7 +386,7 @@ def bench_served(args, local, deterministic=False, saturate=False):
     return {
         "workload": f"{len(jobs)} jobs, " + ("all submitted at once" if saturate else
                                             f"Poisson arrivals at 50/s over {jobs[-1][0]:.1f} s"),
-        "aggregation": "deterministic" if deterministic else "atomic",
+        "aggregation": "exact" if exact else "deterministic" if deterministic else "atomic",
         "sims_per_s": st["sims_per_s"],
         "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
         "drained": ok, "wall_s": wall, "done": st["done"], "failed": st["failed"], "failure_messages": errors,
@@ -665,6 +666,8 @@ def run_ours(args):
         if not args.no_det:
             forms["batched_deterministic"] = bench_batched(args, local, deterministic=True)
             forms["served_deterministic"] = bench_served(args, local, deterministic=True, saturate=True)
+            forms["batched_exact"] = bench_batched(args, local, exact=True)
+            forms["served_exact"] = bench_served(args, local, exact=True, saturate=True)
     if rank == 0 and world == 1 and not args.no_bins:
         forms["binned_aggregation"] = bench_bins(
             args, local, lambda n: torch.cuda.ExternalStream(n.stream(), device=torch.device("cuda", local)))
