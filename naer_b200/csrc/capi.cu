@@ -285,13 +285,15 @@ struct CheckpointHeader {
     uint64_t step, events, payload;
     uint64_t synapses, synapses_padded;
     uint32_t n_ids, n_storage, ring_slots, n_plastic, post_stride, dt_us;
+    int32_t ring_shift;  // exact-sum aggregation: the ring's integer grid 2^-S; -1: float ring
+    uint32_t pad_;
 };
 constexpr char kCheckpointMagic[8] = {'N', 'A', 'E', 'R', 'C', 'K', 'P', 'T'};
 
 CheckpointHeader checkpoint_header(naer::Engine& eng, const naer::NetHost& n) {
     CheckpointHeader h{};
     std::memcpy(h.magic, kCheckpointMagic, 8);
-    h.version = 1;
+    h.version = 2;
     h.stdp_on = n.dev.stdp_on;
     h.step = eng.host_step();
     h.events = eng.events_total();
@@ -304,6 +306,7 @@ CheckpointHeader checkpoint_header(naer::Engine& eng, const naer::NetHost& n) {
     h.n_plastic = n.dev.stdp_on ? n.n_plastic : 0;
     h.post_stride = n.post_stride;
     h.dt_us = n.params.dt_us;
+    h.ring_shift = n.params.aggregation == NAER_AGG_EXACT ? n.fx_shift : -1;
     return h;
 }
 }  // namespace
@@ -336,13 +339,14 @@ int naer_net_restore(naer_net* net, const void* buf, uint64_t size) {
         need(buf != nullptr && size >= sizeof(CheckpointHeader), NAER_E_INVALID, "not a checkpoint");
         CheckpointHeader h;
         std::memcpy(&h, buf, sizeof(h));
-        need(std::memcmp(h.magic, kCheckpointMagic, 8) == 0 && h.version == 1, NAER_E_INVALID, "not a checkpoint");
+        need(std::memcmp(h.magic, kCheckpointMagic, 8) == 0 && h.version == 2, NAER_E_INVALID, "not a checkpoint");
         net->eng->sync();
         const CheckpointHeader mine = checkpoint_header(*net->eng, net->net);
         need(h.stdp_on == mine.stdp_on && h.payload == mine.payload && h.synapses == mine.synapses &&
                  h.synapses_padded == mine.synapses_padded && h.n_ids == mine.n_ids &&
                  h.n_storage == mine.n_storage && h.ring_slots == mine.ring_slots &&
-                 h.n_plastic == mine.n_plastic && h.post_stride == mine.post_stride && h.dt_us == mine.dt_us,
+                 h.n_plastic == mine.n_plastic && h.post_stride == mine.post_stride && h.dt_us == mine.dt_us &&
+                 h.ring_shift == mine.ring_shift,
              NAER_E_INVALID, "checkpoint was taken from a network of another layout");
         need(size >= sizeof(h) + h.payload, NAER_E_INVALID, "checkpoint truncated");
         net->eng->load_state(net->net, static_cast<const uint8_t*>(buf) + sizeof(h));

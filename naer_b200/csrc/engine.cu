@@ -701,41 +701,64 @@ void Engine::free_net(NetHost& n) {
 // ---------------------------------------------------------------------------
 // descriptor tables
 
-// Shift S of the exact-sum aggregation's grid 2^-S for a built network:
-// the largest S <= 30 for which no ring-cell sum can leave int32.  A cell
-// receives at most one event per synapse into its neuron before it is
-// read, of magnitude at most max|w| (at least w_max in a plastic network)
-// times 10 (the largest POISSON multiplicity), each rounded by at most half
-// a unit.  -1: no S >= 0 holds that bound.
-int32_t Engine::exact_shift(NetHost& n) {
+// Shift S of the exact-sum aggregation's grid 2^-S for built networks
+// (fx_shift of each): the largest S <= 30 for which no ring-cell sum can
+// leave int32.  A cell receives at most one event per synapse into its
+// neuron before it is read, of magnitude at most max|w| (at least w_max in a
+// plastic network) times 10 (the largest POISSON multiplicity), each
+// rounded by at most half a unit.  -1: no S >= 0 holds that bound.  The
+// device reductions of every network are queued first and read back with
+// one synchronisation.
+void Engine::exact_shifts(const std::vector<NetHost*>& nets) {
+    if (nets.empty()) return;
     DeviceGuard g(device_);
-    const uint64_t S = n.synapses_padded;
-    uint32_t* in = static_cast<uint32_t*>(dalloc((uint64_t)n.n_storage * 4ull + 16));
-    unsigned int* out = reinterpret_cast<unsigned int*>(in + n.n_storage);  // [0] max |w| bits, [1] max in-degree
+    uint32_t ns_max = 1;
+    for (const NetHost* n : nets) ns_max = std::max(ns_max, n->n_storage);
+    const uint64_t in_bytes = (uint64_t)ns_max * 4ull;
+    const uint64_t st_bytes = (uint64_t)nets.size() * 8ull;
+    uint32_t* in = static_cast<uint32_t*>(dalloc(in_bytes));
+    unsigned int* out = nullptr;
     try {
-        NAER_CK(cudaMemsetAsync(in, 0, (uint64_t)n.n_storage * 4ull + 16, stream_));
+        out = static_cast<unsigned int*>(dalloc(st_bytes));  // per net: max |w| bits, max in-degree
+        NAER_CK(cudaMemsetAsync(out, 0, st_bytes, stream_));
         const uint32_t T = 256;
-        const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((S + T - 1) / T, (uint64_t)sm_count_ * 8));
-        if (S) k_exact_inputs<<<grid, T, 0, stream_>>>(n.tgt, n.w, S, in, out);
-        const uint32_t g2 = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n.n_storage + T - 1) / T, (uint64_t)sm_count_ * 4));
-        if (n.n_storage) k_max_u32<<<g2, T, 0, stream_>>>(in, n.n_storage, out + 1);
+        for (size_t i = 0; i < nets.size(); ++i) {
+            const NetHost& n = *nets[i];
+            const uint64_t S = n.synapses_padded;
+            NAER_CK(cudaMemsetAsync(in, 0, (uint64_t)n.n_storage * 4ull, stream_));
+            const uint32_t g1 = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((S + T - 1) / T, (uint64_t)sm_count_ * 8));
+            if (S) k_exact_inputs<<<g1, T, 0, stream_>>>(n.tgt, n.w, S, in, out + 2 * i);
+            const uint32_t g2 =
+                (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n.n_storage + T - 1) / T, (uint64_t)sm_count_ * 4));
+            if (n.n_storage) k_max_u32<<<g2, T, 0, stream_>>>(in, n.n_storage, out + 2 * i + 1);
+        }
         NAER_CK(cudaGetLastError());
-        unsigned int h[2] = {0, 0};
-        NAER_CK(cudaMemcpyAsync(h, out, 8, cudaMemcpyDeviceToHost, stream_));
+        std::vector<unsigned int> h(2 * nets.size());
+        NAER_CK(cudaMemcpyAsync(h.data(), out, st_bytes, cudaMemcpyDeviceToHost, stream_));
         NAER_CK(cudaStreamSynchronize(stream_));
-        dfree(in, (uint64_t)n.n_storage * 4ull + 16);
+        dfree(out, st_bytes);
+        out = nullptr;
+        dfree(in, in_bytes);
         in = nullptr;
-        float maxw;
-        std::memcpy(&maxw, &h[0], 4);
-        if (n.params.stdp_enabled && n.n_plastic > 0) maxw = std::max(maxw, n.params.w_max);
-        bool poisson = false;
-        for (const PopSpec& ps : n.pops) poisson = poisson || (ps.type == kPOISSON && ps.size > 0);
-        const double bound = (double)h[1] * (double)maxw * (poisson ? 10.0 : 1.0);
-        for (int32_t sh = 30; sh >= 0; --sh)
-            if (bound * std::ldexp(1.0, sh) + (double)h[1] <= 2147483647.0) return sh;
-        return -1;
+        for (size_t i = 0; i < nets.size(); ++i) {
+            NetHost& n = *nets[i];
+            float maxw;
+            std::memcpy(&maxw, &h[2 * i], 4);
+            if (n.params.stdp_enabled && n.n_plastic > 0) maxw = std::max(maxw, n.params.w_max);
+            bool poisson = false;
+            for (const PopSpec& ps : n.pops) poisson = poisson || (ps.type == kPOISSON && ps.size > 0);
+            const uint32_t max_in = h[2 * i + 1];
+            const double bound = (double)max_in * (double)maxw * (poisson ? 10.0 : 1.0);
+            n.fx_shift = -1;
+            for (int32_t sh = 30; sh >= 0; --sh)
+                if (bound * std::ldexp(1.0, sh) + (double)max_in <= 2147483647.0) {
+                    n.fx_shift = sh;
+                    break;
+                }
+        }
     } catch (...) {
-        if (in) dfree(in, (uint64_t)n.n_storage * 4ull + 16);
+        if (out) dfree(out, st_bytes);
+        if (in) dfree(in, in_bytes);
         throw;
     }
 }
@@ -753,6 +776,12 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     std::vector<ChunkDev> chunks;
     h_nets_.clear();
     id_offsets_.clear();
+    if (aggregation == NAER_AGG_EXACT) {  // grids of the networks installed for the first time
+        std::vector<NetHost*> fresh;
+        for (NetHost* n : nets)
+            if (n->fx_shift == kFxUnknown) fresh.push_back(n);
+        exact_shifts(fresh);
+    }
     uint64_t key_base = 0;
     uint64_t qcap = 0;
     uint64_t id_off = 0;
@@ -761,7 +790,6 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
         NetDev d = n.dev;
         d.fx_scale = d.fx_inv = 0.0f;
         if (aggregation == NAER_AGG_EXACT) {
-            if (n.fx_shift == kFxUnknown) n.fx_shift = exact_shift(n);
             if (n.fx_shift < 0)
                 throw Error(NAER_E_OVERFLOW, "weights too large for exact-sum aggregation: no fixed-point grid "
                                              "holds the largest possible ring-cell sum in 32 bits");

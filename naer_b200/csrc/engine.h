@@ -144,7 +144,7 @@ public:
     void build(NetHost& net);
     void free_net(NetHost& net);
     // Installs the nets' descriptor tables; nets must outlive the engine use.
-    int32_t exact_shift(NetHost& n);
+    void exact_shifts(const std::vector<NetHost*>& nets);
     void install(const std::vector<NetHost*>& nets, uint64_t raster_capacity, bool record,
                  uint32_t aggregation);
 

@@ -315,6 +315,11 @@ void Server::build_loop() {
             const double t = now_s();
             try {
                 eng->build(*j->net);
+                if (prm_.aggregation == NAER_AGG_EXACT) {  // its fixed-point grid, off the stepper's path
+                    eng->exact_shifts({j->net.get()});
+                    if (j->net->fx_shift < 0)
+                        throw Error(NAER_E_OVERFLOW, "weights too large for exact-sum aggregation");
+                }
                 if (!j->saved.empty()) {  // a pre-empted job: its state from before
                     eng->load_state(*j->net, j->saved.data());
                     std::vector<uint8_t>().swap(j->saved);

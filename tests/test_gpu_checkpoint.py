@@ -34,6 +34,7 @@ def state_of(net):
     lambda: S.plastic_indegree(n=3000, k=200, drive_weight=21.0).with_(deterministic=True),
     lambda: S.brunel_small(poisson_weight=1.0).with_(deterministic=True),
     lambda: integer_weight_net(n=5000, k=200),  # atomic mode, exact on integer weights
+    lambda: S.plastic_indegree(n=3000, k=200, drive_weight=21.0).with_(exact=True),  # exact-sum mode
 ])
 def test_restore_continues_the_run(lib, make):
     s = make()
@@ -70,6 +71,12 @@ def test_restore_rejects_other_layouts(lib):
             b.restore(ck)
         with pytest.raises(NaerError, match="not a checkpoint"):
             a.restore(b"garbage" * 20)
+    # the same layout with the ring holding fixed-point sums instead of floats
+    with S.build(S.brunel_small(poisson_weight=1.0)) as a, \
+            S.build(S.brunel_small(poisson_weight=1.0).with_(exact=True)) as b:
+        a.run(10)
+        with pytest.raises(NaerError, match="another layout"):
+            b.restore(a.checkpoint())
 
 
 def alone(spec, steps):
