@@ -1111,13 +1111,12 @@ __device__ __forceinline__ void rest_item(const EngineDev& eng, const RestWork& 
 // One first-part item of k_step (piece `piece` of spike e's due part: the
 // delay-1 synapses of a static source, the whole row of a plastic one);
 // the piece-0 warp appends the spike to the raster at rbase + e.
-__device__ __forceinline__ void first_item(const EngineDev& eng, const SpikeRec* __restrict__ queue,
-                                           const uint32_t* __restrict__ qid, uint32_t qb, uint32_t e,
+// (rv, row: spike e's record and row, already loaded)
+__device__ __forceinline__ void first_item(const EngineDev& eng, const int4 rv, const uint4 row,
+                                           const uint32_t* __restrict__ qid, uint32_t e,
                                            uint32_t piece, uint32_t split, unsigned long long s,
                                            unsigned long long rbase, const NetDev* net0, uint32_t lane,
                                            unsigned long long& ev, uint32_t& ovf, const BinTable& bt) {
-    const int4 rv = __ldcg(reinterpret_cast<const int4*>(queue + e));
-    const uint4 row = __ldcg(eng.qrow[qb] + e);  // with the record: no dependent row lookup
     SpikeRec r;
     r.net = (uint32_t)rv.x;
     r.src = (uint32_t)rv.y;
@@ -1425,12 +1424,40 @@ __global__ void __launch_bounds__(kLifThreads, NAER_RUN_MIN_BLOCKS)
         const uint32_t Q = s_q;
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->qtail[(s + 2) & 3ull] = 0u;  // reused by step s+2
         {
+            // this warp's items it = gw, gw + W, ... 32 at a time: lane k
+            // loads item k's record and row, and only the items with work in
+            // them (piece 0 writes the raster entry) are delivered, so the
+            // empty pieces of short parts cost one shared round trip
             const uint32_t split = eng.split_first;
             const uint64_t n1 = (uint64_t)Q * split;
-            for (uint64_t it = gw; it < n1; it += W) {
-                const uint32_t e = (uint32_t)(it / split);
-                first_item(eng, queue, qid, qb, e, (uint32_t)(it - (uint64_t)e * split), split, s, rbase, &s_net0,
-                           lane, ev, ovf, bt);
+            for (uint64_t it0 = gw; it0 < n1; it0 += 32ull * W) {
+                const uint64_t it = it0 + (uint64_t)lane * W;
+                int4 rv = make_int4(0, 0, 0, 0);
+                uint4 row = make_uint4(0, 0, 0, 0);
+                uint32_t e = 0, piece = 0;
+                bool work = false;
+                if (it < n1) {
+                    e = (uint32_t)(it / split);
+                    piece = (uint32_t)(it - (uint64_t)e * split);
+                    rv = __ldcg(reinterpret_cast<const int4*>(queue + e));
+                    row = __ldcg(eng.qrow[qb] + e);  // with the record: no dependent row lookup
+                    const NetDev* np = rv.x == 0 ? &s_net0 : eng.nets + rv.x;
+                    const bool plastic_src = np->stdp_on && (uint32_t)rv.y < np->n_plastic;
+                    const uint64_t pw = plastic_src ? kPlasticPiece : eng.scatter_piece;
+                    work = piece == 0 || (uint64_t)piece * pw < (plastic_src ? row.w : row.z);
+                }
+                uint32_t m = __ballot_sync(0xFFFFFFFFu, work);
+                while (m) {
+                    const int L = __ffs(m) - 1;
+                    m &= m - 1u;
+                    const int4 rvL = make_int4(__shfl_sync(0xFFFFFFFFu, rv.x, L), __shfl_sync(0xFFFFFFFFu, rv.y, L),
+                                               __shfl_sync(0xFFFFFFFFu, rv.z, L), __shfl_sync(0xFFFFFFFFu, rv.w, L));
+                    const uint4 rowL =
+                        make_uint4(__shfl_sync(0xFFFFFFFFu, row.x, L), __shfl_sync(0xFFFFFFFFu, row.y, L),
+                                   __shfl_sync(0xFFFFFFFFu, row.z, L), __shfl_sync(0xFFFFFFFFu, row.w, L));
+                    first_item(eng, rvL, rowL, qid, __shfl_sync(0xFFFFFFFFu, e, L),
+                               __shfl_sync(0xFFFFFFFFu, piece, L), split, s, rbase, &s_net0, lane, ev, ovf, bt);
+                }
             }
         }
         if (wib != 0) {
