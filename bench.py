@@ -309,10 +309,14 @@ def bench_batched(args, local, deterministic=False, exact=False):
     t2 = time.perf_counter()
     tune = b.autotune(64)  # its trial steps are part of the members' simulated time
     done = b.stats()["step"]
+    ph0 = b.phases()
     b.run(steps - done)
     b.finish()
     t3 = time.perf_counter()
     st1 = b.stats()
+    ph1 = b.phases()
+    ph = {k: ph1[k] - ph0[k] for k in ph1 if k != "reserved"}
+    ph_tot = sum(ph.values()) or 1.0
     rng = np.random.default_rng(7)
     pick = rng.choice(len(members), min(args.plain_sample, len(members)), replace=False)
     identical = None
@@ -334,6 +338,7 @@ def bench_batched(args, local, deterministic=False, exact=False):
         "sims_per_s_with_build": len(members) / (sim_s + t1 - t0),
         "events_per_s": (st1["events"] - st0["events"]) / sim_s,
         "us_per_step": sim_s / steps * 1e6,
+        "phase_split": {k: round(v / ph_tot, 3) for k, v in ph.items()},
         "build_s": t1 - t0,
         "autotune": {k: tune[k] for k in ("blocks_per_sm", "launch_steps", "scatter_split", "graph_launches",
                                           "step_kernel", "best_us_per_step", "default_us_per_step", "trials")},

@@ -425,6 +425,9 @@ NAER_API int naer_batch_read_spikes(naer_batch* batch, uint64_t first, uint64_t 
 NAER_API int naer_batch_clear_spikes(naer_batch* batch);
 /* Whole-batch counters (synapses and neurons summed over members). */
 NAER_API int naer_batch_get_stats(naer_batch* batch, naer_stats* st);
+/* The step kernel's phase split for the whole batch, as naer_net_get_phases
+ * (ms, accumulated since compile, measured by the kernel's first block). */
+NAER_API int naer_batch_get_phases(naer_batch* batch, double* phase_ms5);
 NAER_API int naer_batch_read_state(naer_batch* batch, uint32_t member, float* v, uint32_t* refractory);
 NAER_API int naer_batch_stream(naer_batch* batch, void** stream);
 

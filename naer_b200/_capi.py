@@ -240,6 +240,7 @@ PROTOTYPES = {
     "naer_batch_read_spikes": [_vp, C.c_uint64, C.c_uint64, _vp, _vp, _vp, _P(C.c_uint64)],
     "naer_batch_clear_spikes": [_vp],
     "naer_batch_get_stats": [_vp, _P(Stats)],
+    "naer_batch_get_phases": [_vp, _vp],
     "naer_batch_read_state": [_vp, C.c_uint32, _vp, _vp],
     "naer_batch_stream": [_vp, _P(_vp)],
     "naer_server_params_default": [_P(ServerParams)],

@@ -765,6 +765,14 @@ int naer_batch_clear_spikes(naer_batch* batch) {
     });
 }
 
+int naer_batch_get_phases(naer_batch* batch, double* phase_ms5) {
+    return guarded([&] {
+        need(batch && phase_ms5, NAER_E_INVALID, "null argument");
+        need(batch->b->compiled(), NAER_E_STATE, "batch is not compiled");
+        batch->b->engine().get_phases(phase_ms5);
+    });
+}
+
 int naer_batch_get_stats(naer_batch* batch, naer_stats* st) {
     return guarded([&] {
         need(batch && st, NAER_E_INVALID, "null argument");

@@ -116,10 +116,9 @@ __device__ __forceinline__ void load_post_row(const int32_t* row, uint32_t strid
 // The target's whole post row is loaded at once and every decay-table
 // lookup is issued before the sequential weight updates use them.
 // Plays the role of update_synapse (include/naer/kernels/stdp.cl:8-30).
-__device__ __forceinline__ float stdp_update(const StdpView& n, float w, uint32_t tgt, int32_t t,
-                                             int32_t pre_last, float pre_x, uint32_t& overflow) {
-    int32_t r[kPostWordsMax];
-    load_post_row(n.post + (size_t)tgt * n.post_stride, n.post_stride, r);
+// stdp_apply takes the post row already in registers (stdp_update loads it).
+__device__ __forceinline__ float stdp_apply(const StdpView& n, float w, const int32_t (&r)[kPostWordsMax], int32_t t,
+                                            int32_t pre_last, float pre_x, uint32_t& overflow) {
     if (pre_last >= 0) {
         // history entries newer than pre_last form a prefix (newest first)
         uint32_t c = 0;
@@ -150,6 +149,13 @@ __device__ __forceinline__ float stdp_update(const StdpView& n, float w, uint32_
         w = fmaxf(__fsub_rn(w, __fmul_rn(n.a_minus, y)), 0.0f);
     }
     return w;
+}
+
+__device__ __forceinline__ float stdp_update(const StdpView& n, float w, uint32_t tgt, int32_t t,
+                                             int32_t pre_last, float pre_x, uint32_t& overflow) {
+    int32_t r[kPostWordsMax];
+    load_post_row(n.post + (size_t)tgt * n.post_stride, n.post_stride, r);
+    return stdp_apply(n, w, r, t, pre_last, pre_x, overflow);
 }
 
 // Plasticity bookkeeping of plastic neuron i spiking at local step t: post

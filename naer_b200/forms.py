@@ -82,6 +82,12 @@ class Batch:
         capi.call("naer_batch_get_stats", self._h, C.byref(st))
         return {k: getattr(st, k) for k, _ in capi.Stats._fields_}
 
+    def phases(self) -> dict:
+        """The step kernel's device time split (ms since compile, first block)."""
+        ph = (C.c_double * 5)()
+        capi.call("naer_batch_get_phases", self._h, C.cast(ph, C.c_void_p))
+        return {k: ph[i] for i, k in enumerate(["lif", "lif_wait", "scatter", "reserved", "scatter_wait"])}
+
     def read_spikes(self):
         """(member, step, id) arrays of every recorded spike."""
         total = self.stats()["spikes"]
