@@ -87,6 +87,22 @@ def test_batch_autotune_keeps_results(lib):
             assert np.array_equal(st, bst) and np.array_equal(ids, bids)
 
 
+def test_batch_phase_split(lib):
+    """naer_batch_get_phases: the step kernel's time split accumulates while
+    the batch steps (four phases, non-negative, growing with the steps)."""
+    with Batch(small_members(count=3)).compile() as b:
+        b.run(128)
+        b.finish()
+        p0 = b.phases()
+        b.run(256)
+        b.finish()
+        p1 = b.phases()
+    assert set(p1) == {"lif", "lif_wait", "scatter", "reserved", "scatter_wait"}
+    assert all(v >= 0 for v in p0.values()) and p1["reserved"] == 0
+    grown = {k: p1[k] - p0[k] for k in ("lif", "lif_wait", "scatter", "scatter_wait")}
+    assert all(v >= 0 for v in grown.values()) and grown["lif"] > 0 and sum(grown.values()) > 0
+
+
 def test_batch_rejects_bad_member(lib):
     s = S.NetSpec()
     P = s.add_pop(S.POISSON, 10, rate_hz=10.0)
