@@ -466,7 +466,8 @@ typedef struct naer_server_params {
     uint32_t launch_steps;     /* grid steps per persistent step launch, 1..64 (0 = default);
                                   builds run between launches, so short launches let jobs in sooner
                                   and long ones pay less launch overhead per step */
-    uint32_t pad_;
+    uint32_t step_kernel;      /* atomic and exact-sum aggregation: NAER_KERNEL_TWO_BARRIER (default; the
+                                  served job mix completes more jobs per second with it) or NAER_KERNEL_SPLIT */
 } naer_server_params;
 
 #define NAER_JOB_QUEUED 0u

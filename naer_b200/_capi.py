@@ -133,7 +133,7 @@ class ServerParams(C.Structure):
         ("blocks_per_sm", C.c_uint32),
         ("chunk_ms", C.c_double),
         ("launch_steps", C.c_uint32),
-        ("pad_", C.c_uint32),
+        ("step_kernel", C.c_uint32),
     ]
 
 

@@ -825,6 +825,7 @@ int naer_server_params_default(naer_server_params* p) {
     p->blocks_per_sm = 0;
     p->chunk_ms = 10.0;
     p->launch_steps = 0;
+    p->step_kernel = NAER_KERNEL_TWO_BARRIER;
     return NAER_OK;
 }
 
@@ -843,6 +844,8 @@ int naer_server_create(int device, const naer_server_params* params, naer_server
         sp.blocks_per_sm = p.blocks_per_sm;
         sp.chunk_ms = p.chunk_ms;
         if (p.launch_steps) sp.launch_steps = p.launch_steps;
+        need(p.step_kernel <= NAER_KERNEL_TWO_BARRIER, NAER_E_INVALID, "unknown step kernel");
+        sp.step_kernel = p.step_kernel;
         auto h = std::make_unique<naer_server>();
         h->s = std::make_unique<naer::Server>(device, sp);
         *out = h.release();

@@ -260,8 +260,7 @@ uint32_t Engine::fast_chunk_capacity(uint32_t aggregation) {
     int optin = 0;
     NAER_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
     const bool det = aggregation == NAER_AGG_DETERMINISTIC;
-    // exact-sum aggregation runs the split kernel whatever the tuning says
-    const bool split = det || tuning_.step_kernel == NAER_KERNEL_SPLIT || aggregation == NAER_AGG_EXACT;
+    const bool split = det || tuning_.step_kernel == NAER_KERNEL_SPLIT;
     const void* kern = det ? (const void*)k_det_step<true>
                            : split ? (const void*)k_step<true> : (const void*)k_run<true>;
     cudaFuncAttributes fa{};
@@ -864,8 +863,8 @@ void Engine::install(const std::vector<NetHost*>& nets, uint64_t raster_capacity
     // deterministic path's LIF uses the same queue regions.
     const bool det = aggregation == NAER_AGG_DETERMINISTIC;
     const bool exact = aggregation == NAER_AGG_EXACT;
-    // exact-sum aggregation: the split kernel, integer reductions, no binning
-    split_kernel_ = !det && (tuning_.step_kernel == NAER_KERNEL_SPLIT || exact);
+    // exact-sum aggregation: integer reductions in either atomic kernel, no binning
+    split_kernel_ = !det && tuning_.step_kernel == NAER_KERNEL_SPLIT;
     const bool list_kernel = det || split_kernel_;  // one contiguous spike list per step
     const void* kern_smem = det ? (const void*)k_det_step<true>
                                 : split_kernel_ ? (const void*)k_step<true> : (const void*)k_run<true>;
@@ -1050,7 +1049,7 @@ TuneResult Engine::autotune(uint32_t trial_steps) {
                     if (bps == 0 && L == kDriveSlots && sp == 0) {
                         t.scatter_piece = eng_piece_default == 128 ? kScatterPiece : 128u;
                     }
-                    if (bps == 1 && L == kDriveSlots && sp == 0 && aggregation_ == NAER_AGG_ATOMIC)
+                    if (bps == 1 && L == kDriveSlots && sp == 0 && aggregation_ != NAER_AGG_DETERMINISTIC)
                         t.step_kernel = NAER_KERNEL_TWO_BARRIER;
                     // shared-memory binning of the ring reductions
                     if (bps == 0 && L == kDriveSlots / 2 && sp == 0 && aggregation_ == NAER_AGG_ATOMIC)

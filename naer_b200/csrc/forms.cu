@@ -407,6 +407,7 @@ void Server::loop() {
         Tuning tn;
         tn.launch_steps = prm_.launch_steps;
         tn.blocks_per_sm = prm_.blocks_per_sm;
+        tn.step_kernel = prm_.step_kernel;
         eng->set_tuning(tn);
         // Admission keeps the running set within the step kernel's fastest
         // geometry (neuron state in shared memory, most blocks per SM).  A

@@ -55,6 +55,7 @@ struct ServerParams {
     uint32_t blocks_per_sm = 0;    // step-kernel blocks per SM (0 = most that fit)
     double chunk_ms = 10.0;        // target device time per chunk (sets its step count)
     uint32_t launch_steps = 4;     // grid steps per persistent step launch (builds run between launches)
+    uint32_t step_kernel = 1;      // NAER_KERNEL_TWO_BARRIER (k_run) / NAER_KERNEL_SPLIT (k_step)
 };
 
 enum JobState : uint32_t { kJobQueued = 0, kJobRunning = 1, kJobDone = 2, kJobFailed = 3, kJobCancelled = 4 };

@@ -420,6 +420,7 @@ __device__ __forceinline__ void scatter_step(const EngineDev& eng, unsigned long
         StdpView sv;
         if (plastic_src) sv = stdp_view(*np);
         const float mult = (!plastic_src && r.aux0 > 1) ? (float)r.aux0 : 1.0f;
+        const float qs = np->fx_scale;  // exact-sum aggregation: 2^S, else 0
 
         for (uint64_t base = beg + (uint64_t)piece * psz; base < end; base += (uint64_t)split * psz) {
             uint4 tg[kScatterUnroll];
@@ -452,7 +453,9 @@ __device__ __forceinline__ void scatter_step(const EngineDev& eng, unsigned long
                         __stcg(w_a + off + j, w);
                     }
                     if (mult != 1.0f) w = __fmul_rn(w, mult);
-                    red_add_f32(ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt, w);
+                    float* cell = ring + (size_t)ring_slot(tmod, d, D) * Ns + tgt;
+                    if (qs != 0.0f) red_add_s32(cell, __float2int_rn(__fmul_rn(w, qs)));
+                    else red_add_f32(cell, w);
                     ++ev;
                 }
             }

@@ -143,7 +143,8 @@ class Server:
 
     def __init__(self, device: int = 0, budget_bytes: int = 150 * 10**9, chunk_steps: int = 256,
                  deterministic: bool = False, max_jobs: int = 1024, raster_capacity: int = 1 << 24,
-                 blocks_per_sm: int = 0, chunk_ms: float = 10.0, launch_steps: int = 0, exact: bool = False):
+                 blocks_per_sm: int = 0, chunk_ms: float = 10.0, launch_steps: int = 0, exact: bool = False,
+                 step_kernel: int = capi.KERNEL_TWO_BARRIER):
         capi.load()
         p = capi.ServerParams()
         capi.call("naer_server_params_default", C.byref(p))
@@ -155,6 +156,7 @@ class Server:
         p.blocks_per_sm = int(blocks_per_sm)
         p.chunk_ms = float(chunk_ms)
         p.launch_steps = int(launch_steps)
+        p.step_kernel = int(step_kernel)
         h = C.c_void_p()
         capi.call("naer_server_create", int(device), C.byref(p), C.byref(h))
         self._h = h

@@ -85,6 +85,25 @@ def test_exact_multi_chunk_geometry(oracle_mod, lib):
                               chunks=[64, 1, 200, 135])
 
 
+@pytest.mark.parametrize("make, steps", [
+    (poisson_multiplicity_net, 600),
+    (lambda: S.plastic_indegree(n=3000, k=200, drive_weight=21.0), 1500),
+])
+def test_exact_two_barrier_kernel_matches_oracle(oracle_mod, lib, make, steps):
+    """The two-barrier kernel (k_run, the served form's default) reduces the
+    same fixed-point integers: the same bits as the oracle."""
+    assert_matches_oracle(oracle_mod, make().with_(exact=True), steps,
+                          tuning=dict(step_kernel=capi.KERNEL_TWO_BARRIER), chunks=[64, 1, 300, steps - 365])
+
+
+def test_exact_two_barrier_multi_chunk_geometry(oracle_mod, lib):
+    s = S.scatter_outdegree(n=300_000, k=40).with_(exact=True)
+    for state in (capi.STATE_SHARED, capi.STATE_GLOBAL):
+        assert_matches_oracle(oracle_mod, s, 300, tuning=dict(blocks_per_sm=1, neuron_state=state,
+                                                             step_kernel=capi.KERNEL_TWO_BARRIER),
+                              chunks=[64, 1, 235])
+
+
 def test_exact_repeats_and_batch_members(lib):
     """Two runs give the same bits, and batch members their runs alone."""
     specs = [S.scatter_outdegree(n=n, k=150, seed=sd).with_(exact=True) for n, sd in [(40_000, 3), (23_000, 4)]]
