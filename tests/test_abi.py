@@ -166,6 +166,10 @@ def test_server_defaults(lib):
     assert lib.naer_server_params_default(C.byref(p)) == 0
     assert p.budget_bytes == 150 * 10**9 and p.chunk_steps == 256 and p.aggregation == capi.AGG_ATOMIC
     assert p.launch_steps == 0  # library default
+    assert p.step_kernel == capi.KERNEL_TWO_BARRIER
+    p.step_kernel = 7  # refused before any device work
+    h = C.c_void_p()
+    assert lib.naer_server_create(0, C.byref(p), C.byref(h)) == capi.NAER_E_INVALID and not h.value
 
 
 def test_forms_workloads():
