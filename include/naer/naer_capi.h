@@ -390,7 +390,9 @@ typedef struct naer_tuning {
 /* naer_tuning.step_kernel.  SPLIT: one contiguous spike list per step,
  * delay-1 synapses delivered before the next LIF and the rest of each row
  * while the grid waits at its barriers.  TWO_BARRIER: per-block spike
- * regions, the whole scatter between two grid barriers.  Same results. */
+ * regions, the whole scatter between two grid barriers.  Same results; both
+ * serve atomic and exact-sum aggregation (deterministic aggregation has a
+ * kernel of its own). */
 #define NAER_KERNEL_SPLIT 0u
 #define NAER_KERNEL_TWO_BARRIER 1u
 
